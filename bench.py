@@ -1,0 +1,479 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 carousel phase-retrieval backend.
+
+Workload (the carousel configuration): 128 x 128 complex64 patterns, 90 angles
+at 2 degrees, 10 episodes x 10 difference-map iterations per angle, batched
+over B random starts (default 148, one per SM), with the reference driver's
+carousel mix, last-episode convergence error and final projection
+(src/CPRA_MKL.cpp:59-140).  One step = that whole 2D stage for one batch of
+starts.  Inputs are seeded synthetic data (cpra_b200.synth).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs its own batch of
+starts (starts are independent: weak scaling, no data-path collective); the
+reported time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "carousel-phase-retrieval-algorithm_b200"))
+
+METRIC = "pattern-iterations/s"
+DM_BYTES_PER_PIXEL = 56  # read+write x, t1, t2 (complex64) + read A, S (float32) per pattern-iteration
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--starts", type=int, default=148, help="random starts per GPU")
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--angles", type=int, default=90)
+    ap.add_argument("--episodes", type=int, default=10)
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_config(a, ws):
+    return {
+        "workload": f"carousel 2D stage: {a.size}x{a.size} complex64, {a.angles} angles, "
+                    f"{a.episodes} episodes x {a.iters} DM iterations, {a.starts} starts per GPU",
+        "pattern": [a.size, a.size], "angles": a.angles, "episodes": a.episodes, "iters_per_angle": a.iters,
+        "starts_per_gpu": a.starts, "global_batch": a.starts * ws, "beta": 0.9,
+        "l2": "inputs larger than L2 (x is angles*starts*size^2*8 bytes per GPU)",
+        "parallelism": f"replicas over starts x{ws}",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        load = [v for v in sm if v > 0.5 * (mx or max(sm))] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the reference's MklImpl<T> operators + DFTI shim)
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(A, S, size, iters, seconds, threads):
+    """pattern-iterations/s of the reference operator code on the host cores:
+    1 start, `iters` DM iterations per angle over as many angles as fit in
+    about `seconds`.  Returns (rate, sample_description, cores)."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import ref_lib
+    if not ref_lib.available():
+        return None, "oracle/_ref not built", 0
+    cores = ref_lib.set_threads(threads)
+    M = N = size
+    MN = M * N
+    rng = np.random.default_rng(0)
+    impl = ref_lib.RefImpl(np.float32, M, N, 1, 1)
+
+    def run(n_angles):
+        x = (rng.uniform(0, 1, MN) + 1j * rng.uniform(0, 1, MN)).astype(np.complex64)
+        t0 = time.perf_counter()
+        for p in range(n_angles):
+            q = p % A.shape[0]
+            t1, t2 = x.copy(), x.copy()
+            impl.dm_iterations(x, t1, t2, np.ascontiguousarray(A[q].ravel()), np.ascontiguousarray(S[q].ravel()),
+                               MN, 1, 0.9, iters)
+        return time.perf_counter() - t0
+
+    t = run(2)
+    per_angle = max(t / 2, 1e-4)
+    n = max(2, int(seconds / per_angle))
+    t = run(n)
+    rate = n * iters / t
+    return rate, f"1 start x {n} angles x {iters} DM iterations at {M}x{N} (reference MklImpl operators, " \
+                 f"project DFTI shim FFT)", cores
+
+
+# ---------------------------------------------------------------------------
+# plain per-operator path on the GPU: torch.fft (cuFFT) + element-wise kernels
+# in the reference CUDA backend's call order (CUDA_Impl.inl), for comparison
+# ---------------------------------------------------------------------------
+def per_op_rate(torch, A, S, B, size, iters, reps=2):
+    dev = torch.device("cuda")
+    M = N = size
+    Ad = torch.from_numpy(A[0]).to(dev)
+    Sd = torch.from_numpy(S[0]).to(dev)
+    x = torch.rand(B, M, N, dtype=torch.complex64, device=dev)
+    t1, t2 = x.clone(), x.clone()
+    beta = float(np.float32(0.9))
+
+    def fwd(t):
+        t = torch.fft.fftshift(t, dim=(-2, -1))
+        t = torch.fft.fft2(t)
+        return torch.fft.fftshift(t, dim=(-2, -1))
+
+    def bwd(t):
+        t = torch.fft.fftshift(t, dim=(-2, -1))
+        t = torch.fft.ifft2(t)
+        return torch.fft.fftshift(t, dim=(-2, -1))
+
+    def dc(t):
+        keep = (Ad == 0) | (t.abs() == 0)
+        return torch.where(keep, t, torch.polar(Ad.expand_as(t.real), t.angle()))
+
+    def sc(t):
+        return torch.complex(torch.where(Sd < 0.9, torch.zeros_like(t.real), t.real), torch.zeros_like(t.real))
+
+    def it(x, t1, t2):
+        t1 = bwd(dc(fwd(t1)))
+        t1 = (-1 / beta) * x + (1 + 1 / beta) * t1
+        t1 = sc(t1)
+        t2 = sc(t2)
+        t2 = (1 / beta) * x + (1 - 1 / beta) * t2
+        t2 = bwd(dc(fwd(t2)))
+        x = beta * t1 + x
+        x = -beta * t2 + x
+        return x, t1, t2
+
+    for _ in range(3):
+        x, t1, t2 = it(x, t1, t2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps * iters):
+        x, t1, t2 = it(x, t1, t2)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return B * reps * iters / (ms / 1e3)
+
+
+def read_traffic(kernel_key):
+    """dram bytes per pattern-iteration of the fused kernel from the committed
+    ncu summary (profiles/ncu_traffic.txt: `<kernel> <bytes_per_pattern_iteration>`)."""
+    f = REPO / "profiles" / "ncu_traffic.txt"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        parts = ln.split()
+        if len(parts) >= 2 and parts[0] == kernel_key:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    f = REPO / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(a, ws, rank):
+    """--impl reference: the reference's CPU operator code on this host's cores."""
+    if rank != 0:
+        return
+    from cpra_b200 import synth
+    d = synth.carousel(n=a.size, P=min(a.angles, 8))
+    threads = os.cpu_count() or 1
+    sys.path.insert(0, str(REPO / "oracle"))
+    import ref_lib
+    if not ref_lib.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcpra_mklref.so is not built"}))
+        return
+    cores = ref_lib.set_threads(threads)
+    M = N = a.size
+    MN = M * N
+    impl = ref_lib.RefImpl(np.float32, M, N, 1, 1)
+    rng = np.random.default_rng(0)
+    angles_per_step = 4
+
+    def step():
+        x = (rng.uniform(0, 1, MN) + 1j * rng.uniform(0, 1, MN)).astype(np.complex64)
+        for p in range(angles_per_step):
+            t1, t2 = x.copy(), x.copy()
+            impl.dm_iterations(x, t1, t2, np.ascontiguousarray(d["A"][p].ravel()),
+                               np.ascontiguousarray(d["S"][p].ravel()), MN, 1, 0.9, a.iters)
+
+    for _ in range(a.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    t = time.perf_counter() - t0
+    units = a.steps * angles_per_step * a.iters
+    rate = units / t
+    sample = f"1 start x {angles_per_step} angles x {a.iters} DM iterations per step at {M}x{N}"
+    line = {
+        "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": workload_config(a, ws),
+        "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference MklImpl<float> operators compiled unchanged; FFT from the project DFTI shim (oneMKL absent)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    ws, rank, local = dist_env()
+    if a.impl == "reference":
+        run_reference_arm(a, ws, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import cpra_b200
+    from cpra_b200 import synth
+
+    M = N = a.size
+    P, B, E, IT = a.angles, a.starts, a.episodes, a.iters
+    MN = M * N
+    d = synth.carousel(n=a.size, P=P, seed=1)
+    A_h = torch.from_numpy(np.ascontiguousarray(d["A"]).ravel()).pin_memory()
+    S_h = torch.from_numpy(np.ascontiguousarray(d["S"]).ravel()).pin_memory()
+    dev = torch.device("cuda", local)
+    A = A_h.to(dev)
+    S = S_h.to(dev)
+
+    impl = cpra_b200.B200Impl(M, N, 1, B)
+    # initial guesses: the reference's Initialize semantics (uniform [0,1) re and im), seeded per rank
+    impl.set_option(cpra_b200.OPT_SEED, 1234 + rank)
+    x0 = torch.empty(P * B * MN, dtype=torch.complex64, device=dev)
+    impl.Initialize(torch.view_as_real(x0), 2 * x0.numel())
+    impl.Sync()
+    x = torch.empty_like(x0)
+    err = np.zeros(P * B, np.float32)
+
+    def step_resident():
+        x.copy_(x0)
+        impl.cpra_run(x, A, S, P, B, E, IT, 0, 0.9, final_step=True, err=err)
+
+    units_per_step = P * B * E * IT  # DM pattern-iterations per step per GPU
+
+    def timed(fn, steps, warmup, kernel_timing=False):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if kernel_timing:
+            impl.set_option(cpra_b200.OPT_KERNEL_TIMING, 1)
+            impl.kernel_timing()
+        n0 = cpra_b200.kernels_launched()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        launches = cpra_b200.kernels_launched() - n0
+        ms = e0.elapsed_time(e1)
+        kt = impl.kernel_timing() if kernel_timing else None
+        if kernel_timing:
+            impl.set_option(cpra_b200.OPT_KERNEL_TIMING, 0)
+        if ws > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, launches, kt
+
+    with ClockSampler(local) as clk:
+        ms, launches, kt = timed(step_resident, a.steps, a.warmup, kernel_timing=True)
+    clocks = clk.summary()
+    ms_per_step = ms / a.steps
+    value = units_per_step * ws * a.steps / (ms / 1e3)
+
+    # ---- end to end through the public API with host buffers ----
+    x0_h = torch.empty(x0.numel(), dtype=torch.complex64).pin_memory()
+    x0_h.copy_(x0.cpu())
+    out_h = torch.empty_like(x0_h).pin_memory()
+
+    def step_e2e():
+        A.copy_(A_h, non_blocking=True)
+        S.copy_(S_h, non_blocking=True)
+        x.copy_(x0_h, non_blocking=True)
+        impl.cpra_run(x, A, S, P, B, E, IT, 0, 0.9, final_step=True, err=err)
+        out_h.copy_(x, non_blocking=True)
+
+    e2e_steps = max(1, min(a.steps, 3))
+    ms_e2e, _, _ = timed(step_e2e, e2e_steps, 1)
+    h2d = x0_h.numel() * 8 + A_h.numel() * 4 + S_h.numel() * 4
+    d2h = out_h.numel() * 8 + err.nbytes
+    e2e = {"value": units_per_step * ws * e2e_steps / (ms_e2e / 1e3), "unit": METRIC,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+           "ms_per_step": ms_e2e / e2e_steps}
+
+    # ---- roofline of the dominant kernel (fused DM iterations) ----
+    peak, peak_kind = measured_peak()
+    roof = None
+    if kt and kt[1] > 0:
+        kms, klaunches, kpi = kt
+        avg_s = kms / klaunches / 1e3
+        alg_bytes = DM_BYTES_PER_PIXEL * MN * kpi / klaunches
+        achieved = alg_bytes / avg_s / 1e9
+        tr = read_traffic(f"k_dm_{M}")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr * kpi / klaunches) if tr is not None else None,
+                "kernel": f"k_dm<{M}> (fused difference-map iterations)",
+                "avg_launch_ms": kms / klaunches, "launches": klaunches,
+                "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
+                "share_of_step": kms / ms}
+
+    result = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded ellipsoid volume, Poisson 1e7 photons)",
+        "config": workload_config(a, ws), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
+        "clocks": clocks,
+        "convergence_error_median": float(np.median(err)),
+    }
+
+    if rank == 0 and ws == 1 and not a.no_extras:
+        try:
+            result["per_op_path"] = {"value": per_op_rate(torch, d["A"], d["S"], B, M, IT), "unit": METRIC,
+                                     "impl": "torch.fft (cuFFT) + torch element-wise kernels, reference CUDA "
+                                             "backend call order, same GPU"}
+        except Exception as ex:  # the comparison must not sink the line
+            result["per_op_path"] = {"error": str(ex)[:200]}
+        try:
+            result["episode3d"] = episode_3d(torch, cpra_b200, d, dev)
+        except Exception as ex:
+            result["episode3d"] = {"error": str(ex)[:200]}
+
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        rate, sample, cores = cpu_reference_rate(d["A"], d["S"], M, IT, a.cpu_seconds, os.cpu_count() or 1)
+        result["cpu_baseline"] = None if rate is None else {
+            "value": rate, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    impl.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def episode_3d(torch, cpra_b200, d, dev, iters3d=10):
+    """3D stage of the carousel configuration: Forward2D of the retrieved
+    planes, trilinear merge of the P complex central slices into an n^3 Fourier
+    volume, then `iters3d` iterations of the benchmark's 3D step
+    (src/benchmark_mkl.cpp:164-170: Forward3D, complex DataConstraint,
+    Backward3D, SpaceConstraint).  Returns device times in ms."""
+    n = d["A"].shape[-1]
+    P = d["A"].shape[0]
+    planes = torch.rand(P * n * n, dtype=torch.complex64, device=dev)
+    ang = torch.from_numpy(d["angles"]).to(dev)
+    impl2 = cpra_b200.B200Impl(n, n, 1, P)
+    impl3 = cpra_b200.B200Impl(n, n, n, 1)
+    vol = torch.empty(n ** 3, dtype=torch.complex64, device=dev)
+    C = torch.empty_like(vol)
+    sup = torch.ones(n ** 3, device=dev)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    for rep in range(2):
+        torch.cuda.synchronize()
+        e[0].record()
+        impl2.Forward2D(planes)
+        impl2.Sync()
+        impl3.Complex2DTo3DInterpolation(planes, C, ang, n, n, P, n)
+        impl3.Sync()
+        e[1].record()
+        vol.copy_(C)
+        for _ in range(iters3d):
+            impl3.Forward3D(vol)
+            impl3.DataConstraint(vol, C, n ** 3, 1)
+            impl3.Backward3D(vol)
+            impl3.SpaceConstraint(vol, sup, n ** 3, 1)
+        impl3.Sync()
+        e[2].record()
+        torch.cuda.synchronize()
+    return {"merge_ms": e[0].elapsed_time(e[1]), "iters3d": iters3d, "loop3d_ms": e[1].elapsed_time(e[2]),
+            "total_ms": e[0].elapsed_time(e[2]), "volume": [n, n, n], "slices": P}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,298 @@
+"""Python bindings of the B200 carousel phase-retrieval backend.
+
+Mirrors the reference's operator interface ``CPRA::CpraImpl<T>``
+(include/CPRA_Impl.hpp:18-63) and its factory ``NewCpraImpl``
+(include/Impl_Factory.hpp:14-30) over the C ABI of ``libcpra_b200.so``
+(include/cpra_b200.h): same method names, same argument meaning, ``False`` for
+argument errors (the reference's ``return false``) and an exception for CUDA
+failures (the reference throws ``CPRA::cuda_error``).
+
+Data arguments are CUDA tensors (``torch``) or raw device addresses (``int``).
+There is no CPU path: importing this module fails if the CUDA library is not
+built, and every operator runs on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from pathlib import Path
+
+__all__ = [
+    "IMPL_TYPE", "CpraB200Error", "B200Impl", "NewCpraImpl", "library_path", "lib",
+    "OK", "EARG", "ECUDA", "EUNSUP", "OPT_FUSION", "OPT_SPACE_MODE", "OPT_DATA_MODE", "OPT_SEED",
+    "OPT_KERNEL_TIMING",
+]
+
+OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
+F32, F64 = 0, 1
+OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING = 1, 2, 3, 4, 5
+
+_HERE = Path(__file__).resolve().parent
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("CPRA_B200_LIB", _HERE / "libcpra_b200.so"))
+
+
+class CpraB200Error(RuntimeError):
+    """A CUDA runtime failure or an unsupported shape reported by the backend."""
+
+
+class IMPL_TYPE(enum.IntEnum):
+    """``enum IMPL_TYPE`` of include/CPRA_Impl.hpp:15 with the B200 entry added."""
+    CUDA = 0
+    MKL = 1
+    B200 = 2
+
+
+_lib = None
+
+# name -> (argtypes) ; every entry point returns int
+_SIGS = {
+    "cpra_b200_create": [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64],
+    "cpra_b200_destroy": [C.c_void_p],
+    "cpra_b200_set_option": [C.c_void_p, C.c_int, C.c_int64],
+    "cpra_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
+    "cpra_b200_alloc": [C.c_void_p, C.POINTER(C.c_void_p), C.c_uint64, C.c_int],
+    "cpra_b200_free": [C.c_void_p, C.c_void_p],
+    "cpra_b200_initialize": [C.c_void_p, C.c_void_p, C.c_uint64],
+    "cpra_b200_forward2d": [C.c_void_p, C.c_void_p],
+    "cpra_b200_backward2d": [C.c_void_p, C.c_void_p],
+    "cpra_b200_fftshift2d": [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64],
+    "cpra_b200_forward3d": [C.c_void_p, C.c_void_p],
+    "cpra_b200_backward3d": [C.c_void_p, C.c_void_p],
+    "cpra_b200_fftshift3d": [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64],
+    "cpra_b200_space_constraint": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64],
+    "cpra_b200_data_constraint_real": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64],
+    "cpra_b200_data_constraint_complex": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64],
+    "cpra_b200_merge_add": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_uint64],
+    "cpra_b200_normalization": [C.c_void_p, C.c_void_p, C.c_double, C.c_uint64],
+    "cpra_b200_real2d_to_3d": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4,
+    "cpra_b200_complex2d_to_3d": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4,
+    "cpra_b200_converge_error": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4,
+    "cpra_b200_memcpy": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64],
+    "cpra_b200_sync": [C.c_void_p],
+    "cpra_b200_dm_iterations": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                C.c_void_p, C.c_uint64, C.c_uint64, C.c_double, C.c_int],
+    "cpra_b200_cpra_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
+                           C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
+    "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+}
+
+
+def lib():
+    """Load libcpra_b200.so (fails loudly if it is not built)."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not path.exists():
+            raise ImportError(f"{path} not found: build it with "
+                              "`python carousel-phase-retrieval-algorithm_b200/build.py`")
+        L = C.CDLL(str(path))
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.cpra_b200_last_error.argtypes = []
+        L.cpra_b200_last_error.restype = C.c_char_p
+        L.cpra_b200_kernels_launched.argtypes = []
+        L.cpra_b200_kernels_launched.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def kernels_launched() -> int:
+    """Kernels launched by libcpra_b200.so in this process so far."""
+    return int(lib().cpra_b200_kernels_launched())
+
+
+def last_error() -> str:
+    return lib().cpra_b200_last_error().decode(errors="replace")
+
+
+def _addr(a) -> int:
+    """Device address of a tensor / integer address (None -> 0)."""
+    if a is None:
+        return 0
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        if hasattr(a, "is_cuda") and not a.is_cuda and a.numel() > 0:
+            raise ValueError("B200 operators take CUDA tensors (there is no CPU path)")
+        return a.data_ptr()
+    if hasattr(a, "ctypes"):  # numpy array: host pointer (ConvergeError's output only)
+        return a.ctypes.data
+    raise TypeError(f"cannot take the address of {type(a).__name__}")
+
+
+def _check(rc: int, what: str) -> bool:
+    if rc == OK:
+        return True
+    if rc == EARG:
+        return False
+    raise CpraB200Error(f"{what}: {last_error()}")
+
+
+class B200Impl:
+    """``CpraImpl<T>`` implemented by the B200 backend (``T`` = float32 or
+    float64), constructed like ``CudaImpl(m, n, l, batch_size)``
+    (include/CUDA_Impl.cuh:16-52)."""
+
+    def __init__(self, m: int, n: int, l: int, batch_size: int, dtype: str = "float32"):
+        self.dtype = dtype
+        self.dbl = dtype in ("float64", "double")
+        self.m, self.n, self.l, self.batch = int(m), int(n), int(l), int(batch_size)
+        h = C.c_void_p()
+        rc = lib().cpra_b200_create(C.byref(h), F64 if self.dbl else F32, self.m, self.n, self.l, self.batch)
+        if rc != OK:
+            raise CpraB200Error(f"cpra_b200_create: {last_error()}")
+        self._h = h
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().cpra_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_option(self, option: int, value: int) -> bool:
+        return _check(lib().cpra_b200_set_option(self._h, option, int(value)), "set_option")
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().cpra_b200_get_stream(self._h, C.byref(s)), "get_stream")
+        return s.value or 0
+
+    # -- CpraImpl<T> (include/CPRA_Impl.hpp:23-60) ----------------------------
+    def Initialize(self, flat_data_ptr, num) -> bool:
+        return _check(lib().cpra_b200_initialize(self._h, _addr(flat_data_ptr), int(num)), "Initialize")
+
+    def Forward2D(self, flat_input) -> bool:
+        return _check(lib().cpra_b200_forward2d(self._h, _addr(flat_input)), "Forward2D")
+
+    def Backward2D(self, flat_input) -> bool:
+        return _check(lib().cpra_b200_backward2d(self._h, _addr(flat_input)), "Backward2D")
+
+    def FFTShift2D(self, flat_input, M, N, Batch) -> bool:
+        return _check(lib().cpra_b200_fftshift2d(self._h, _addr(flat_input), int(M), int(N), int(Batch)),
+                      "FFTShift2D")
+
+    def Forward3D(self, flat_input) -> bool:
+        return _check(lib().cpra_b200_forward3d(self._h, _addr(flat_input)), "Forward3D")
+
+    def Backward3D(self, flat_input) -> bool:
+        return _check(lib().cpra_b200_backward3d(self._h, _addr(flat_input)), "Backward3D")
+
+    def FFTShift3D(self, flat_input, M, N, L, Batch) -> bool:
+        return _check(lib().cpra_b200_fftshift3d(self._h, _addr(flat_input), int(M), int(N), int(L), int(Batch)),
+                      "FFTShift3D")
+
+    def SpaceConstraint(self, flat_src_data, flat_constr_data, num, batch_size) -> bool:
+        return _check(lib().cpra_b200_space_constraint(self._h, _addr(flat_src_data), _addr(flat_constr_data),
+                                                       int(num), int(batch_size)), "SpaceConstraint")
+
+    def DataConstraint(self, flat_src_data, flat_constr_data, num, batch_size) -> bool:
+        """Real (modulus) or complex overload, chosen by the constraint's dtype
+        like the reference's two overloads (include/CPRA_Impl.hpp:39,41)."""
+        cplx = getattr(flat_constr_data, "is_complex", lambda: False)()
+        f = lib().cpra_b200_data_constraint_complex if cplx else lib().cpra_b200_data_constraint_real
+        return _check(f(self._h, _addr(flat_src_data), _addr(flat_constr_data), int(num), int(batch_size)),
+                      "DataConstraint")
+
+    def DataConstraintComplex(self, flat_src_data, flat_constr_data, num, batch_size) -> bool:
+        return _check(lib().cpra_b200_data_constraint_complex(self._h, _addr(flat_src_data), _addr(flat_constr_data),
+                                                              int(num), int(batch_size)), "DataConstraint")
+
+    def MergeAddData(self, flat_src, flat_dst, alpha, beta, num) -> bool:
+        return _check(lib().cpra_b200_merge_add(self._h, _addr(flat_src), _addr(flat_dst), float(alpha),
+                                                float(beta), int(num)), "MergeAddData")
+
+    def Normalization(self, flat_src, norm, num) -> bool:
+        return _check(lib().cpra_b200_normalization(self._h, _addr(flat_src), float(norm), int(num)),
+                      "Normalization")
+
+    def Real2DTo3DInterpolation(self, flat_2d_src, flat_3d_dst, angles, m, n, p, l) -> bool:
+        return _check(lib().cpra_b200_real2d_to_3d(self._h, _addr(flat_2d_src), _addr(flat_3d_dst), _addr(angles),
+                                                   int(m), int(n), int(p), int(l)), "Real2DTo3DInterpolation")
+
+    def Complex2DTo3DInterpolation(self, flat_2d_src, flat_3d_dst, angles, m, n, p, l) -> bool:
+        return _check(lib().cpra_b200_complex2d_to_3d(self._h, _addr(flat_2d_src), _addr(flat_3d_dst),
+                                                      _addr(angles), int(m), int(n), int(p), int(l)),
+                      "Complex2DTo3DInterpolation")
+
+    def ConvergeError(self, flat_old, flat_new, flat_error, m, n, l=1, batch_size=1) -> bool:
+        """``flat_error`` is host memory (numpy array of T, or a CPU tensor),
+        as include/CPRA_Impl.hpp:55 requires."""
+        return _check(lib().cpra_b200_converge_error(self._h, _addr(flat_old), _addr(flat_new),
+                                                     _host_addr(flat_error), int(m), int(n), int(l),
+                                                     int(batch_size)), "ConvergeError")
+
+    def Memcpy(self, dst, src, nbytes) -> bool:
+        return _check(lib().cpra_b200_memcpy(self._h, _addr(dst), _addr(src), int(nbytes)), "Memcpy")
+
+    def Sync(self) -> bool:
+        return _check(lib().cpra_b200_sync(self._h), "Sync")
+
+    # -- extensions -------------------------------------------------------------
+    def dm_iterations(self, x, t1, t2, A, S, batch, beta, iters, a_stride=0, s_stride=0) -> bool:
+        """``iters`` fused difference-map iterations (src/CPRA_MKL.cpp:94-110)."""
+        return _check(lib().cpra_b200_dm_iterations(self._h, _addr(x), _addr(t1), _addr(t2), _addr(A),
+                                                    int(a_stride), _addr(S), int(s_stride), int(batch),
+                                                    float(beta), int(iters)), "dm_iterations")
+
+    def cpra_run(self, x, A, S, P, batch, epi, iters, pre_iter, beta, final_step=True, err=None) -> bool:
+        """The carousel driver of src/CPRA_MKL.cpp:35-140 on resident buffers;
+        ``err`` (host array of P*batch, optional) receives the last episode's
+        convergence errors."""
+        return _check(lib().cpra_b200_cpra_run(self._h, _addr(x), _addr(A), _addr(S), int(P), int(batch), int(epi),
+                                               int(iters), int(pre_iter), float(beta), 1 if final_step else 0,
+                                               _host_addr(err) if err is not None else 0), "cpra_run")
+
+    def kernel_timing(self):
+        """(ms, launches, pattern_iterations) of the fused launches timed since
+        the last call (needs set_option(OPT_KERNEL_TIMING, 1))."""
+        ms, n, pi = C.c_double(), C.c_uint64(), C.c_uint64()
+        _check(lib().cpra_b200_kernel_timing(self._h, C.byref(ms), C.byref(n), C.byref(pi)), "kernel_timing")
+        return ms.value, n.value, pi.value
+
+    def alloc(self, nbytes: int, managed: bool = True) -> int:
+        p = C.c_void_p()
+        _check(lib().cpra_b200_alloc(self._h, C.byref(p), int(nbytes), 1 if managed else 0), "alloc")
+        return p.value or 0
+
+    def free(self, ptr: int) -> bool:
+        return _check(lib().cpra_b200_free(self._h, int(ptr)), "free")
+
+
+def _host_addr(a) -> int:
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "ctypes"):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError("ConvergeError needs a host buffer")
+
+
+def NewCpraImpl(impl_type, m, n, l, batch_size, dtype: str = "float32") -> B200Impl:
+    """Factory of include/Impl_Factory.hpp:14-30 with the B200 case; like the
+    reference it throws for a type that is not compiled in."""
+    if IMPL_TYPE(impl_type) != IMPL_TYPE.B200:
+        raise ValueError("Wrong impl type! Only the B200 backend is built in this package.")
+    return B200Impl(m, n, l, batch_size, dtype)

@@ -1,0 +1,966 @@
+// C-ABI of the B200 backend (include/cpra_b200.h): context, argument checks,
+// and the call recorder that turns the reference driver's per-operator
+// difference-map iterations into fused launches.
+//
+// Recorder.  The reference drivers issue each difference-map iteration as 12
+// operator calls (src/CPRA_MKL.cpp:94-110).  A context holds back a
+// Forward2D and the calls that follow it while they still form a prefix of
+// that pattern; when all 12 have arrived it holds the whole iteration, and
+// further identical iterations only increment a counter.  Anything else
+// (another operator, Memcpy, Sync, ConvergeError, a call that breaks the
+// pattern) first launches what is held -- the fused kernel for whole
+// iterations, the per-operator kernels for a partial prefix -- and then runs
+// normally.  Program order is preserved, so results are the per-operator
+// results; the fused kernel performs the same arithmetic.
+#include "../../include/cpra_b200.h"
+#include "cpra_internal.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace cpra_b200;
+
+namespace cpra_b200 {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int sm_count() {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+    return n;
+}
+
+}  // namespace cpra_b200
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(CPRA_B200_ECUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define CPRA_CHECK_CUDA(expr, where)                   \
+    do {                                               \
+        cudaError_t _e = (expr);                       \
+        if (_e != cudaSuccess) return cuda_fail(_e, where); \
+    } while (0)
+
+enum class OpKind { Fwd2D, Bwd2D, DataReal, Merge, Space };
+
+struct Op {
+    OpKind kind;
+    void* dst;        // operand modified in place
+    const void* src;  // constraint plane or merge source
+    uint64_t num, batch;
+    double alpha, beta;
+};
+
+struct DmPattern {
+    void *x, *t1, *t2;
+    const void *A, *S;
+    uint64_t num, batch;
+    DmCoef c;
+    bool operator==(const DmPattern& o) const {
+        return x == o.x && t1 == o.t1 && t2 == o.t2 && A == o.A && S == o.S && num == o.num && batch == o.batch &&
+               c.a1 == o.c.a1 && c.b1 == o.c.b1 && c.a2 == o.c.a2 && c.b2 == o.c.b2 && c.a3 == o.c.a3 &&
+               c.b3 == o.c.b3 && c.a4 == o.c.a4 && c.b4 == o.c.b4;
+    }
+};
+
+// exp(-2 pi i t / L) for t < L, long double, exact on the quadrant points
+template <typename T>
+std::vector<T> twiddle_table(uint64_t L) {
+    std::vector<T> w(2 * L);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (uint64_t t = 0; t < L; ++t) {
+        long double c, s;
+        if ((4 * t) % L == 0) {
+            const int q = (int)((4 * t) / L);
+            const long double cq[4] = {1.0L, 0.0L, -1.0L, 0.0L};
+            const long double sq[4] = {0.0L, 1.0L, 0.0L, -1.0L};
+            c = cq[q];
+            s = sq[q];
+        } else {
+            const long double a = 2.0L * pi * (long double)t / (long double)L;
+            c = cosl(a);
+            s = sinl(a);
+        }
+        w[2 * t] = (T)c;
+        w[2 * t + 1] = (T)(-s);
+    }
+    return w;
+}
+
+}  // namespace
+
+struct cpra_b200_ctx {
+    bool dbl = false;
+    uint64_t m = 1, n = 1, l = 1, batch = 1;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::map<uint64_t, void*> tw;  // length -> device table
+    void* work = nullptr;
+    uint64_t work_bytes = 0;
+    double* partials = nullptr;
+    double* sums = nullptr;
+    double* host_sums = nullptr;
+    uint64_t red_cap = 0;  // batch members the reduction buffers hold
+    bool fusion = true;
+    int space_mode = SPACE_THRESHOLD;
+    int data_mode = DATA_SKIP_ZERO;
+    uint64_t seed = 0x5eedull;
+    uint64_t init_calls = 0;
+    std::vector<Op> pending;
+    DmPattern held{};
+    int held_iters = 0;
+    int deferred_error = CPRA_B200_OK;
+    std::string deferred_msg;
+    // opt-in timing of fused launches
+    bool timing = false;
+    std::vector<cudaEvent_t> free_events;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timed;
+    uint64_t timed_pattern_iters = 0;
+    // driver-level buffers of cpra_b200_cpra_run: t1, t2, old (batch planes each)
+    void* drv = nullptr;
+    uint64_t drv_bytes = 0;
+    double* err_sums = nullptr;
+    double* host_err = nullptr;
+    uint64_t err_cap = 0;
+
+    size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
+    size_t csize() const { return 2 * esize(); }
+    uint64_t plane() const { return m * n; }
+    double round_t(double v) const { return dbl ? v : (double)(float)v; }
+};
+
+namespace {
+
+const void* twiddles(cpra_b200_ctx* c, uint64_t L) {
+    auto it = c->tw.find(L);
+    return it == c->tw.end() ? nullptr : it->second;
+}
+
+int ensure_twiddles(cpra_b200_ctx* c, uint64_t L) {
+    if (L < 1 || c->tw.count(L)) return CPRA_B200_OK;
+    void* d = nullptr;
+    const size_t bytes = 2 * L * c->esize();
+    CPRA_CHECK_CUDA(cudaMalloc(&d, bytes), "cudaMalloc(twiddles)");
+    cudaError_t e;
+    if (c->dbl) {
+        auto h = twiddle_table<double>(L);
+        e = cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice);
+    } else {
+        auto h = twiddle_table<float>(L);
+        e = cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(e, "cudaMemcpy(twiddles)");
+    }
+    c->tw[L] = d;
+    return CPRA_B200_OK;
+}
+
+int ensure_work(cpra_b200_ctx* c, uint64_t bytes) {
+    if (c->work_bytes >= bytes) return CPRA_B200_OK;
+    if (c->work) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_bytes = 0;
+    }
+    CPRA_CHECK_CUDA(cudaMalloc(&c->work, bytes), "cudaMalloc(work)");
+    c->work_bytes = bytes;
+    return CPRA_B200_OK;
+}
+
+int ensure_reduction(cpra_b200_ctx* c, uint64_t members) {
+    if (c->red_cap >= members) return CPRA_B200_OK;
+    if (c->partials) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(c->partials);
+        cudaFree(c->sums);
+        cudaFreeHost(c->host_sums);
+        c->partials = c->sums = c->host_sums = nullptr;
+        c->red_cap = 0;
+    }
+    CPRA_CHECK_CUDA(cudaMalloc(&c->partials, sizeof(double) * 2 * CONVERGE_BLOCKS * members), "cudaMalloc(partials)");
+    CPRA_CHECK_CUDA(cudaMalloc(&c->sums, sizeof(double) * 2 * members), "cudaMalloc(sums)");
+    CPRA_CHECK_CUDA(cudaMallocHost(&c->host_sums, sizeof(double) * 2 * members), "cudaMallocHost(sums)");
+    c->red_cap = members;
+    return CPRA_B200_OK;
+}
+
+bool overlap(const void* a, uint64_t abytes, const void* b, uint64_t bbytes) {
+    const char* pa = static_cast<const char*>(a);
+    const char* pb = static_cast<const char*>(b);
+    return pa < pb + bbytes && pb < pa + abytes;
+}
+
+// ---- per-operator execution ---------------------------------------------------
+int run_fft2d(cpra_b200_ctx* c, void* x, bool inverse) {
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "2D transform: each size must be 1 or even and at most 4096");
+    const bool pow2 = ((c->m & (c->m - 1)) == 0) && ((c->n & (c->n - 1)) == 0) && c->m <= 1024 && c->n <= 1024;
+    if (!pow2) {
+        int r = ensure_work(c, c->batch * c->plane() * c->csize());
+        if (r) return r;
+    }
+    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n) (include/MKL_Impl.hpp:40)
+    const double scale = c->dbl ? 1.0 / (double)(c->m * c->n) : (double)(1.0f / (float)(c->m * c->n));
+    CPRA_CHECK_CUDA(launch_fft2d(c->dbl, x, c->m, c->n, c->batch, inverse, scale, twiddles(c, c->m),
+                                 twiddles(c, c->n), c->work, c->stream),
+                    inverse ? "Backward2D" : "Forward2D");
+    return CPRA_B200_OK;
+}
+
+int exec_op(cpra_b200_ctx* c, const Op& op) {
+    switch (op.kind) {
+        case OpKind::Fwd2D: return run_fft2d(c, op.dst, false);
+        case OpKind::Bwd2D: return run_fft2d(c, op.dst, true);
+        case OpKind::DataReal:
+            CPRA_CHECK_CUDA(launch_data_constraint_real(c->dbl, op.dst, op.src, op.num, op.num / op.batch, c->data_mode,
+                                                        c->stream),
+                            "DataConstraint");
+            return CPRA_B200_OK;
+        case OpKind::Space:
+            CPRA_CHECK_CUDA(launch_space_constraint(c->dbl, op.dst, op.src, op.num, op.num / op.batch, c->space_mode,
+                                                    c->stream),
+                            "SpaceConstraint");
+            return CPRA_B200_OK;
+        case OpKind::Merge:
+            CPRA_CHECK_CUDA(launch_merge_add(c->dbl, op.src, op.dst, op.alpha, op.beta, op.num, c->stream),
+                            "MergeAddData");
+            return CPRA_B200_OK;
+    }
+    return fail(CPRA_B200_EARG, "unknown operator");
+}
+
+int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters) {
+    DmArgs a;
+    a.x = p.x;
+    a.t1 = p.t1;
+    a.t2 = p.t2;
+    a.A = p.A;
+    a.a_stride = 0;
+    a.S = p.S;
+    a.s_stride = 0;
+    a.M = c->m;
+    a.N = c->n;
+    a.batch = c->batch;
+    a.iters = iters;
+    a.space_mode = c->space_mode;
+    a.data_mode = c->data_mode;
+    a.c = p.c;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (c->timing) {
+        for (cudaEvent_t& e : ev) {
+            if (!c->free_events.empty()) {
+                e = c->free_events.back();
+                c->free_events.pop_back();
+            } else {
+                CPRA_CHECK_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+            }
+        }
+        CPRA_CHECK_CUDA(cudaEventRecord(ev[0], c->stream), "cudaEventRecord");
+    }
+    CPRA_CHECK_CUDA(launch_dm_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "fused difference-map iteration");
+    if (c->timing) {
+        CPRA_CHECK_CUDA(cudaEventRecord(ev[1], c->stream), "cudaEventRecord");
+        c->timed.emplace_back(ev[0], ev[1]);
+        c->timed_pattern_iters += c->batch * (uint64_t)iters;
+    }
+    return CPRA_B200_OK;
+}
+
+// `iters` iterations of pattern p: fused when the shape allows, else per call
+int dm_any(cpra_b200_ctx* c, const DmPattern& p, int iters) {
+    if (iters <= 0) return CPRA_B200_OK;
+    if (dm_fused_supported(c->dbl, c->m, c->n)) return launch_fused(c, p, iters);
+    const uint64_t num = p.num;
+    const uint64_t B = p.batch;
+    for (int i = 0; i < iters; ++i) {
+        const Op seq[12] = {
+            {OpKind::Fwd2D, p.t1, nullptr, 0, 0, 0, 0},   {OpKind::DataReal, p.t1, p.A, num, B, 0, 0},
+            {OpKind::Bwd2D, p.t1, nullptr, 0, 0, 0, 0},   {OpKind::Merge, p.t1, p.x, num, 1, p.c.a1, p.c.b1},
+            {OpKind::Space, p.t1, p.S, num, B, 0, 0},     {OpKind::Space, p.t2, p.S, num, B, 0, 0},
+            {OpKind::Merge, p.t2, p.x, num, 1, p.c.a2, p.c.b2}, {OpKind::Fwd2D, p.t2, nullptr, 0, 0, 0, 0},
+            {OpKind::DataReal, p.t2, p.A, num, B, 0, 0},  {OpKind::Bwd2D, p.t2, nullptr, 0, 0, 0, 0},
+            {OpKind::Merge, p.x, p.t1, num, 1, p.c.a3, p.c.b3}, {OpKind::Merge, p.x, p.t2, num, 1, p.c.a4, p.c.b4}};
+        for (const Op& op : seq) {
+            int r = exec_op(c, op);
+            if (r) return r;
+        }
+    }
+    return CPRA_B200_OK;
+}
+
+// launch everything held, in program order
+int flush(cpra_b200_ctx* c) {
+    int rc = CPRA_B200_OK;
+    if (c->held_iters > 0) {
+        rc = launch_fused(c, c->held, c->held_iters);
+        c->held_iters = 0;
+    }
+    std::vector<Op> ops;
+    ops.swap(c->pending);
+    for (const Op& op : ops) {
+        int r = exec_op(c, op);
+        if (r && !rc) rc = r;
+    }
+    if (rc && !c->deferred_error) {
+        c->deferred_error = rc;
+        c->deferred_msg = g_last_error;
+    }
+    return rc;
+}
+
+// surface an error from a launch that was deferred by the recorder
+int take_deferred(cpra_b200_ctx* c) {
+    if (!c->deferred_error) return CPRA_B200_OK;
+    int rc = c->deferred_error;
+    c->deferred_error = CPRA_B200_OK;
+    return fail(rc, "deferred launch failed: " + c->deferred_msg);
+}
+
+bool fusable_shape(const cpra_b200_ctx* c) { return c->fusion && dm_fused_supported(c->dbl, c->m, c->n); }
+
+// Does `op` extend the pending prefix (of length k) of the pattern?
+bool extends(const cpra_b200_ctx* c, const Op& op) {
+    const std::vector<Op>& P = c->pending;
+    const size_t k = P.size();
+    const uint64_t num = c->plane() * c->batch;
+    const uint64_t cbytes = num * c->csize();
+    const uint64_t rbytes = c->plane() * c->esize();
+    auto T1 = [&]() { return P[0].dst; };
+    auto is_ew = [&](OpKind kind) {
+        return op.kind == kind && op.num == num && op.batch == c->batch && op.num % op.batch == 0 &&
+               op.num / op.batch == c->plane();
+    };
+    switch (k) {
+        case 1:  // DataConstraint(t1, A)
+            return is_ew(OpKind::DataReal) && op.dst == T1() && !overlap(op.src, rbytes, T1(), cbytes);
+        case 2:  // Backward2D(t1)
+            return op.kind == OpKind::Bwd2D && op.dst == T1();
+        case 3:  // MergeAddData(x, t1, a1, b1)
+            return op.kind == OpKind::Merge && op.num == num && op.dst == T1() && !overlap(op.src, cbytes, T1(), cbytes) &&
+                   !overlap(op.src, cbytes, P[1].src, rbytes);
+        case 4:  // SpaceConstraint(t1, S)
+            return is_ew(OpKind::Space) && op.dst == T1() && !overlap(op.src, rbytes, T1(), cbytes) &&
+                   !overlap(op.src, rbytes, P[3].src, cbytes);
+        case 5: {  // SpaceConstraint(t2, S)
+            const void* X = P[3].src;
+            return is_ew(OpKind::Space) && op.src == P[4].src && !overlap(op.dst, cbytes, T1(), cbytes) &&
+                   !overlap(op.dst, cbytes, X, cbytes) && !overlap(op.dst, cbytes, P[1].src, rbytes) &&
+                   !overlap(op.dst, cbytes, P[4].src, rbytes);
+        }
+        case 6:  // MergeAddData(x, t2, a2, b2)
+            return op.kind == OpKind::Merge && op.num == num && op.src == P[3].src && op.dst == P[5].dst;
+        case 7:  // Forward2D(t2)
+            return op.kind == OpKind::Fwd2D && op.dst == P[5].dst;
+        case 8:  // DataConstraint(t2, A)
+            return is_ew(OpKind::DataReal) && op.dst == P[5].dst && op.src == P[1].src;
+        case 9:  // Backward2D(t2)
+            return op.kind == OpKind::Bwd2D && op.dst == P[5].dst;
+        case 10:  // MergeAddData(t1, x, a3, b3)
+            return op.kind == OpKind::Merge && op.num == num && op.src == T1() && op.dst == P[3].src;
+        case 11:  // MergeAddData(t2, x, a4, b4)
+            return op.kind == OpKind::Merge && op.num == num && op.src == P[5].dst && op.dst == P[3].src;
+        default: return false;
+    }
+}
+
+DmPattern pattern_of(const std::vector<Op>& P) {
+    DmPattern d;
+    d.t1 = P[0].dst;
+    d.A = P[1].src;
+    d.x = const_cast<void*>(P[3].src);
+    d.S = P[4].src;
+    d.t2 = P[5].dst;
+    d.num = P[1].num;
+    d.batch = P[1].batch;
+    d.c = {P[3].alpha, P[3].beta, P[6].alpha, P[6].beta, P[10].alpha, P[10].beta, P[11].alpha, P[11].beta};
+    return d;
+}
+
+// Entry for every operator that the recorder may hold.
+int submit(cpra_b200_ctx* c, const Op& op) {
+    if (!fusable_shape(c)) {
+        int r = flush(c);
+        if (r) return take_deferred(c);
+        return exec_op(c, op);
+    }
+    if (c->pending.empty()) {
+        if (op.kind == OpKind::Fwd2D) {
+            if (c->held_iters > 0 && op.dst != c->held.t1) {
+                int r = flush(c);
+                if (r) return take_deferred(c);
+            }
+            c->pending.push_back(op);
+            return take_deferred(c);
+        }
+        int r = flush(c);
+        if (r) return take_deferred(c);
+        return exec_op(c, op);
+    }
+    if (extends(c, op)) {
+        c->pending.push_back(op);
+        if (c->pending.size() == 12) {
+            DmPattern p = pattern_of(c->pending);
+            c->pending.clear();
+            if (c->held_iters > 0 && p == c->held) {
+                ++c->held_iters;
+            } else {
+                if (c->held_iters > 0) {
+                    int r = launch_fused(c, c->held, c->held_iters);
+                    c->held_iters = 0;
+                    if (r) return r;
+                }
+                c->held = p;
+                c->held_iters = 1;
+            }
+        }
+        return take_deferred(c);
+    }
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    return submit(c, op);
+}
+
+int check_ctx(cpra_b200_ctx* c) {
+    if (!c) return fail(CPRA_B200_EARG, "null context");
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    return CPRA_B200_OK;
+}
+
+#define CTX_OR_RETURN(c)            \
+    do {                            \
+        int _r = check_ctx(c);      \
+        if (_r) return _r;          \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+const char* cpra_b200_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t cpra_b200_kernels_launched(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int cpra_b200_create(cpra_b200_ctx** out, int dtype, uint64_t m, uint64_t n, uint64_t l, uint64_t batch_size) {
+    if (!out) return fail(CPRA_B200_EARG, "null output pointer");
+    *out = nullptr;
+    if (dtype != CPRA_B200_F32 && dtype != CPRA_B200_F64) return fail(CPRA_B200_EARG, "dtype must be F32 or F64");
+    if (m == 0 || n == 0 || l == 0 || batch_size == 0) return fail(CPRA_B200_EARG, "sizes must be positive");
+    auto* c = new cpra_b200_ctx();
+    c->dbl = (dtype == CPRA_B200_F64);
+    c->m = m;
+    c->n = n;
+    c->l = l;
+    c->batch = batch_size;
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e == cudaSuccess) e = cudaStreamCreate(&c->stream);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "cudaStreamCreate");
+    }
+    for (uint64_t L : {m, n, l}) {
+        if (L <= 4096) {
+            int r = ensure_twiddles(c, L);
+            if (r) {
+                cpra_b200_destroy(c);
+                return r;
+            }
+        }
+    }
+    *out = c;
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_destroy(cpra_b200_ctx* c) {
+    if (!c) return CPRA_B200_OK;
+    cudaSetDevice(c->device);
+    int rc = flush(c);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->tw) cudaFree(kv.second);
+    if (c->work) cudaFree(c->work);
+    if (c->partials) cudaFree(c->partials);
+    if (c->sums) cudaFree(c->sums);
+    if (c->host_sums) cudaFreeHost(c->host_sums);
+    if (c->drv) cudaFree(c->drv);
+    if (c->err_sums) cudaFree(c->err_sums);
+    if (c->host_err) cudaFreeHost(c->host_err);
+    for (auto& pr : c->timed) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (cudaEvent_t e : c->free_events) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return rc;
+}
+
+int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
+    CTX_OR_RETURN(c);
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    switch (option) {
+        case CPRA_B200_OPT_FUSION: c->fusion = value != 0; break;
+        case CPRA_B200_OPT_SPACE_MODE:
+            if (value != SPACE_THRESHOLD && value != SPACE_POSITIVE_SCALED) return fail(CPRA_B200_EARG, "space mode");
+            c->space_mode = (int)value;
+            break;
+        case CPRA_B200_OPT_DATA_MODE:
+            if (value != DATA_SKIP_ZERO && value != DATA_ALWAYS) return fail(CPRA_B200_EARG, "data mode");
+            c->data_mode = (int)value;
+            break;
+        case CPRA_B200_OPT_SEED: c->seed = (uint64_t)value; c->init_calls = 0; break;
+        case CPRA_B200_OPT_KERNEL_TIMING: c->timing = value != 0; break;
+        default: return fail(CPRA_B200_EARG, "unknown option");
+    }
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_get_stream(cpra_b200_ctx* c, void** stream) {
+    CTX_OR_RETURN(c);
+    if (!stream) return fail(CPRA_B200_EARG, "null output pointer");
+    *stream = (void*)c->stream;
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_alloc(cpra_b200_ctx* c, void** out, uint64_t bytes, int managed) {
+    CTX_OR_RETURN(c);
+    if (!out) return fail(CPRA_B200_EARG, "null output pointer");
+    *out = nullptr;
+    if (bytes == 0) return fail(CPRA_B200_EARG, "zero-byte allocation");
+    if (managed)
+        CPRA_CHECK_CUDA(cudaMallocManaged(out, bytes, cudaMemAttachGlobal), "cudaMallocManaged");
+    else
+        CPRA_CHECK_CUDA(cudaMalloc(out, bytes), "cudaMalloc");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_free(cpra_b200_ctx* c, void* ptr) {
+    CTX_OR_RETURN(c);
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    if (ptr) CPRA_CHECK_CUDA(cudaFree(ptr), "cudaFree");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_initialize(cpra_b200_ctx* c, void* flat, uint64_t num) {
+    CTX_OR_RETURN(c);
+    if (num < 1) return fail(CPRA_B200_EARG, "Initialize: num < 1");  // MKL_Impl.inl:11
+    if (!flat) return fail(CPRA_B200_EARG, "Initialize: null pointer");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_uniform(c->dbl, flat, num, c->seed, c->init_calls++, c->stream), "Initialize");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_forward2d(cpra_b200_ctx* c, void* x) {
+    CTX_OR_RETURN(c);
+    if (!x) return fail(CPRA_B200_EARG, "Forward2D: null pointer");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "Forward2D: each size must be 1 or even and at most 4096");
+    return submit(c, Op{OpKind::Fwd2D, x, nullptr, 0, 0, 0, 0});
+}
+
+int cpra_b200_backward2d(cpra_b200_ctx* c, void* x) {
+    CTX_OR_RETURN(c);
+    if (!x) return fail(CPRA_B200_EARG, "Backward2D: null pointer");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "Backward2D: each size must be 1 or even and at most 4096");
+    return submit(c, Op{OpKind::Bwd2D, x, nullptr, 0, 0, 0, 0});
+}
+
+static bool shift_size_ok(uint64_t v) { return v == 1 || (v % 2) == 0; }
+
+int cpra_b200_fftshift2d(cpra_b200_ctx* c, void* x, uint64_t M, uint64_t N, uint64_t B) {
+    CTX_OR_RETURN(c);
+    if (!x) return fail(CPRA_B200_EARG, "FFTShift2D: null pointer");
+    if (!shift_size_ok(M) || !shift_size_ok(N))
+        return fail(CPRA_B200_EARG, "FFTShift2D: sizes must be even (or 1); the reference swap is a shift only then");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_fftshift2d(c->dbl, x, M, N, B, c->stream), "FFTShift2D");
+    return CPRA_B200_OK;
+}
+
+static int run_fft3d(cpra_b200_ctx* c, void* x, bool inverse) {
+    if (!x) return fail(CPRA_B200_EARG, inverse ? "Backward3D: null pointer" : "Forward3D: null pointer");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
+        return fail(CPRA_B200_EUNSUP, "3D transform: each size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    auto p2 = [](uint64_t v) { return (v & (v - 1)) == 0 && v <= 1024; };
+    if (!(p2(c->m) && p2(c->n) && p2(c->l))) {
+        r = ensure_work(c, c->batch * c->m * c->n * c->l * c->csize());
+        if (r) return r;
+    }
+    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
+    const uint64_t vol = c->m * c->n * c->l;
+    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
+    CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, inverse, scale, twiddles(c, c->m),
+                                 twiddles(c, c->n), twiddles(c, c->l), c->work, c->stream),
+                    inverse ? "Backward3D" : "Forward3D");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_forward3d(cpra_b200_ctx* c, void* x) {
+    CTX_OR_RETURN(c);
+    return run_fft3d(c, x, false);
+}
+
+int cpra_b200_backward3d(cpra_b200_ctx* c, void* x) {
+    CTX_OR_RETURN(c);
+    return run_fft3d(c, x, true);
+}
+
+int cpra_b200_fftshift3d(cpra_b200_ctx* c, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t B) {
+    CTX_OR_RETURN(c);
+    if (!x) return fail(CPRA_B200_EARG, "FFTShift3D: null pointer");
+    if (!shift_size_ok(M) || !shift_size_ok(N) || !shift_size_ok(L))
+        return fail(CPRA_B200_EARG, "FFTShift3D: sizes must be even (or 1)");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_fftshift3d(c->dbl, x, M, N, L, B, c->stream), "FFTShift3D");
+    return CPRA_B200_OK;
+}
+
+static int ew_args(const char* what, const void* x, const void* k, uint64_t num, uint64_t batch) {
+    // MKL_Impl.inl:73,89,112: num == 0 or batch_size == 0 -> false
+    if (num == 0 || batch == 0) return fail(CPRA_B200_EARG, std::string(what) + ": num and batch_size must be positive");
+    if (num / batch == 0) return fail(CPRA_B200_EARG, std::string(what) + ": num < batch_size (empty plane)");
+    if (!x || !k) return fail(CPRA_B200_EARG, std::string(what) + ": null pointer");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_space_constraint(cpra_b200_ctx* c, void* x, const void* s, uint64_t num, uint64_t batch) {
+    CTX_OR_RETURN(c);
+    int r = ew_args("SpaceConstraint", x, s, num, batch);
+    if (r) return r;
+    return submit(c, Op{OpKind::Space, x, s, num, batch, 0, 0});
+}
+
+int cpra_b200_data_constraint_real(cpra_b200_ctx* c, void* x, const void* a, uint64_t num, uint64_t batch) {
+    CTX_OR_RETURN(c);
+    int r = ew_args("DataConstraint", x, a, num, batch);
+    if (r) return r;
+    return submit(c, Op{OpKind::DataReal, x, a, num, batch, 0, 0});
+}
+
+int cpra_b200_data_constraint_complex(cpra_b200_ctx* c, void* x, const void* k, uint64_t num, uint64_t batch) {
+    CTX_OR_RETURN(c);
+    int r = ew_args("DataConstraint(complex)", x, k, num, batch);
+    if (r) return r;
+    r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_data_constraint_complex(c->dbl, x, k, num, num / batch, c->stream), "DataConstraint(complex)");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_merge_add(cpra_b200_ctx* c, const void* src, void* dst, double alpha, double beta, uint64_t num) {
+    CTX_OR_RETURN(c);
+    const double a = c->round_t(alpha), b = c->round_t(beta);
+    // MKL_Impl.inl:34: alpha == 0 or num == 0 -> false
+    if (a == 0.0 || num == 0) return fail(CPRA_B200_EARG, "MergeAddData: alpha == 0 or num == 0");
+    if (!src || !dst) return fail(CPRA_B200_EARG, "MergeAddData: null pointer");
+    return submit(c, Op{OpKind::Merge, dst, src, num, 1, a, b});
+}
+
+int cpra_b200_normalization(cpra_b200_ctx* c, void* x, double norm, uint64_t num) {
+    CTX_OR_RETURN(c);
+    const double nt = c->round_t(norm);
+    // MKL_Impl.inl:55: norm == 0 or num == 0 -> false
+    if (nt == 0.0 || num == 0) return fail(CPRA_B200_EARG, "Normalization: norm == 0 or num == 0");
+    if (!x) return fail(CPRA_B200_EARG, "Normalization: null pointer");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    // MKL_Impl.inl:57-58: scal by T(1.0 / norm)
+    CPRA_CHECK_CUDA(launch_scale(c->dbl, x, c->round_t(1.0 / nt), num, c->stream), "Normalization");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_real2d_to_3d(cpra_b200_ctx* c, const void* src, void* dst, const void* angles, uint64_t m, uint64_t n,
+                           uint64_t p, uint64_t l) {
+    CTX_OR_RETURN(c);
+    if (!src || !dst || !angles) return fail(CPRA_B200_EARG, "Real2DTo3DInterpolation: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "Real2DTo3DInterpolation: zero size");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_real2d_to_3d(c->dbl, src, dst, angles, m, n, p, l, c->stream), "Real2DTo3DInterpolation");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_complex2d_to_3d(cpra_b200_ctx* c, const void* src, void* dst, const void* angles, uint64_t m,
+                              uint64_t n, uint64_t p, uint64_t l) {
+    CTX_OR_RETURN(c);
+    if (!src || !dst || !angles) return fail(CPRA_B200_EARG, "Complex2DTo3DInterpolation: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "Complex2DTo3DInterpolation: zero size");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_complex2d_to_3d(c->dbl, src, dst, angles, m, n, p, l, c->stream),
+                    "Complex2DTo3DInterpolation");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_converge_error(cpra_b200_ctx* c, void* old_, const void* new_, void* err_host, uint64_t m, uint64_t n,
+                             uint64_t l, uint64_t batch) {
+    CTX_OR_RETURN(c);
+    if (!old_ || !new_ || !err_host) return fail(CPRA_B200_EARG, "ConvergeError: null pointer");
+    if (m == 0 || n == 0 || l == 0 || batch == 0) return fail(CPRA_B200_EARG, "ConvergeError: zero size");
+    if (batch > 65535) return fail(CPRA_B200_EUNSUP, "ConvergeError: batch_size above 65535");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    r = ensure_reduction(c, batch);
+    if (r) return r;
+    // CUDA_Impl.inl:155: old <- 1*new + (-1)*old
+    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, new_, old_, 1.0, -1.0, m * n * l * batch, c->stream), "ConvergeError");
+    CPRA_CHECK_CUDA(launch_norm_pairs(c->dbl, old_, new_, m * n, m * n * l, batch, c->partials, c->sums, c->stream),
+                    "ConvergeError");
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost, c->stream),
+                    "ConvergeError");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "ConvergeError");
+    for (uint64_t i = 0; i < batch; ++i) {
+        const double e = std::sqrt(c->host_sums[2 * i]) / std::sqrt(c->host_sums[2 * i + 1]);
+        if (c->dbl)
+            static_cast<double*>(err_host)[i] = e;
+        else
+            static_cast<float*>(err_host)[i] = (float)e;
+    }
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_memcpy(cpra_b200_ctx* c, void* dst, const void* src, uint64_t bytes) {
+    CTX_OR_RETURN(c);
+    if ((!dst || !src) && bytes) return fail(CPRA_B200_EARG, "Memcpy: null pointer");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    if (bytes) CPRA_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream), "Memcpy");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_sync(cpra_b200_ctx* c) {
+    CTX_OR_RETURN(c);
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "Sync");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_dm_iterations(cpra_b200_ctx* c, void* x, void* t1, void* t2, const void* A, uint64_t a_stride,
+                            const void* S, uint64_t s_stride, uint64_t batch, double beta, int iters) {
+    CTX_OR_RETURN(c);
+    if (!x || !t1 || !t2 || !A || !S) return fail(CPRA_B200_EARG, "dm_iterations: null pointer");
+    if (batch == 0 || iters < 0) return fail(CPRA_B200_EARG, "dm_iterations: batch must be positive, iters >= 0");
+    const double b = c->round_t(beta);
+    if (b == 0.0) return fail(CPRA_B200_EARG, "dm_iterations: beta == 0");
+    if (!dm_fused_supported(c->dbl, c->m, c->n))
+        return fail(CPRA_B200_EUNSUP, "dm_iterations: fused path needs float and square 32, 64 or 128 planes");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    if (iters == 0) return CPRA_B200_OK;
+    // src/CPRA_MKL.cpp:98,103,109,110: coefficients in double from a T beta, passed as T
+    DmArgs a;
+    a.x = x;
+    a.t1 = t1;
+    a.t2 = t2;
+    a.A = A;
+    a.a_stride = a_stride;
+    a.S = S;
+    a.s_stride = s_stride;
+    a.M = c->m;
+    a.N = c->n;
+    a.batch = batch;
+    a.iters = iters;
+    a.space_mode = c->space_mode;
+    a.data_mode = c->data_mode;
+    a.c = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
+           c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
+    CPRA_CHECK_CUDA(launch_dm_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "dm_iterations");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, uint64_t* pattern_iters) {
+    CTX_OR_RETURN(c);
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "kernel_timing");
+    double total = 0.0;
+    for (auto& pr : c->timed) {
+        float t = 0.0f;
+        CPRA_CHECK_CUDA(cudaEventElapsedTime(&t, pr.first, pr.second), "cudaEventElapsedTime");
+        total += t;
+        c->free_events.push_back(pr.first);
+        c->free_events.push_back(pr.second);
+    }
+    if (ms) *ms = total;
+    if (launches) *launches = c->timed.size();
+    if (pattern_iters) *pattern_iters = c->timed_pattern_iters;
+    c->timed.clear();
+    c->timed_pattern_iters = 0;
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
+                       int iters, int pre_iter, double beta, int final_step, void* err_host) {
+    CTX_OR_RETURN(c);
+    if (!x || !A || !S) return fail(CPRA_B200_EARG, "cpra_run: null pointer");
+    if (P < 2) return fail(CPRA_B200_EARG, "cpra_run: P >= 2 (the carousel mix reads angles p-1 and p+1)");
+    if (batch != c->batch) return fail(CPRA_B200_EARG, "cpra_run: batch must equal the context's batch_size");
+    if (epi < 0 || iters < 0 || pre_iter < 0) return fail(CPRA_B200_EARG, "cpra_run: negative count");
+    if (err_host && epi > 0 && iters < 1) return fail(CPRA_B200_EARG, "cpra_run: the error step needs iters >= 1");
+    const double b = c->round_t(beta);
+    if (b == 0.0) return fail(CPRA_B200_EARG, "cpra_run: beta == 0");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "cpra_run: each plane size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t MN = c->plane(), MNB = MN * batch;
+    const uint64_t cb = MNB * c->csize();
+    if (c->drv_bytes < 3 * cb) {
+        if (c->drv) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(c->drv);
+            c->drv = nullptr;
+            c->drv_bytes = 0;
+        }
+        CPRA_CHECK_CUDA(cudaMalloc(&c->drv, 3 * cb), "cudaMalloc(driver buffers)");
+        c->drv_bytes = 3 * cb;
+    }
+    const bool want_err = err_host && epi > 0;
+    if (want_err) {
+        r = ensure_reduction(c, batch);
+        if (r) return r;
+        if (c->err_cap < P * batch) {
+            if (c->err_sums) {
+                cudaStreamSynchronize(c->stream);
+                cudaFree(c->err_sums);
+                cudaFreeHost(c->host_err);
+                c->err_sums = c->host_err = nullptr;
+                c->err_cap = 0;
+            }
+            CPRA_CHECK_CUDA(cudaMalloc(&c->err_sums, sizeof(double) * 2 * P * batch), "cudaMalloc(errors)");
+            CPRA_CHECK_CUDA(cudaMallocHost(&c->host_err, sizeof(double) * 2 * P * batch), "cudaMallocHost(errors)");
+            c->err_cap = P * batch;
+        }
+    }
+    char* base = static_cast<char*>(x);
+    char* t1 = static_cast<char*>(c->drv);
+    char* t2 = t1 + cb;
+    char* old = t2 + cb;
+    const char* Ab = static_cast<const char*>(A);
+    const char* Sb = static_cast<const char*>(S);
+    const uint64_t rb = MN * c->esize();
+    auto xp = [&](uint64_t p) { return static_cast<void*>(base + cb * p); };
+    // src/CPRA_MKL.cpp:98,103,109,110: coefficients in double from a T beta, passed as T
+    const DmCoef coef = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
+                         c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
+    auto pattern = [&](uint64_t p, uint64_t cp) {
+        DmPattern d;
+        d.x = xp(p);
+        d.t1 = t1;
+        d.t2 = t2;
+        d.A = Ab + rb * cp;
+        d.S = Sb + rb * cp;
+        d.num = MNB;
+        d.batch = batch;
+        d.c = coef;
+        return d;
+    };
+    auto copy = [&](void* dst, const void* src) {
+        return cudaMemcpyAsync(dst, src, cb, cudaMemcpyDeviceToDevice, c->stream);
+    };
+    // Step A (:35-55): pre-reconstruction of angle 0 with the first constraint planes
+    if (pre_iter > 0) {
+        CPRA_CHECK_CUDA(copy(t1, xp(0)), "cpra_run");
+        CPRA_CHECK_CUDA(copy(t2, xp(0)), "cpra_run");
+        if ((r = dm_any(c, pattern(0, 0), pre_iter))) return r;
+    }
+    // Step B (:59-124)
+    for (int e = 0; e < epi; ++e) {
+        for (uint64_t p = 0; p < P; ++p) {
+            if (p == P - 1) {
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
+            } else if (p == 0) {
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
+            } else {
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.0, MNB, c->stream), "cpra_run");
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 1.0, MNB, c->stream), "cpra_run");
+            }
+            CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+            CPRA_CHECK_CUDA(copy(t2, xp(p)), "cpra_run");
+            const DmPattern pat = pattern(p, p);
+            const bool err_here = want_err && e == epi - 1;
+            if (!err_here) {
+                if ((r = dm_any(c, pat, iters))) return r;
+                continue;
+            }
+            if ((r = dm_any(c, pat, iters - 1))) return r;
+            CPRA_CHECK_CUDA(copy(old, xp(p)), "cpra_run");
+            if ((r = dm_any(c, pat, 1))) return r;
+            CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+            if ((r = run_fft2d(c, old, false))) return r;
+            if ((r = run_fft2d(c, t1, false))) return r;
+            // ConvergeError (CUDA_Impl.inl:145-172): old <- t1 - old, ||old_i|| / ||t1_i||
+            CPRA_CHECK_CUDA(launch_merge_add(c->dbl, t1, old, 1.0, -1.0, MNB, c->stream), "cpra_run");
+            CPRA_CHECK_CUDA(launch_norm_pairs(c->dbl, old, t1, MN, MN, batch, c->partials, c->err_sums + 2 * batch * p,
+                                              c->stream),
+                            "cpra_run");
+        }
+    }
+    // final projection (:126-140)
+    if (final_step) {
+        for (uint64_t p = 0; p < P; ++p) {
+            const DmPattern pat = pattern(p, p);
+            CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+            const Op seq[5] = {{OpKind::Fwd2D, t1, nullptr, 0, 0, 0, 0},
+                               {OpKind::DataReal, t1, pat.A, MNB, batch, 0, 0},
+                               {OpKind::Bwd2D, t1, nullptr, 0, 0, 0, 0},
+                               {OpKind::Merge, t1, xp(p), MNB, 1, coef.a1, coef.b1},
+                               {OpKind::Space, t1, pat.S, MNB, batch, 0, 0}};
+            for (const Op& op : seq)
+                if ((r = exec_op(c, op))) return r;
+            CPRA_CHECK_CUDA(copy(xp(p), t1), "cpra_run");
+        }
+    }
+    if (want_err) {
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_err, c->err_sums, sizeof(double) * 2 * P * batch,
+                                        cudaMemcpyDeviceToHost, c->stream),
+                        "cpra_run");
+        CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "cpra_run");
+        for (uint64_t i = 0; i < P * batch; ++i) {
+            const double v = std::sqrt(c->host_err[2 * i]) / std::sqrt(c->host_err[2 * i + 1]);
+            if (c->dbl)
+                static_cast<double*>(err_host)[i] = v;
+            else
+                static_cast<float*>(err_host)[i] = (float)v;
+        }
+    }
+    return CPRA_B200_OK;
+}
+
+}  // extern "C"

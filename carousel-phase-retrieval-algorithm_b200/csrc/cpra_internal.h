@@ -1,0 +1,89 @@
+// Host-side interface between the C-ABI layer (capi.cu) and the kernel
+// launchers (kernels_*.cu).  Every launcher enqueues on the given stream and
+// returns a cudaError_t from cudaGetLastError(); argument validation happens in
+// the C-ABI layer before any launcher is called.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cpra_b200 {
+
+// Process-wide count of kernels this library has launched (every launcher
+// calls count_launches after its launches; read by cpra_b200_kernels_launched).
+void count_launches(uint64_t n = 1);
+
+// ---- transforms (kernels_fft.cu) ---------------------------------------
+// Shifted 2D transform of `batch` MxN planes in place:
+//   forward : x <- s * D (.) FFT(D (.) x)
+//   inverse : x <- D (.) (IFFT(s * D (.) x) * scale)
+// with D = (-1)^(row+col) and s = (-1)^(M/2 + N/2), which equals
+// fftshift o DFT o fftshift for even M, N.  `tw_m`, `tw_n` are device tables
+// exp(-2 pi i t / M) and exp(-2 pi i t / N) in the element precision.
+// `work` is a device buffer of at least batch*M*N elements, used only by the
+// non-power-of-two path.
+cudaError_t launch_fft2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t batch, bool inverse, double scale,
+                         const void* tw_m, const void* tw_n, void* work, cudaStream_t st);
+// Shifted 3D transform of `batch` volumes laid out [L][M][N] (N fastest).
+cudaError_t launch_fft3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch, bool inverse,
+                         double scale, const void* tw_m, const void* tw_n, const void* tw_l, void* work,
+                         cudaStream_t st);
+// True when the 2D shape runs as one CTA per plane (one HBM round trip).
+bool fft2d_single_cta(bool dbl, uint64_t M, uint64_t N);
+// True when a 1D length is supported at all by the transforms.
+bool fft_length_supported(uint64_t L);
+
+// ---- element-wise operators (kernels_ew.cu) ------------------------------
+enum SpaceMode : int { SPACE_THRESHOLD = 0, SPACE_POSITIVE_SCALED = 1 };
+enum DataMode : int { DATA_SKIP_ZERO = 0, DATA_ALWAYS = 1 };
+
+cudaError_t launch_space_constraint(bool dbl, void* x, const void* s, uint64_t num, uint64_t plane, int mode,
+                                    cudaStream_t st);
+cudaError_t launch_data_constraint_real(bool dbl, void* x, const void* a, uint64_t num, uint64_t plane, int mode,
+                                        cudaStream_t st);
+cudaError_t launch_data_constraint_complex(bool dbl, void* x, const void* c, uint64_t num, uint64_t plane,
+                                           cudaStream_t st);
+cudaError_t launch_merge_add(bool dbl, const void* src, void* dst, double alpha, double beta, uint64_t num,
+                             cudaStream_t st);
+cudaError_t launch_scale(bool dbl, void* x, double factor, uint64_t num, cudaStream_t st);
+cudaError_t launch_fftshift2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t batch, cudaStream_t st);
+cudaError_t launch_fftshift3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch,
+                              cudaStream_t st);
+cudaError_t launch_uniform(bool dbl, void* x, uint64_t num, uint64_t seed, uint64_t stream_id, cudaStream_t st);
+// ||old_i|| and ||new_i|| over `span` elements at stride `stride` for i < batch,
+// accumulated in double into sums[2*batch] (deterministic two-level reduction
+// through `partials`, >= batch * CONVERGE_BLOCKS * 2 doubles).
+constexpr int CONVERGE_BLOCKS = 64;
+cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t span, uint64_t stride,
+                              uint64_t batch, double* partials, double* sums, cudaStream_t st);
+cudaError_t launch_real2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m, uint64_t n,
+                                uint64_t p, uint64_t l, cudaStream_t st);
+cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m,
+                                   uint64_t n, uint64_t p, uint64_t l, cudaStream_t st);
+
+// ---- fused difference-map iterations (kernels_dm.cu) ---------------------
+// Coefficients of the four MergeAddData calls of one iteration
+// (dst = alpha*src + beta*dst), in call order.
+struct DmCoef {
+    double a1, b1;  // x  -> t1
+    double a2, b2;  // x  -> t2
+    double a3, b3;  // t1 -> x
+    double a4, b4;  // t2 -> x
+};
+struct DmArgs {
+    void* x;
+    void* t1;
+    void* t2;
+    const void* A;       // modulus constraint plane(s)
+    uint64_t a_stride;   // elements between consecutive patterns' planes (0: shared)
+    const void* S;       // support plane(s)
+    uint64_t s_stride;
+    uint64_t M, N, batch;
+    int iters;
+    int space_mode;
+    int data_mode;
+    DmCoef c;
+};
+bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
+cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
+
+}  // namespace cpra_b200

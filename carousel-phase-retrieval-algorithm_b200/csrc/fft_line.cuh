@@ -1,0 +1,146 @@
+// Line FFTs held in registers by small groups of cooperating threads.
+//
+// A line of power-of-two length L is split as L = R * TPL: each of TPL
+// threads of one warp holds R = L / TPL values.  A forward transform is
+//   X[m + R*s] = sum_q W_TPL^(q*s) * W_L^(q*m) * sum_k x[q + TPL*k] W_R^(k*m)
+// i.e. an R-point DFT in registers, a twiddle by W_L^(q*m), one exchange of
+// the line through shared memory, and a TPL-point DFT in registers.  The
+// inverse runs the same steps in the opposite order.  Both directions are
+// unnormalised; scaling is applied by the caller.
+//
+// Register layouts (q = the thread's rank in its group, 0 <= q < TPL):
+//   natural : v[k]    = x[q + TPL*k]                  k < R
+//   split   : o[j][s] = X[m_j + R*s],  m_j = q + TPL*j  j < R/TPL, s < TPL
+// The caller loads and stores those positions; nothing is ever reordered in
+// memory by a bit-reversal pass.
+#pragma once
+#include "cpra_common.cuh"
+
+namespace cpra_b200 {
+
+template <int R>
+__host__ __device__ __forceinline__ constexpr int brev(int j) {
+    int r = 0;
+    for (int b = 1, t = R >> 1; b < R; b <<= 1, t >>= 1)
+        if (j & b) r |= t;
+    return r;
+}
+
+// a * W_32^k (forward: exp(-2 pi i k/32), inverse: exp(+2 pi i k/32)); k is a
+// compile-time constant after unrolling, so the branches fold away and the
+// multiplications by 1, -1, +-i are exact.
+template <typename T, bool INV>
+__device__ __forceinline__ Cx<T> rot32(Cx<T> a, int k) {
+    k &= 31;
+    if (k == 0) return a;
+    if (k == 16) return cneg(a);
+    if (k == 8) return INV ? Cx<T>{-a.y, a.x} : Cx<T>{a.y, -a.x};
+    if (k == 24) return INV ? Cx<T>{a.y, -a.x} : Cx<T>{-a.y, a.x};
+    const Cx<T> w = {tw32_cos<T>(k), INV ? tw32_sin<T>(k) : -tw32_sin<T>(k)};
+    return cmul(a, w);
+}
+
+// In-place radix-2 decimation-in-frequency DFT of R <= 32 register values:
+// natural order in, v[i] = X[brev<R>(i)] out.
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void dft_regs(Cx<T> (&v)[R]) {
+    static_assert(R >= 1 && R <= 32 && (R & (R - 1)) == 0, "R must be a power of two <= 32");
+#pragma unroll
+    for (int half = R / 2; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int base = 0; base < R; base += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const Cx<T> a = v[base + j];
+                const Cx<T> b = v[base + j + half];
+                v[base + j] = cadd(a, b);
+                v[base + j + half] = rot32<T, INV>(csub(a, b), j * (32 / (2 * half)));
+            }
+        }
+    }
+}
+
+// Exchange slot of element (m, q) in a line's L-slot scratch.  The rotation
+// (q + m) mod TPL spreads both the writes (fixed m, all q) and the reads
+// (fixed owned m_j and source p, all q) over distinct shared-memory banks for
+// rows (slot stride 1, line stride L+TPL) and columns (slot stride L+TPL).
+template <int TPL>
+__device__ __forceinline__ int xslot(int m, int q) { return m * TPL + ((q + m) & (TPL - 1)); }
+
+template <typename T, int L, int TPL>
+struct LineFFT {
+    static constexpr int R = L / TPL;
+    static constexpr int J = R / TPL;
+    static_assert(TPL >= 1 && TPL <= 32 && (TPL & (TPL - 1)) == 0, "TPL must be a power of two <= 32");
+    static_assert(R <= 32 && R >= TPL, "need TPL <= R <= 32");
+
+    // natural -> split.  scratch: the line's L slots in shared memory, slot u at
+    // scratch[u * ss] (may be the storage the values were loaded from; the
+    // group's warp is synchronised before it is overwritten);
+    // twL[t] = exp(-2 pi i t / L).
+    template <bool INV>
+    __device__ __forceinline__ static void natural_to_split(Cx<T> (&v)[R], Cx<T> (&o)[J][TPL], Cx<T>* scratch,
+                                                            int ss, const Cx<T>* twL, int q) {
+        dft_regs<T, R, INV>(v);
+        if constexpr (TPL == 1) {
+#pragma unroll
+            for (int j = 0; j < J; ++j) o[j][0] = v[brev<R>(j)];
+        } else {
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < R; ++m) {
+                Cx<T> y = v[brev<R>(m)];
+                const int t = q * m;  // < L
+                if (m != 0) y = INV ? cmulc(y, twL[t]) : cmul(y, twL[t]);
+                scratch[xslot<TPL>(m, q) * ss] = y;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int m = q + TPL * j;
+                Cx<T> w[TPL];
+#pragma unroll
+                for (int p = 0; p < TPL; ++p) w[p] = scratch[xslot<TPL>(m, p) * ss];
+                dft_regs<T, TPL, INV>(w);
+#pragma unroll
+                for (int s = 0; s < TPL; ++s) o[j][s] = w[brev<TPL>(s)];
+            }
+            __syncwarp();
+        }
+    }
+
+    // split -> natural (the reverse of natural_to_split's data movement)
+    template <bool INV>
+    __device__ __forceinline__ static void split_to_natural(Cx<T> (&o)[J][TPL], Cx<T> (&v)[R], Cx<T>* scratch,
+                                                            int ss, const Cx<T>* twL, int q) {
+        if constexpr (TPL == 1) {
+#pragma unroll
+            for (int m = 0; m < R; ++m) v[m] = o[m][0];
+        } else {
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                const int m = q + TPL * j;
+                Cx<T> w[TPL];
+#pragma unroll
+                for (int s = 0; s < TPL; ++s) w[s] = o[j][s];
+                dft_regs<T, TPL, INV>(w);  // w[i] = Z[m][brev(i)]
+#pragma unroll
+                for (int i = 0; i < TPL; ++i) {
+                    const int p = brev<TPL>(i);
+                    Cx<T> z = w[i];
+                    const int t = p * m;
+                    if (t != 0) z = INV ? cmulc(z, twL[t]) : cmul(z, twL[t]);
+                    scratch[xslot<TPL>(m, p) * ss] = z;
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < R; ++m) v[m] = scratch[xslot<TPL>(m, q) * ss];
+            __syncwarp();
+        }
+        dft_regs<T, R, INV>(v);  // v[i] = x[q + TPL * brev<R>(i)]
+    }
+};
+
+}  // namespace cpra_b200

@@ -1,0 +1,397 @@
+// Element-wise operators of the CpraImpl<T> interface and the reductions and
+// interpolations around them.  All are grid-stride kernels sized to whole
+// waves over the SMs.  Constraint planes are broadcast over the batch the way
+// the reference indexes them, element i using plane element i % (num/batch)
+// (include/detail/MKL_Impl.inl:83,98,121): each thread keeps one plane value
+// in a register and applies it to every repetition, so a plane is read once.
+#include "cpra_internal.h"
+#include "ops_ew.cuh"
+
+#include <cmath>
+
+namespace cpra_b200 {
+
+namespace {
+
+constexpr int EW_THREADS = 256;
+
+__device__ __forceinline__ uint64_t gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
+
+template <typename T>
+__global__ void k_space(Cx<T>* __restrict__ x, const T* __restrict__ s, uint64_t num, uint64_t plane, int mode) {
+    for (uint64_t j = gtid(); j < plane; j += gstride()) {
+        const T sv = s[j];
+        for (uint64_t i = j; i < num; i += plane) x[i] = space_apply(x[i], sv, mode);
+    }
+}
+
+template <typename T>
+__global__ void k_data_real(Cx<T>* __restrict__ x, const T* __restrict__ a, uint64_t num, uint64_t plane,
+                            int mode) {
+    for (uint64_t j = gtid(); j < plane; j += gstride()) {
+        const T av = a[j];
+        for (uint64_t i = j; i < num; i += plane) x[i] = data_apply(x[i], av, mode);
+    }
+}
+
+template <typename T>
+__global__ void k_data_complex(Cx<T>* __restrict__ x, const Cx<T>* __restrict__ c, uint64_t num,
+                               uint64_t plane) {
+    for (uint64_t j = gtid(); j < plane; j += gstride()) {
+        const Cx<T> cv = c[j];
+        for (uint64_t i = j; i < num; i += plane) x[i] = data_apply_complex(x[i], cv);
+    }
+}
+
+// src may alias dst exactly (test/unitest_mkl.cpp:33 calls MergeAddData(x, x, ...))
+template <typename T>
+__global__ void k_merge(const Cx<T>* src, Cx<T>* dst, T alpha, T beta, uint64_t num) {
+    for (uint64_t i = gtid(); i < num; i += gstride()) dst[i] = merge_apply(src[i], dst[i], alpha, beta);
+}
+
+template <typename T>
+__global__ void k_scale(Cx<T>* __restrict__ x, T f, uint64_t num) {
+    for (uint64_t i = gtid(); i < num; i += gstride()) x[i] = cscale(x[i], f);
+}
+
+// In-place fftshift of [batch][M][N] planes: element (r, c) trades places with
+// ((r + M/2) % M, (c + N/2) % N), which is MKL_Impl.inl:180-209's quadrant swap
+// for even sizes and a one-axis shift when one size is 1.  Each pair is
+// visited once (from its member with r < M/2, or c < N/2 when M == 1).
+template <typename T>
+__global__ void k_shift2d(Cx<T>* __restrict__ x, uint64_t M, uint64_t N, uint64_t batch) {
+    const uint64_t rows = (M >= 2) ? M / 2 : 1;
+    const uint64_t cols = (M >= 2) ? N : N / 2;
+    const uint64_t total = batch * rows * cols;
+    for (uint64_t e = gtid(); e < total; e += gstride()) {
+        const uint64_t c = e % cols;
+        const uint64_t r = (e / cols) % rows;
+        const uint64_t b = e / (cols * rows);
+        const uint64_t r2 = (r + M / 2) % M, c2 = (c + N / 2) % N;
+        Cx<T>* base = x + b * M * N;
+        const Cx<T> u = base[r * N + c];
+        base[r * N + c] = base[r2 * N + c2];
+        base[r2 * N + c2] = u;
+    }
+}
+
+// [batch][L][M][N] volumes: MKL_Impl.inl:212-251's octant swap
+template <typename T>
+__global__ void k_shift3d(Cx<T>* __restrict__ x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch) {
+    const uint64_t deps = (L >= 2) ? L / 2 : 1;
+    const uint64_t rows = (L >= 2) ? M : ((M >= 2) ? M / 2 : 1);
+    const uint64_t cols = (L >= 2 || M >= 2) ? N : N / 2;
+    const uint64_t total = batch * deps * rows * cols;
+    for (uint64_t e = gtid(); e < total; e += gstride()) {
+        const uint64_t c = e % cols;
+        const uint64_t r = (e / cols) % rows;
+        const uint64_t d = (e / (cols * rows)) % deps;
+        const uint64_t b = e / (cols * rows * deps);
+        const uint64_t d2 = (d + L / 2) % L, r2 = (r + M / 2) % M, c2 = (c + N / 2) % N;
+        Cx<T>* base = x + b * L * M * N;
+        const uint64_t i1 = (d * M + r) * N + c, i2 = (d2 * M + r2) * N + c2;
+        const Cx<T> u = base[i1];
+        base[i1] = base[i2];
+        base[i2] = u;
+    }
+}
+
+// splitmix64 finaliser (S. Vigna), a counter-based stream: value i of stream
+// (seed, id) depends only on (seed, id, i), not on the launch shape
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void k_uniform(T* __restrict__ x, uint64_t num, uint64_t key) {
+    for (uint64_t i = gtid(); i < num; i += gstride()) {
+        const uint64_t r = mix64(key + mix64(i));
+        if constexpr (sizeof(T) == 4)
+            x[i] = (float)(r >> 40) * 0x1.0p-24f;  // [0, 1), 24 random bits
+        else
+            x[i] = (double)(r >> 11) * 0x1.0p-53;  // [0, 1), 53 random bits
+    }
+}
+
+// Sums of |a|^2 and |b|^2 over member i's `span` elements, in double.
+// Stage 1: grid (CONVERGE_BLOCKS, batch); each block writes one partial pair.
+template <typename T>
+__global__ void k_norm_partial(const Cx<T>* __restrict__ a, const Cx<T>* __restrict__ b, uint64_t span,
+                               uint64_t stride, double* __restrict__ partials) {
+    __shared__ double sa[EW_THREADS], sb[EW_THREADS];
+    const uint64_t m = blockIdx.y;
+    const Cx<T>* pa = a + m * stride;
+    const Cx<T>* pb = b + m * stride;
+    double accA = 0.0, accB = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)EW_THREADS + threadIdx.x; i < span;
+         i += (uint64_t)gridDim.x * EW_THREADS) {
+        const Cx<T> u = pa[i], v = pb[i];
+        accA = fma((double)u.x, (double)u.x, fma((double)u.y, (double)u.y, accA));
+        accB = fma((double)v.x, (double)v.x, fma((double)v.y, (double)v.y, accB));
+    }
+    sa[threadIdx.x] = accA;
+    sb[threadIdx.x] = accB;
+    __syncthreads();
+    for (int h = EW_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sa[threadIdx.x] += sa[threadIdx.x + h];
+            sb[threadIdx.x] += sb[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[(m * gridDim.x + blockIdx.x) * 2 + 0] = sa[0];
+        partials[(m * gridDim.x + blockIdx.x) * 2 + 1] = sb[0];
+    }
+}
+
+// Stage 2: member i's partials summed in index order (deterministic)
+__global__ void k_norm_final(const double* __restrict__ partials, double* __restrict__ sums, uint64_t batch,
+                             int blocks) {
+    for (uint64_t m = gtid(); m < batch; m += gstride()) {
+        double sA = 0.0, sB = 0.0;
+        for (int k = 0; k < blocks; ++k) {
+            sA += partials[(m * blocks + k) * 2 + 0];
+            sB += partials[(m * blocks + k) * 2 + 1];
+        }
+        sums[2 * m + 0] = sA;
+        sums[2 * m + 1] = sB;
+    }
+}
+
+// C round(): halfway cases away from zero
+__device__ __forceinline__ double round_away(double v) { return round(v); }
+
+// Deterministic gather form of ker_Real2DTo3DInterpolation +
+// ker_NormRealInterpolation (CUDA_Impl_Kernel.cuh:68-119).  Forward mapping of
+// slice pixel (xIn, yIn) of slice p (column-major, yIn fastest): xr = xIn - N/2,
+// yr = M/2 - yIn, 3D point (yr sin a, xr, yr cos a), nearest voxel (j, k, l)
+// stored at z = L/2 - j, x = N/2 + k, y = M/2 - l, flat z*M*N + x*M + y, weight
+// 50 for distance <= 0.02 else 1/distance, skipped for distance >= 0.5.  A
+// voxel can only be reached from the pixel with xIn = x and yr the integer
+// nearest to j sin a + l cos a (any other yr is >= 0.5 away along the slice),
+// so each voxel visits every slice once and sums its weights in slice order.
+template <typename T>
+__global__ void k_real2d_to_3d(const T* __restrict__ src, T* __restrict__ dst, const T* __restrict__ ang,
+                               int64_t M, int64_t N, int64_t P, int64_t L) {
+    const uint64_t total = (uint64_t)M * N * L;
+    for (uint64_t idx = gtid(); idx < total; idx += gstride()) {
+        const int64_t y = (int64_t)(idx % M);
+        const int64_t x = (int64_t)((idx / M) % N);
+        const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
+        const int64_t j = L / 2 - z, k = x - N / 2, l = M / 2 - y;
+        double acc = 0.0, wsum = 0.0;
+        for (int64_t p = 0; p < P; ++p) {
+            const double a = (double)ang[p];
+            const double sa = sin(a), ca = cos(a);
+            const double yr = rint((double)j * sa + (double)l * ca);
+            const int64_t yIn = M / 2 - (int64_t)yr;
+            if (yIn < 0 || yIn >= M) continue;
+            const double x3 = yr * sa, z3 = yr * ca;
+            if ((int64_t)round_away(x3) != j || (int64_t)round_away(z3) != l) continue;
+            const double dist = sqrt((x3 - (double)j) * (x3 - (double)j) + (z3 - (double)l) * (z3 - (double)l));
+            if (!(dist < 0.5)) continue;
+            const double w = (dist <= 0.02) ? 50.0 : 1.0 / dist;
+            acc += w * (double)src[p * M * N + x * M + yIn];
+            wsum += w;
+        }
+        dst[idx] = (wsum > 0.0) ? (T)(acc / wsum) : (T)0;
+    }
+}
+
+// Complex2DTo3DInterpolation (the reference leaves it a stub,
+// include/CUDA_Impl.cuh:89): gather-form trilinear merge of P complex central
+// slices into a [L][N][M] volume with the geometry of the real merge above.
+// Voxel (z, x, y) is the point (j, k, l) = (L/2 - z, x - N/2, M/2 - y); for
+// slice p at angle a its in-plane coordinates are (yr, xr) = (j sin a + l cos
+// a, k) and its distance to the plane is d = j cos a - l sin a.  Slices with
+// |d| < 1 contribute (1 - |d|) times the slice bilinearly sampled at
+// (yIn, xIn) = (M/2 - yr, N/2 + k); the voxel is the weight-normalised sum, or
+// 0 (left unconstrained by the complex DataConstraint) when nothing reaches it.
+template <typename T>
+__global__ void k_complex2d_to_3d(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst,
+                                  const T* __restrict__ ang, int64_t M, int64_t N, int64_t P, int64_t L) {
+    const uint64_t total = (uint64_t)M * N * L;
+    for (uint64_t idx = gtid(); idx < total; idx += gstride()) {
+        const int64_t y = (int64_t)(idx % M);
+        const int64_t x = (int64_t)((idx / M) % N);
+        const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
+        const double j = (double)(L / 2 - z), l = (double)(M / 2 - y);
+        double accx = 0.0, accy = 0.0, wsum = 0.0;
+        for (int64_t p = 0; p < P; ++p) {
+            const double a = (double)ang[p];
+            const double sa = sin(a), ca = cos(a);
+            const double d = j * ca - l * sa;
+            const double wd = 1.0 - fabs(d);
+            if (!(wd > 0.0)) continue;
+            const double yIn = (double)(M / 2) - (j * sa + l * ca);
+            const double y0f = floor(yIn);
+            const int64_t y0 = (int64_t)y0f;
+            const double fy = yIn - y0f;
+            double sx = 0.0, sy = 0.0, sw = 0.0;
+            for (int dy = 0; dy < 2; ++dy) {
+                const int64_t yy = y0 + dy;
+                const double wy = dy ? fy : 1.0 - fy;
+                if (yy < 0 || yy >= M || wy == 0.0) continue;
+                const Cx<T> v = src[p * M * N + x * M + yy];
+                sx += wy * (double)v.x;
+                sy += wy * (double)v.y;
+                sw += wy;
+            }
+            if (sw == 0.0) continue;
+            accx += wd * sx;
+            accy += wd * sy;
+            wsum += wd * sw;
+        }
+        dst[idx] = (wsum > 0.0) ? Cx<T>{(T)(accx / wsum), (T)(accy / wsum)} : Cx<T>{T(0), T(0)};
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_space_constraint(bool dbl, void* x, const void* s, uint64_t num, uint64_t plane, int mode,
+                                    cudaStream_t st) {
+    const unsigned g = ew_grid(plane, EW_THREADS);
+    if (dbl)
+        k_space<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)s, num, plane, mode);
+    else
+        k_space<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)s, num, plane, mode);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_data_constraint_real(bool dbl, void* x, const void* a, uint64_t num, uint64_t plane, int mode,
+                                        cudaStream_t st) {
+    const unsigned g = ew_grid(plane, EW_THREADS);
+    if (dbl)
+        k_data_real<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)a, num, plane, mode);
+    else
+        k_data_real<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)a, num, plane, mode);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_data_constraint_complex(bool dbl, void* x, const void* c, uint64_t num, uint64_t plane,
+                                           cudaStream_t st) {
+    const unsigned g = ew_grid(plane, EW_THREADS);
+    if (dbl)
+        k_data_complex<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const Cx<double>*)c, num, plane);
+    else
+        k_data_complex<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const Cx<float>*)c, num, plane);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_add(bool dbl, const void* src, void* dst, double alpha, double beta, uint64_t num,
+                             cudaStream_t st) {
+    const unsigned g = ew_grid(num, EW_THREADS);
+    if (dbl)
+        k_merge<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst, alpha, beta, num);
+    else
+        k_merge<float><<<g, EW_THREADS, 0, st>>>((const Cx<float>*)src, (Cx<float>*)dst, (float)alpha,
+                                                 (float)beta, num);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale(bool dbl, void* x, double factor, uint64_t num, cudaStream_t st) {
+    const unsigned g = ew_grid(num, EW_THREADS);
+    if (dbl)
+        k_scale<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, factor, num);
+    else
+        k_scale<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (float)factor, num);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fftshift2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t batch, cudaStream_t st) {
+    const uint64_t work = batch * M * N / 2;
+    if (work == 0) return cudaSuccess;
+    const unsigned g = ew_grid(work, EW_THREADS);
+    if (dbl)
+        k_shift2d<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, M, N, batch);
+    else
+        k_shift2d<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, M, N, batch);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fftshift3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch,
+                              cudaStream_t st) {
+    const uint64_t work = batch * M * N * L / 2;
+    if (work == 0) return cudaSuccess;
+    const unsigned g = ew_grid(work, EW_THREADS);
+    if (dbl)
+        k_shift3d<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, M, N, L, batch);
+    else
+        k_shift3d<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, M, N, L, batch);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_uniform(bool dbl, void* x, uint64_t num, uint64_t seed, uint64_t stream_id, cudaStream_t st) {
+    const unsigned g = ew_grid(num, EW_THREADS);
+    const uint64_t key = seed * 0xD1B54A32D192ED03ull + stream_id * 0x8CB92BA72F3D8DD7ull;
+    if (dbl)
+        k_uniform<double><<<g, EW_THREADS, 0, st>>>((double*)x, num, key);
+    else
+        k_uniform<float><<<g, EW_THREADS, 0, st>>>((float*)x, num, key);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t span, uint64_t stride,
+                              uint64_t batch, double* partials, double* sums, cudaStream_t st) {
+    if (batch == 0) return cudaSuccess;
+    if (batch > 65535) return cudaErrorInvalidValue;
+    dim3 grid(CONVERGE_BLOCKS, (unsigned)batch);
+    if (dbl)
+        k_norm_partial<double><<<grid, EW_THREADS, 0, st>>>((const Cx<double>*)a, (const Cx<double>*)b, span,
+                                                            stride, partials);
+    else
+        k_norm_partial<float><<<grid, EW_THREADS, 0, st>>>((const Cx<float>*)a, (const Cx<float>*)b, span, stride,
+                                                           partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_norm_final<<<ew_grid(batch, 64), 64, 0, st>>>(partials, sums, batch, CONVERGE_BLOCKS);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_real2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m, uint64_t n,
+                                uint64_t p, uint64_t l, cudaStream_t st) {
+    const uint64_t total = m * n * l;
+    if (total == 0) return cudaSuccess;
+    const unsigned g = ew_grid(total, EW_THREADS);
+    if (dbl)
+        k_real2d_to_3d<double><<<g, EW_THREADS, 0, st>>>((const double*)src, (double*)dst, (const double*)angles,
+                                                         (int64_t)m, (int64_t)n, (int64_t)p, (int64_t)l);
+    else
+        k_real2d_to_3d<float><<<g, EW_THREADS, 0, st>>>((const float*)src, (float*)dst, (const float*)angles,
+                                                        (int64_t)m, (int64_t)n, (int64_t)p, (int64_t)l);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m,
+                                   uint64_t n, uint64_t p, uint64_t l, cudaStream_t st) {
+    const uint64_t total = m * n * l;
+    if (total == 0) return cudaSuccess;
+    const unsigned g = ew_grid(total, EW_THREADS);
+    if (dbl)
+        k_complex2d_to_3d<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst,
+                                                            (const double*)angles, (int64_t)m, (int64_t)n,
+                                                            (int64_t)p, (int64_t)l);
+    else
+        k_complex2d_to_3d<float><<<g, EW_THREADS, 0, st>>>((const Cx<float>*)src, (Cx<float>*)dst,
+                                                           (const float*)angles, (int64_t)m, (int64_t)n,
+                                                           (int64_t)p, (int64_t)l);
+    count_launches();
+    return cudaGetLastError();
+}
+
+}  // namespace cpra_b200

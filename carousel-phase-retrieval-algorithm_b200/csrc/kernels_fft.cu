@@ -1,0 +1,335 @@
+// Shifted 2D / 3D transforms (Forward2D, Backward2D, Forward3D, Backward3D).
+//
+// The reference computes fftshift -> DFT -> fftshift with three passes over
+// memory (include/detail/MKL_Impl.inl:128-178, include/detail/CUDA_Impl.inl:
+// 20-84).  For even sizes shift o DFT o shift equals s * D (.) DFT(D (.) x)
+// with D = (-1)^(sum of indices) and s = (-1)^(sum of half sizes), so here the
+// shifts are sign flips applied while the data is in registers:
+//   * square planes up to 128 x 128 (float) / 64 x 64 (double): one CTA per
+//     plane holds the whole plane in shared memory, one HBM round trip;
+//   * other power-of-two lengths up to 1024: one pass per axis, each pass
+//     staging a tile of lines in shared memory;
+//   * other even lengths: a direct O(L^2) DFT pass per axis.
+#include "cpra_internal.h"
+#include "fft2d_cta.cuh"
+
+namespace cpra_b200 {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// one plane per CTA
+// ---------------------------------------------------------------------------
+template <typename T, int L, bool INV>
+__global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, const Cx<T>* __restrict__ twg,
+                                                     T scale, int s_neg) {
+    using P = Plane<T, L>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
+    Cx<T>* tw = buf + L * P::LS;
+    const int t = threadIdx.x, line = t >> 2, q = t & 3;
+    for (int i = t; i < L; i += P::NT) tw[i] = twg[i];
+    Cx<T>* g = data + (size_t)blockIdx.x * L * L;
+    __syncthreads();
+    if constexpr (!INV) {
+        Cx<T> v[P::R];
+#pragma unroll
+        for (int k = 0; k < P::R; ++k) {
+            const int n = q + P::TPL * k;
+            v[k] = csign(g[line * L + n], line + n);
+        }
+        P::template rows_to_buf<false>(v, buf, tw, line, q);
+        __syncthreads();
+        Cx<T> o[P::J][P::TPL];
+        P::template col_from_buf<false>(o, buf, tw, line, q);
+#pragma unroll
+        for (int j = 0; j < P::J; ++j)
+#pragma unroll
+            for (int s = 0; s < P::TPL; ++s) {
+                const int f = P::split_pos(q, j, s);
+                g[f * L + line] = csign(o[j][s], f + line + s_neg);
+            }
+    } else {
+        Cx<T> o[P::J][P::TPL];
+#pragma unroll
+        for (int j = 0; j < P::J; ++j)
+#pragma unroll
+            for (int s = 0; s < P::TPL; ++s) {
+                const int f = P::split_pos(q, j, s);
+                o[j][s] = csign(g[f * L + line], f + line + s_neg);
+            }
+        P::template col_to_buf<true>(o, buf, tw, line, q);
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, line, q);
+#pragma unroll
+        for (int j = 0; j < P::J; ++j)
+#pragma unroll
+            for (int s = 0; s < P::TPL; ++s) {
+                const int f = P::split_pos(q, j, s);
+                g[line * L + f] = csign(cscale(o[j][s], scale), line + f);
+            }
+    }
+}
+
+template <typename T, int L>
+cudaError_t plane_fft(void* x, uint64_t batch, bool inverse, T scale, int s_neg, const void* tw, cudaStream_t st) {
+    using P = Plane<T, L>;
+    const size_t smem = P::buf_bytes() + sizeof(Cx<T>) * L;
+    auto kf = inverse ? k_plane_fft<T, L, true> : k_plane_fft<T, L, false>;
+    cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kf<<<(unsigned)batch, P::NT, smem, st>>>((Cx<T>*)x, (const Cx<T>*)tw, scale, s_neg);
+    count_launches();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// one axis of a [Bo][L][Bi] array, power-of-two L <= 1024
+// ---------------------------------------------------------------------------
+constexpr int AXIS_THREADS = 256;
+
+template <typename T, int L, int TPL>
+__global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ data, uint64_t Bo, uint64_t Bi,
+                                                           uint64_t tiles_i, const Cx<T>* __restrict__ twg,
+                                                           int inverse, int shift, int out_neg, T scale,
+                                                           int do_scale) {
+    constexpr int LINES = AXIS_THREADS / TPL;
+    constexpr int PADL = TPL < 16 ? TPL : 0;
+    constexpr int LSX = L + PADL;
+    constexpr int R = L / TPL;
+    constexpr int J = R / TPL;
+    using F = LineFFT<T, L, TPL>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
+    Cx<T>* tw = buf + LINES * LSX;
+    const int t = threadIdx.x;
+    for (int i = t; i < L; i += AXIS_THREADS) tw[i] = twg[i];
+
+    const uint64_t tile = blockIdx.x;
+    const bool contig = (Bi == 1);
+    uint64_t o0 = 0, i0 = 0;
+    if (contig) {
+        o0 = tile * LINES;
+    } else {
+        o0 = tile / tiles_i;
+        i0 = (tile % tiles_i) * LINES;
+    }
+    for (int e = t; e < LINES * L; e += AXIS_THREADS) {
+        int l, n;
+        uint64_t gidx;
+        bool ok;
+        if (contig) {
+            l = e / L;
+            n = e % L;
+            ok = (o0 + l) < Bo;
+            gidx = (o0 + l) * (uint64_t)L + n;
+        } else {
+            l = e % LINES;
+            n = e / LINES;
+            ok = (i0 + l) < Bi;
+            gidx = (o0 * L + n) * Bi + i0 + l;
+        }
+        buf[l * LSX + n] = ok ? data[gidx] : Cx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+
+    const int line = t / TPL, q = t % TPL;
+    Cx<T> v[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int n = q + TPL * k;
+        v[k] = buf[line * LSX + n];
+        if (shift) v[k] = csign(v[k], n);
+    }
+    Cx<T> o[J][TPL];
+    if (inverse)
+        F::template natural_to_split<true>(v, o, buf + line * LSX, 1, tw, q);
+    else
+        F::template natural_to_split<false>(v, o, buf + line * LSX, 1, tw, q);
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) {
+            const int f = q + TPL * j + R * s;
+            Cx<T> w = o[j][s];
+            if (do_scale) w = cscale(w, scale);
+            if (shift) w = csign(w, f + out_neg);
+            buf[line * LSX + f] = w;
+        }
+    __syncthreads();
+    for (int e = t; e < LINES * L; e += AXIS_THREADS) {
+        int l, n;
+        uint64_t gidx;
+        bool ok;
+        if (contig) {
+            l = e / L;
+            n = e % L;
+            ok = (o0 + l) < Bo;
+            gidx = (o0 + l) * (uint64_t)L + n;
+        } else {
+            l = e % LINES;
+            n = e / LINES;
+            ok = (i0 + l) < Bi;
+            gidx = (o0 * L + n) * Bi + i0 + l;
+        }
+        if (ok) data[gidx] = buf[l * LSX + n];
+    }
+}
+
+template <typename T, int L, int TPL>
+cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shift, int out_neg, T scale,
+                       bool do_scale, const void* tw, cudaStream_t st) {
+    constexpr int LINES = AXIS_THREADS / TPL;
+    constexpr int PADL = TPL < 16 ? TPL : 0;
+    const size_t smem = sizeof(Cx<T>) * ((size_t)LINES * (L + PADL) + L);
+    auto kf = k_axis_fft<T, L, TPL>;
+    cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    uint64_t tiles_i = 1, tiles;
+    if (Bi == 1) {
+        tiles = (Bo + LINES - 1) / LINES;
+    } else {
+        tiles_i = (Bi + LINES - 1) / LINES;
+        tiles = Bo * tiles_i;
+    }
+    if (tiles == 0) return cudaSuccess;
+    if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+    kf<<<(unsigned)tiles, AXIS_THREADS, smem, st>>>((Cx<T>*)x, Bo, Bi, tiles_i, (const Cx<T>*)tw, inverse ? 1 : 0,
+                                                    shift ? 1 : 0, out_neg, scale, do_scale ? 1 : 0);
+    count_launches();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// one axis, any length: direct DFT, out of place
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_axis_dft(const Cx<T>* __restrict__ in, Cx<T>* __restrict__ out, uint64_t Bo, uint64_t L,
+                           uint64_t Bi, const Cx<T>* __restrict__ tw, int inverse, int shift, int out_neg, T scale,
+                           int do_scale) {
+    const uint64_t total = Bo * L * Bi;
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = idx % Bi;
+        const uint64_t f = (idx / Bi) % L;
+        const uint64_t o = idx / (Bi * L);
+        const Cx<T>* line = in + o * L * Bi + i;
+        Cx<T> acc = {T(0), T(0)};
+        uint64_t w = 0;
+        for (uint64_t n = 0; n < L; ++n) {
+            Cx<T> a = line[n * Bi];
+            if (shift && (n & 1)) a = cneg(a);
+            const Cx<T> t = inverse ? cmulc(a, tw[w]) : cmul(a, tw[w]);
+            acc = cadd(acc, t);
+            w += f;
+            if (w >= L) w -= L;
+        }
+        if (do_scale) acc = cscale(acc, scale);
+        if (shift) acc = csign(acc, (int)(f & 1) + out_neg);
+        out[idx] = acc;
+    }
+}
+
+template <typename T>
+cudaError_t axis_dft_t(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi, bool inverse, bool shift,
+                       int out_neg, T scale, bool do_scale, const void* tw, cudaStream_t st) {
+    const uint64_t total = Bo * L * Bi;
+    if (total == 0) return cudaSuccess;
+    k_axis_dft<T><<<ew_grid(total, 256), 256, 0, st>>>((const Cx<T>*)x, (Cx<T>*)work, Bo, L, Bi,
+                                                       (const Cx<T>*)tw, inverse ? 1 : 0, shift ? 1 : 0, out_neg,
+                                                       scale, do_scale ? 1 : 0);
+    count_launches();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(x, work, total * sizeof(Cx<T>), cudaMemcpyDeviceToDevice, st);
+}
+
+bool is_pow2(uint64_t n) { return n > 0 && (n & (n - 1)) == 0; }
+
+template <typename T>
+cudaError_t axis_pass(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi, bool inverse, T scale,
+                      bool do_scale, const void* tw, cudaStream_t st) {
+    const int out_neg = (int)((L / 2) & 1);  // s_a = (-1)^(L/2)
+    if (L == 1) {
+        if (!do_scale) return cudaSuccess;
+        return launch_scale(sizeof(T) == 8, x, (double)scale, Bo * Bi, st);
+    }
+    if (!is_pow2(L) || L > 1024) return axis_dft_t<T>(x, work, Bo, L, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+    switch (L) {
+        case 2: return axis_fft_t<T, 2, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 4: return axis_fft_t<T, 4, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 8: return axis_fft_t<T, 8, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 16: return axis_fft_t<T, 16, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 32: return axis_fft_t<T, 32, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 64: return axis_fft_t<T, 64, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 128: return axis_fft_t<T, 128, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 256: return axis_fft_t<T, 256, 8>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 512: return axis_fft_t<T, 512, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 1024: return axis_fft_t<T, 1024, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t fft2d_t(void* x, uint64_t M, uint64_t N, uint64_t batch, bool inverse, T scale, const void* tw_m,
+                    const void* tw_n, void* work, cudaStream_t st) {
+    if (M == N && fft2d_single_cta(sizeof(T) == 8, M, N)) {
+        const int s_neg = (int)(((M / 2) + (N / 2)) & 1);
+        switch (M) {
+            case 32: return plane_fft<T, 32>(x, batch, inverse, scale, s_neg, tw_m, st);
+            case 64: return plane_fft<T, 64>(x, batch, inverse, scale, s_neg, tw_m, st);
+            case 128:
+                if constexpr (sizeof(T) == 4) return plane_fft<T, 128>(x, batch, inverse, scale, s_neg, tw_m, st);
+                break;
+            default: break;
+        }
+    }
+    cudaError_t e;
+    if (!inverse) {
+        if ((e = axis_pass<T>(x, work, batch * M, N, 1, false, scale, false, tw_n, st)) != cudaSuccess) return e;
+        return axis_pass<T>(x, work, batch, M, N, false, scale, false, tw_m, st);
+    }
+    if ((e = axis_pass<T>(x, work, batch, M, N, true, scale, false, tw_m, st)) != cudaSuccess) return e;
+    return axis_pass<T>(x, work, batch * M, N, 1, true, scale, true, tw_n, st);
+}
+
+template <typename T>
+cudaError_t fft3d_t(void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch, bool inverse, T scale,
+                    const void* tw_m, const void* tw_n, const void* tw_l, void* work, cudaStream_t st) {
+    cudaError_t e;
+    if (!inverse) {
+        if ((e = axis_pass<T>(x, work, batch * L * M, N, 1, false, scale, false, tw_n, st)) != cudaSuccess) return e;
+        if ((e = axis_pass<T>(x, work, batch * L, M, N, false, scale, false, tw_m, st)) != cudaSuccess) return e;
+        return axis_pass<T>(x, work, batch, L, M * N, false, scale, false, tw_l, st);
+    }
+    if ((e = axis_pass<T>(x, work, batch, L, M * N, true, scale, false, tw_l, st)) != cudaSuccess) return e;
+    if ((e = axis_pass<T>(x, work, batch * L, M, N, true, scale, false, tw_m, st)) != cudaSuccess) return e;
+    return axis_pass<T>(x, work, batch * L * M, N, 1, true, scale, true, tw_n, st);
+}
+
+}  // namespace
+
+bool fft2d_single_cta(bool dbl, uint64_t M, uint64_t N) {
+    if (M != N) return false;
+    if (dbl) return M == 32 || M == 64;
+    return M == 32 || M == 64 || M == 128;
+}
+
+bool fft_length_supported(uint64_t L) { return L >= 1 && L <= 4096 && (L == 1 || (L % 2) == 0); }
+
+cudaError_t launch_fft2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t batch, bool inverse, double scale,
+                         const void* tw_m, const void* tw_n, void* work, cudaStream_t st) {
+    if (batch == 0) return cudaSuccess;
+    return dbl ? fft2d_t<double>(x, M, N, batch, inverse, scale, tw_m, tw_n, work, st)
+               : fft2d_t<float>(x, M, N, batch, inverse, (float)scale, tw_m, tw_n, work, st);
+}
+
+cudaError_t launch_fft3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch, bool inverse,
+                         double scale, const void* tw_m, const void* tw_n, const void* tw_l, void* work,
+                         cudaStream_t st) {
+    if (batch == 0) return cudaSuccess;
+    return dbl ? fft3d_t<double>(x, M, N, L, batch, inverse, scale, tw_m, tw_n, tw_l, work, st)
+               : fft3d_t<float>(x, M, N, L, batch, inverse, (float)scale, tw_m, tw_n, tw_l, work, st);
+}
+
+}  // namespace cpra_b200

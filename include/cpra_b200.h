@@ -1,0 +1,157 @@
+/*
+ * cpra_b200.h - C ABI of the B200 backend for carousel phase retrieval.
+ *
+ * One entry point per virtual of the reference's operator interface
+ * CPRA::CpraImpl<T> (include/CPRA_Impl.hpp:18-63), plus construction,
+ * allocation and a few extensions.  Plain pointers and sizes only; no CUDA or
+ * C++ types cross this boundary.  The C++ drop-in backend B200Impl<T>
+ * (include/cpra_b200/B200_Impl.hpp) and the Python bindings both sit on it.
+ *
+ * Conventions (the reference's, include/CPRA_Impl.hpp):
+ *  - Data pointers are device-accessible: memory from cpra_b200_alloc (managed
+ *    by default, like the reference's CudaManagedAllocator,
+ *    include/Allocator.hpp:36-52) or any device allocation.  Complex data is
+ *    interleaved (re, im) in the context's element type.
+ *  - Operators are asynchronous on the context's stream, except
+ *    cpra_b200_converge_error (writes a host pointer) and cpra_b200_sync.
+ *    Consecutive calls that form the reference's difference-map iteration
+ *    (src/CPRA_MKL.cpp:94-110) may be held back and run as one fused launch;
+ *    cpra_b200_sync, cpra_b200_memcpy, cpra_b200_converge_error and any call
+ *    outside that pattern run everything held first.  Read results only after
+ *    cpra_b200_sync (as the reference's drivers do before touching buffers).
+ *  - Element-wise constraints broadcast their plane over the batch:
+ *    element i uses constraint element i % (num / batch_size).
+ *  - Return codes: CPRA_B200_OK, CPRA_B200_EARG for argument errors (the
+ *    reference returns false, include/detail/MKL_Impl.inl:11,34,55,73,89,112),
+ *    CPRA_B200_ECUDA for CUDA runtime failures (the reference throws
+ *    CPRA::cuda_error, include/CUDA_Error_Check.hpp:29-82), CPRA_B200_EUNSUP
+ *    for shapes this backend does not implement.  cpra_b200_last_error()
+ *    returns the calling thread's last message.
+ *  - A context is not thread-safe (neither is the reference's,
+ *    include/CUDA_Impl.cuh:45-46): use one per host thread.
+ */
+#ifndef CPRA_B200_H
+#define CPRA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPRA_B200_OK 0
+#define CPRA_B200_EARG 1
+#define CPRA_B200_ECUDA 2
+#define CPRA_B200_EUNSUP 3
+
+#define CPRA_B200_F32 0
+#define CPRA_B200_F64 1
+
+/* options for cpra_b200_set_option */
+#define CPRA_B200_OPT_FUSION 1     /* 1 (default): fuse recognised iterations; 0: run every call as it comes */
+#define CPRA_B200_OPT_SPACE_MODE 2 /* 0 (default): MKL_Impl.inl:70-84 threshold; 1: CUDA_Impl_Kernel.cuh:16-28 */
+#define CPRA_B200_OPT_DATA_MODE 3  /* 0 (default): MKL_Impl.inl:86-106 (A==0 unconstrained); 1: CUDA kernel */
+#define CPRA_B200_OPT_SEED 4       /* seed of cpra_b200_initialize's counter-based stream */
+#define CPRA_B200_OPT_KERNEL_TIMING 5 /* 1: bracket each fused launch with CUDA events (cpra_b200_kernel_timing) */
+
+typedef struct cpra_b200_ctx cpra_b200_ctx;
+
+/* Replaces CudaImpl(m, n, l, batch_size) (include/CUDA_Impl.cuh:16-52) and the
+ * factory case NewCpraImpl(IMPL_TYPE, m, n, l, batch) (include/Impl_Factory.hpp:14-30).
+ * dtype: CPRA_B200_F32 or CPRA_B200_F64.  Binds the current CUDA device. */
+int cpra_b200_create(cpra_b200_ctx** out, int dtype, uint64_t m, uint64_t n, uint64_t l, uint64_t batch_size);
+/* Replaces ~CudaImpl (include/CUDA_Impl.cuh:105-112). */
+int cpra_b200_destroy(cpra_b200_ctx* ctx);
+const char* cpra_b200_last_error(void);
+/* Number of kernels this library has launched in this process (all contexts). */
+uint64_t cpra_b200_kernels_launched(void);
+int cpra_b200_set_option(cpra_b200_ctx* ctx, int option, int64_t value);
+/* The context's stream as a cudaStream_t (for interoperation). */
+int cpra_b200_get_stream(cpra_b200_ctx* ctx, void** stream);
+
+/* Replaces AllocatorInterface::allocate/deallocate for the CUDA backend
+ * (include/Allocator.hpp:36-52 managed, :18-34 device). managed != 0 gives
+ * host-accessible memory. */
+int cpra_b200_alloc(cpra_b200_ctx* ctx, void** out, uint64_t bytes, int managed);
+int cpra_b200_free(cpra_b200_ctx* ctx, void* ptr);
+
+/* CpraImpl::Initialize (include/CPRA_Impl.hpp:23): num values uniform in [0, 1). */
+int cpra_b200_initialize(cpra_b200_ctx* ctx, void* flat_data, uint64_t num);
+/* CpraImpl::Forward2D / Backward2D (include/CPRA_Impl.hpp:25,27): fftshift, DFT
+ * over the context's m x n planes (batch_size of them), fftshift; Backward2D
+ * scales by 1/(m*n). */
+int cpra_b200_forward2d(cpra_b200_ctx* ctx, void* flat_input);
+int cpra_b200_backward2d(cpra_b200_ctx* ctx, void* flat_input);
+/* CpraImpl::FFTShift2D (include/CPRA_Impl.hpp:29). */
+int cpra_b200_fftshift2d(cpra_b200_ctx* ctx, void* flat_input, uint64_t M, uint64_t N, uint64_t batch);
+/* CpraImpl::Forward3D / Backward3D (include/CPRA_Impl.hpp:31,33) on [l][m][n]
+ * volumes; FFTShift3D (:35). */
+int cpra_b200_forward3d(cpra_b200_ctx* ctx, void* flat_input);
+int cpra_b200_backward3d(cpra_b200_ctx* ctx, void* flat_input);
+int cpra_b200_fftshift3d(cpra_b200_ctx* ctx, void* flat_input, uint64_t M, uint64_t N, uint64_t L, uint64_t batch);
+/* CpraImpl::SpaceConstraint (include/CPRA_Impl.hpp:37). */
+int cpra_b200_space_constraint(cpra_b200_ctx* ctx, void* flat_src, const void* flat_constr, uint64_t num,
+                               uint64_t batch_size);
+/* CpraImpl::DataConstraint, real modulus overload (include/CPRA_Impl.hpp:39). */
+int cpra_b200_data_constraint_real(cpra_b200_ctx* ctx, void* flat_src, const void* flat_constr, uint64_t num,
+                                   uint64_t batch_size);
+/* CpraImpl::DataConstraint, complex overload (include/CPRA_Impl.hpp:41). */
+int cpra_b200_data_constraint_complex(cpra_b200_ctx* ctx, void* flat_src, const void* flat_constr, uint64_t num,
+                                      uint64_t batch_size);
+/* CpraImpl::MergeAddData (include/CPRA_Impl.hpp:45): dst = alpha*src + beta*dst.
+ * alpha and beta are rounded to the context's element type. */
+int cpra_b200_merge_add(cpra_b200_ctx* ctx, const void* flat_src, void* flat_dst, double alpha, double beta,
+                        uint64_t num);
+/* CpraImpl::Normalization (include/CPRA_Impl.hpp:48): x *= 1/norm. */
+int cpra_b200_normalization(cpra_b200_ctx* ctx, void* flat_src, double norm, uint64_t num);
+/* CpraImpl::Real2DTo3DInterpolation (include/CPRA_Impl.hpp:53). */
+int cpra_b200_real2d_to_3d(cpra_b200_ctx* ctx, const void* flat_2d_src, void* flat_3d_dst, const void* angles,
+                           uint64_t m, uint64_t n, uint64_t p, uint64_t l);
+/* CpraImpl::Complex2DTo3DInterpolation (include/CPRA_Impl.hpp:54), a stub in
+ * the reference; here the trilinear gather merge of complex central slices. */
+int cpra_b200_complex2d_to_3d(cpra_b200_ctx* ctx, const void* flat_2d_src, void* flat_3d_dst, const void* angles,
+                              uint64_t m, uint64_t n, uint64_t p, uint64_t l);
+/* CpraImpl::ConvergeError (include/CPRA_Impl.hpp:56; CUDA_Impl.inl:145-172):
+ * old <- new - old over m*n*l*batch elements, then err_host[i] =
+ * ||old_i|| / ||new_i|| over the first m*n elements of member i.  err_host is a
+ * host (or managed) pointer of the element type; the call is synchronous. */
+int cpra_b200_converge_error(cpra_b200_ctx* ctx, void* flat_old, const void* flat_new, void* err_host, uint64_t m,
+                             uint64_t n, uint64_t l, uint64_t batch_size);
+/* CpraImpl::Memcpy (include/CPRA_Impl.hpp:58): asynchronous copy on the stream. */
+int cpra_b200_memcpy(cpra_b200_ctx* ctx, void* dst, const void* src, uint64_t bytes);
+/* CpraImpl::Sync (include/CPRA_Impl.hpp:60). */
+int cpra_b200_sync(cpra_b200_ctx* ctx);
+
+/* Extension: `iters` difference-map iterations of src/CPRA_MKL.cpp:94-110 in one
+ * call, with the driver's coefficients derived from beta
+ * (-1/beta, 1+1/beta), (1/beta, 1-1/beta), (beta, 1), (-beta, 1).  Pattern b of
+ * the batch uses A + b*a_stride and S + b*s_stride (0: one shared plane, the
+ * reference's broadcast).  x, t1, t2 hold `batch` m x n planes. */
+int cpra_b200_dm_iterations(cpra_b200_ctx* ctx, void* x, void* t1, void* t2, const void* A, uint64_t a_stride,
+                            const void* S, uint64_t s_stride, uint64_t batch, double beta, int iters);
+
+/* Extension: the reference's carousel driver ShrinkWrap_CPRA_MKL_Sample
+ * (src/CPRA_MKL.cpp:35-140) on `P` angles of `batch` starts each, x laid out
+ * [P][batch][m][n] (the context's plane size; batch must equal the context's):
+ *   pre_iter iterations on angle 0 (:35-55),
+ *   epi episodes over the angles in Gauss-Seidel order with the carousel mix
+ *   (:59-124), `iters` iterations per angle,
+ *   and, if final_step != 0, the final projection of every angle (:126-140).
+ * A and S hold one m x n plane per angle.  If err_host is not null it receives
+ * the P*batch convergence errors of the last episode (:86-91,113-121, computed
+ * as ConvergeError does); t1/t2/old are context-owned device buffers.
+ * P >= 2 (the mix reads angles p-1 and p+1). */
+int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S, uint64_t P, uint64_t batch,
+                       int epi, int iters, int pre_iter, double beta, int final_step, void* err_host);
+
+/* With CPRA_B200_OPT_KERNEL_TIMING on: total device time (ms) and number of
+ * the fused difference-map launches since the last call, measured with CUDA
+ * events on the context's stream; `pattern_iters` gets the patterns times
+ * iterations they processed.  Synchronises the stream.  Resets the counters. */
+int cpra_b200_kernel_timing(cpra_b200_ctx* ctx, double* ms, uint64_t* launches, uint64_t* pattern_iters);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CPRA_B200_H */

@@ -1,0 +1,436 @@
+"""Parity of the B200 backend with the oracle and the reference build (GPU).
+
+Every operator is called through the C ABI (cpra_b200 -> libcpra_b200.so) on
+seeded inputs and compared with the golden fixtures produced by the
+reference's own MklImpl<T> source (tests/golden/make_golden.py) and with the
+oracle.  Tolerances: integer/permutation/element-wise arithmetic bit-exact;
+one FP32 transform 1e-6 relative L2; difference-map iterations 1e-5 relative
+L2 per iteration (the stated per-iteration bound); FP64 transforms 1e-13.
+"""
+import numpy as np
+import pytest
+
+import cpra_oracle as O
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(GOLDEN / "ref_golden.npz")
+FP32_FFT_TOL = 1e-6
+FP32_DM_TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def tb(cuda):
+    import torch
+    import cpra_b200
+    return torch, cpra_b200
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+# ---- reference unit tests, on the B200 backend ---------------------------------------
+def test_kat_merge_norm_mkl(tb):
+    """test/unitest_mkl.cpp:15-40 on the B200 backend."""
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 1, 1, 1, 1)
+    x = dev(torch, np.full(1000, 10 + 10j, np.complex64))
+    assert impl.MergeAddData(x, x, 0.5, 0.5, 1000)
+    assert impl.Sync()
+    np.testing.assert_array_equal(host(x), np.full(1000, 10 + 10j, np.complex64))
+    assert impl.Normalization(x, 10, 1000)
+    assert impl.Sync()
+    np.testing.assert_array_equal(host(x), np.full(1000, 1 + 1j, np.complex64))
+
+
+def test_kat_merge_norm_cuda_managed(tb):
+    """test/unitest_cuda.cu:13-41: managed memory written and read by the host."""
+    torch, cb = tb
+    import ctypes
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 1, 1, 1, 1)
+    p = impl.alloc(8 * 10, managed=True)
+    buf = (ctypes.c_float * 20).from_address(p)
+    for i in range(20):
+        buf[i] = 10.0
+    assert impl.MergeAddData(p, p, 1, 1, 10)
+    assert impl.Sync()
+    assert all(buf[i] == 20.0 for i in range(20))
+    assert impl.Normalization(p, 20, 10)
+    assert impl.Sync()
+    assert all(buf[i] == 1.0 for i in range(20))
+    assert impl.free(p)
+
+
+def test_kat_initialize(tb):
+    """test/unitest_cuda.cu:4-11 (values in [0, 1]) plus determinism per seed."""
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 1, 1, 1, 1)
+    a = torch.full((1000,), -1.0, device="cuda")
+    assert impl.Initialize(a, 1000) and impl.Sync()
+    v = host(a)
+    assert np.all((v >= 0) & (v <= 1)) and v.std() > 0.2
+    impl2 = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 1, 1, 1, 1)
+    b = torch.zeros(1000, device="cuda")
+    impl2.Initialize(b, 1000); impl2.Sync()
+    np.testing.assert_array_equal(v, host(b))
+    assert not impl.Initialize(a, 0)
+
+
+def test_kat_2d_dft_double(tb):
+    """test/unitest_mkl.cpp:42-71 (10x10 ones, double, 1e-14)."""
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 10, 10, 1, 1, dtype="float64")
+    x = dev(torch, np.ones(100, np.complex128))
+    assert impl.Forward2D(x) and impl.Sync()
+    want = np.zeros(100, np.complex128)
+    want[55] = 100
+    assert np.max(np.abs(host(x) - want)) <= 1e-14
+    assert impl.Backward2D(x) and impl.Sync()
+    assert np.max(np.abs(host(x) - 1)) <= 1e-14
+
+
+# ---- transforms --------------------------------------------------------------------
+@pytest.mark.parametrize("tag,T,M,N,B", [("f32_64", np.float32, 64, 64, 2), ("f64_32", np.float64, 32, 32, 2),
+                                         ("f32_128", np.float32, 128, 128, 1), ("f32_16x8", np.float32, 16, 8, 3)])
+def test_transforms_vs_reference(tb, tag, T, M, N, B):
+    torch, cb = tb
+    tol = FP32_FFT_TOL if T == np.float32 else 1e-13
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B, dtype=np.dtype(T).name)
+    x = G[f"{tag}_x"]
+    y = dev(torch, x)
+    assert impl.Forward2D(y) and impl.Sync()
+    assert O.rel_l2(host(y), G[f"{tag}_fwd"]) < tol
+    y = dev(torch, x)
+    assert impl.Backward2D(y) and impl.Sync()
+    assert O.rel_l2(host(y), G[f"{tag}_bwd"]) < tol
+    y = dev(torch, x)
+    assert impl.FFTShift2D(y, M, N, B) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G[f"{tag}_shift"])
+
+
+@pytest.mark.parametrize("M,N,B", [(256, 256, 2), (512, 512, 1), (64, 256, 2), (160, 160, 1), (2, 4, 3)])
+def test_transforms_other_sizes_vs_oracle(tb, M, N, B):
+    torch, cb = tb
+    rng = np.random.default_rng(M * 1000 + N)
+    x = (rng.standard_normal(M * N * B) + 1j * rng.standard_normal(M * N * B)).astype(np.complex64)
+    o = O.OracleImpl(np.float32, M, N, 1, B)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B)
+    tol = FP32_FFT_TOL * (4 if max(M, N) > 128 else 1) * (20 if (M & (M - 1)) else 1)
+    for fn in ("Forward2D", "Backward2D"):
+        a = x.copy(); getattr(o, fn)(a)
+        y = dev(torch, x)
+        assert getattr(impl, fn)(y) and impl.Sync()
+        assert O.rel_l2(host(y), a) < tol, fn
+
+
+def test_forward_backward_roundtrip_large(tb):
+    """Size-independent property at the full pattern size of the 512^2 case."""
+    torch, cb = tb
+    M = N = 512
+    B = 4
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn(M * N * B, dtype=torch.complex64, device="cuda", generator=g)
+    y = x.clone()
+    assert impl.Forward2D(y) and impl.Backward2D(y) and impl.Sync()
+    assert (torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)).item() < 2e-6
+    # Parseval: ||F x||^2 = MN ||x||^2
+    y = x.clone()
+    impl.Forward2D(y); impl.Sync()
+    r = (torch.linalg.vector_norm(y) ** 2 / (M * N * torch.linalg.vector_norm(x) ** 2)).item()
+    assert abs(r - 1) < 1e-5
+
+
+def test_shift3d_vs_reference(tb):
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 6, 8, 4, 2)
+    y = dev(torch, G["shift3d_x"])
+    assert impl.FFTShift3D(y, 6, 8, 4, 2) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G["shift3d_out"])
+
+
+@pytest.mark.parametrize("T,n,B", [(np.float32, 8, 2), (np.float32, 32, 1), (np.float32, 128, 1),
+                                   (np.float64, 16, 1), (np.float32, 10, 1)])
+def test_transforms_3d_vs_oracle(tb, T, n, B):
+    torch, cb = tb
+    rng = np.random.default_rng(n)
+    C = O.complex_dtype(T)
+    x = (rng.standard_normal(n ** 3 * B) + 1j * rng.standard_normal(n ** 3 * B)).astype(C)
+    o = O.OracleImpl(T, n, n, n, B)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, n, n, n, B, dtype=np.dtype(T).name)
+    tol = (5e-6 if n % 2 == 0 and (n & (n - 1)) == 0 else 2e-5) if T == np.float32 else 1e-13
+    for fn in ("Forward3D", "Backward3D"):
+        a = x.copy(); getattr(o, fn)(a)
+        y = dev(torch, x)
+        assert getattr(impl, fn)(y) and impl.Sync()
+        assert O.rel_l2(host(y), a) < tol, fn
+
+
+# ---- element-wise operators ----------------------------------------------------------
+def test_elementwise_vs_reference(tb):
+    torch, cb = tb
+    M = N = 32
+    B = 3
+    num = M * N * B
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B)
+    x = G["ew_x"]
+    A, S, Cc = dev(torch, G["ew_A"]), dev(torch, G["ew_S"]), dev(torch, G["ew_C"])
+    y = dev(torch, x); assert impl.SpaceConstraint(y, S, num, B) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G["ew_sc"])
+    y = dev(torch, x); assert impl.DataConstraint(y, Cc, num, B) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G["ew_dc_complex"])
+    beta = np.float32(0.9)
+    y = dev(torch, x)
+    assert impl.MergeAddData(dev(torch, G["ew_src"]), y, -1.0 / beta, 1.0 + 1.0 / beta, num) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G["ew_merge"])
+    y = dev(torch, x); assert impl.Normalization(y, 3.0, num) and impl.Sync()
+    np.testing.assert_array_equal(host(y), G["ew_norm3"])
+    y = dev(torch, x); assert impl.DataConstraint(y, A, num, B) and impl.Sync()
+    got, ref = host(y), G["ew_dc_real"]
+    assert np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)) < 4e-7
+    Af = np.tile(G["ew_A"], B)
+    np.testing.assert_array_equal(got[Af == 0], x[Af == 0])
+    assert got[5] == 0
+
+
+def test_elementwise_cuda_modes(tb):
+    """The reference CUDA kernels' semantics behind the mode options
+    (CUDA_Impl_Kernel.cuh:16-38)."""
+    torch, cb = tb
+    M = N = 32
+    B = 3
+    num = M * N * B
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B)
+    assert impl.set_option(cb.OPT_SPACE_MODE, 1) and impl.set_option(cb.OPT_DATA_MODE, 1)
+    o = O.OracleImpl(np.float32, M, N, 1, B, space_mode="cuda")
+    x = G["ew_x"]
+    a = x.copy(); o.SpaceConstraint(a, G["ew_S"], num, B)
+    y = dev(torch, x); impl.SpaceConstraint(y, dev(torch, G["ew_S"]), num, B); impl.Sync()
+    np.testing.assert_array_equal(host(y), a)
+    y = dev(torch, x); impl.DataConstraint(y, dev(torch, G["ew_A"]), num, B); impl.Sync()
+    got = host(y)
+    Af = np.tile(G["ew_A"], B)
+    nz = (Af == 0) & (np.abs(x) > 0)
+    assert np.all(got[nz] == 0)   # no A == 0 skip: polar(0, arg z) = 0
+
+
+def test_argument_errors(tb):
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 8, 8, 1, 2)
+    x = torch.zeros(128, dtype=torch.complex64, device="cuda")
+    s = torch.zeros(64, device="cuda")
+    assert not impl.MergeAddData(x, x, 0.0, 1.0, 128)
+    assert not impl.MergeAddData(x, x, 1.0, 1.0, 0)
+    assert not impl.Normalization(x, 0.0, 128)
+    assert not impl.SpaceConstraint(x, s, 0, 2)
+    assert not impl.SpaceConstraint(x, s, 128, 0)
+    assert not impl.DataConstraint(x, s, 1, 2)      # empty plane
+    assert not impl.FFTShift2D(x, 7, 8, 1)          # odd: not a shift in the reference either
+    assert not impl.Initialize(s, 0)
+    assert impl.Sync()
+    odd = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 7, 8, 1, 1)
+    with pytest.raises(cb.CpraB200Error):
+        odd.Forward2D(x)
+
+
+def test_merge_broadcast_ragged_batch(tb):
+    """num not a multiple of batch: element i uses plane element i % (num/batch)."""
+    torch, cb = tb
+    rng = np.random.default_rng(11)
+    num, batch = 1000, 3
+    x = (rng.standard_normal(num) + 1j * rng.standard_normal(num)).astype(np.complex64)
+    S = rng.uniform(0, 1, num // batch).astype(np.float32)
+    o = O.OracleImpl(np.float32, 1, 1, 1, 1)
+    a = x.copy(); o.SpaceConstraint(a, S, num, batch)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 1, 1, 1, 1)
+    y = dev(torch, x); impl.SpaceConstraint(y, dev(torch, S), num, batch); impl.Sync()
+    np.testing.assert_array_equal(host(y), a)
+
+
+# ---- difference-map iterations --------------------------------------------------------
+def dm_per_call(impl, x, t1, t2, A, S, num, B, beta):
+    """src/CPRA_MKL.cpp:94-110, one interface call at a time."""
+    b = float(np.float32(beta))
+    impl.Forward2D(t1)
+    impl.DataConstraint(t1, A, num, B)
+    impl.Backward2D(t1)
+    impl.MergeAddData(x, t1, -1.0 / b, 1.0 + 1.0 / b, num)
+    impl.SpaceConstraint(t1, S, num, B)
+    impl.SpaceConstraint(t2, S, num, B)
+    impl.MergeAddData(x, t2, 1.0 / b, 1.0 - 1.0 / b, num)
+    impl.Forward2D(t2)
+    impl.DataConstraint(t2, A, num, B)
+    impl.Backward2D(t2)
+    impl.MergeAddData(t1, x, b, 1.0, num)
+    impl.MergeAddData(t2, x, -1.0 * b, 1.0, num)
+
+
+@pytest.mark.parametrize("iters", [1, 5])
+@pytest.mark.parametrize("fusion", [0, 1])
+def test_dm_iterations_vs_reference(tb, iters, fusion):
+    torch, cb = tb
+    M = N = 64
+    B = 2
+    num = M * N * B
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, 1, B)
+    impl.set_option(cb.OPT_FUSION, fusion)
+    x, t1, t2 = (dev(torch, G["dm_x0"]) for _ in range(3))
+    A, S = dev(torch, G["dm_A"]), dev(torch, G["dm_S"])
+    for _ in range(iters):
+        dm_per_call(impl, x, t1, t2, A, S, num, B, 0.9)
+    assert impl.Sync()
+    for name, v in (("x", x), ("t1", t1), ("t2", t2)):
+        assert O.rel_l2(host(v), G[f"dm{iters}_{name}"]) < FP32_DM_TOL * iters, name
+
+
+@pytest.mark.parametrize("L,B,iters", [(128, 3, 4), (64, 5, 3), (32, 2, 6)])
+def test_fused_equals_per_call_bitwise(tb, L, B, iters):
+    """One fused launch, the recorder-fused call stream and the per-call kernels
+    write identical bits."""
+    torch, cb = tb
+    rng = np.random.default_rng(L + B)
+    num = L * L * B
+    amps = (rng.uniform(0, 40, L * L) * (rng.uniform(0, 1, L * L) > 0.1)).astype(np.float32)
+    sup = (rng.uniform(0, 1, L * L) > 0.5).astype(np.float32)
+    x0 = (rng.uniform(0, 1, num) + 1j * rng.uniform(0, 1, num)).astype(np.complex64)
+    outs = []
+    for mode in ("per_call", "recorded", "dm_api"):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        impl.set_option(cb.OPT_FUSION, 0 if mode == "per_call" else 1)
+        x, t1, t2 = (dev(torch, x0) for _ in range(3))
+        A, S = dev(torch, amps), dev(torch, sup)
+        if mode == "dm_api":
+            assert impl.dm_iterations(x, t1, t2, A, S, B, 0.9, iters)
+        else:
+            for _ in range(iters):
+                dm_per_call(impl, x, t1, t2, A, S, num, B, 0.9)
+        assert impl.Sync()
+        outs.append([host(v) for v in (x, t1, t2)])
+    for k in (1, 2):
+        for a, b in zip(outs[0], outs[k]):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_fused_per_pattern_constraints(tb):
+    """dm_iterations with per-pattern modulus/support planes equals running each
+    pattern on its own with a shared plane."""
+    torch, cb = tb
+    L, B, iters = 64, 4, 3
+    rng = np.random.default_rng(5)
+    A = rng.uniform(0, 10, (B, L * L)).astype(np.float32)
+    S = (rng.uniform(0, 1, (B, L * L)) > 0.4).astype(np.float32)
+    x0 = (rng.uniform(0, 1, (B, L * L)) + 1j * rng.uniform(0, 1, (B, L * L))).astype(np.complex64)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    x, t1, t2 = (dev(torch, x0.ravel()) for _ in range(3))
+    assert impl.dm_iterations(x, t1, t2, dev(torch, A.ravel()), dev(torch, S.ravel()), B, 0.9, iters,
+                              a_stride=L * L, s_stride=L * L) and impl.Sync()
+    one = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, 1)
+    for b in range(B):
+        xb, t1b, t2b = (dev(torch, x0[b]) for _ in range(3))
+        one.dm_iterations(xb, t1b, t2b, dev(torch, A[b]), dev(torch, S[b]), 1, 0.9, iters)
+        one.Sync()
+        np.testing.assert_array_equal(host(xb), host(x)[b * L * L:(b + 1) * L * L])
+
+
+def cpra_driver(impl, torch, M, N, L, P, B, A, S, x, epi, iters, pre_iter, beta, err):
+    """src/CPRA_MKL.cpp:35-140 issued through the interface, unchanged."""
+    MNB = M * N * B
+    t1 = torch.empty(MNB, dtype=x.dtype, device=x.device)
+    t2 = torch.empty_like(t1)
+    old = torch.empty_like(t1)
+    nb = MNB * x.element_size()
+    b = float(np.float32(beta))
+    impl.Memcpy(t1, x, nb)
+    impl.Memcpy(t2, x, nb)
+    for _ in range(pre_iter):
+        dm_per_call(impl, x[:MNB], t1, t2, A, S, MNB, B, beta)
+    impl.Sync()
+    for e in range(epi):
+        for p in range(P):
+            xp = x[MNB * p: MNB * (p + 1)]
+            if p == P - 1:
+                impl.MergeAddData(x[MNB * (p - 1): MNB * p], xp, 0.5, 0.5, MNB)
+            elif p == 0:
+                impl.MergeAddData(x[MNB * (p + 1): MNB * (p + 2)], xp, 0.5, 0.5, MNB)
+            else:
+                impl.MergeAddData(x[MNB * (p - 1): MNB * p], xp, 0.5, 0, MNB)
+                impl.MergeAddData(x[MNB * (p + 1): MNB * (p + 2)], xp, 0.5, 1, MNB)
+            impl.Memcpy(t1, xp, nb)
+            impl.Memcpy(t2, xp, nb)
+            Ap, Sp = A[M * N * p: M * N * (p + 1)], S[M * N * p: M * N * (p + 1)]
+            for i in range(iters):
+                last = (i == iters - 1 and e == epi - 1)
+                if last:
+                    impl.Memcpy(old, xp, nb)
+                dm_per_call(impl, xp, t1, t2, Ap, Sp, MNB, B, beta)
+                if last:
+                    impl.Memcpy(t1, xp, nb)
+                    impl.Forward2D(old)
+                    impl.Forward2D(t1)
+                    impl.ConvergeError(old, t1, err[B * p: B * (p + 1)], M, N, 1, B)
+    for p in range(P):
+        xp = x[MNB * p: MNB * (p + 1)]
+        Ap, Sp = A[M * N * p: M * N * (p + 1)], S[M * N * p: M * N * (p + 1)]
+        impl.Memcpy(t1, xp, nb)
+        impl.Forward2D(t1)
+        impl.DataConstraint(t1, Ap, MNB, B)
+        impl.Backward2D(t1)
+        impl.MergeAddData(xp, t1, -1.0 / b, 1.0 + 1.0 / b, MNB)
+        impl.SpaceConstraint(t1, Sp, MNB, B)
+        impl.Memcpy(xp, t1, nb)
+    impl.Sync()
+
+
+@pytest.mark.parametrize("fusion", [0, 1])
+def test_cpra_episode_driver_vs_reference(tb, fusion):
+    torch, cb = tb
+    M, N, L, P, B, epi, it, pre = (int(v) for v in G["cpra_cfg"])
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B)
+    impl.set_option(cb.OPT_FUSION, fusion)
+    x = dev(torch, G["cpra_x0"])
+    err = np.zeros(P * B, np.float32)
+    cpra_driver(impl, torch, M, N, L, P, B, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), x, epi, it, pre,
+                0.9, err)
+    assert O.rel_l2(host(x), G["cpra_x"]) < 1e-3
+    _, err_o = O.cpra_sample(np.float32, M, N, L, P, B, G["cpra_A"], G["cpra_S"], G["cpra_x0"], epi, it, pre, 0.9)
+    assert np.all(np.isfinite(err)) and np.max(np.abs(err - err_o) / np.abs(err_o)) < 1e-2
+
+
+def test_converge_error_vs_oracle(tb):
+    torch, cb = tb
+    rng = np.random.default_rng(2)
+    M, N, L, B = 16, 16, 4, 3
+    n = M * N * L * B
+    old = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    new = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    o = O.OracleImpl(np.float32, M, N, L, B)
+    a = old.copy(); err_o = np.zeros(B, np.float32)
+    o.ConvergeError(a, new, err_o, M, N, L, B)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B)
+    y = dev(torch, old)
+    err = np.zeros(B, np.float32)
+    assert impl.ConvergeError(y, dev(torch, new), err, M, N, L, B)
+    np.testing.assert_array_equal(host(y), a)     # old <- new - old, element-wise exact
+    np.testing.assert_allclose(err, err_o, rtol=1e-6)
+
+
+def test_real2d_to_3d_vs_oracle(tb):
+    torch, cb = tb
+    rng = np.random.default_rng(9)
+    M = N = L = 32
+    P = 12
+    src = rng.uniform(0, 1, P * M * N).astype(np.float32)
+    ang = np.deg2rad(np.linspace(0, 165, P)).astype(np.float32)
+    want = O.real2d_to_3d(np.float32, src, ang, M, N, P, L)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, 1)
+    dst = torch.zeros(M * N * L, device="cuda")
+    assert impl.Real2DTo3DInterpolation(dev(torch, src), dst, dev(torch, ang), M, N, P, L) and impl.Sync()
+    got = host(dst)
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+    assert (want != 0).sum() > 0.05 * want.size
