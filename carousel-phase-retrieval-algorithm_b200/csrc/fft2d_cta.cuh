@@ -24,7 +24,10 @@ struct Plane {
     static constexpr int NT = L * TPL;
     using F = LineFFT<T, L, TPL>;
 
+    static constexpr int TW_ENTRIES = F::TW_ENTRIES;
+
     static constexpr size_t buf_bytes() { return sizeof(Cx<T>) * (size_t)L * LS; }
+    static constexpr size_t tw_bytes() { return sizeof(Cx<T>) * (size_t)TW_ENTRIES; }
 
     // column / row index of output element (j, s) of rank q in split layout
     __device__ __forceinline__ static int split_pos(int q, int j, int s) { return q + TPL * j + R * s; }

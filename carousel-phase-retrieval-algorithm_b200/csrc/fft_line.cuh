@@ -74,13 +74,27 @@ struct LineFFT {
     static_assert(TPL >= 1 && TPL <= 32 && (TPL & (TPL - 1)) == 0, "TPL must be a power of two <= 32");
     static_assert(R <= 32 && R >= TPL, "need TPL <= R <= 32");
 
+    // Twiddle table layout: twq[p * TWS + m] = exp(-2 pi i p m / L) for p < TPL,
+    // m < R.  The row pitch R + 1 puts the TPL ranks' entries for one m on
+    // distinct shared-memory banks.
+    static constexpr int TWS = R + 1;
+    static constexpr int TW_ENTRIES = TPL * TWS;
+    // fill a twiddle table from the full table tw[t] = exp(-2 pi i t / L)
+    __device__ __forceinline__ static void fill_twiddles(Cx<T>* twq, const Cx<T>* __restrict__ tw, int tid,
+                                                         int nthreads) {
+        for (int i = tid; i < TW_ENTRIES; i += nthreads) {
+            const int p = i / TWS, m = i % TWS;
+            twq[i] = (m < R) ? tw[p * m] : Cx<T>{T(1), T(0)};
+        }
+    }
+
     // natural -> split.  scratch: the line's L slots in shared memory, slot u at
     // scratch[u * ss] (may be the storage the values were loaded from; the
-    // group's warp is synchronised before it is overwritten);
-    // twL[t] = exp(-2 pi i t / L).
+    // group's warp is synchronised before it is overwritten); twq: the table
+    // above.
     template <bool INV>
     __device__ __forceinline__ static void natural_to_split(Cx<T> (&v)[R], Cx<T> (&o)[J][TPL], Cx<T>* scratch,
-                                                            int ss, const Cx<T>* twL, int q) {
+                                                            int ss, const Cx<T>* twq, int q) {
         dft_regs<T, R, INV>(v);
         if constexpr (TPL == 1) {
 #pragma unroll
@@ -90,8 +104,7 @@ struct LineFFT {
 #pragma unroll
             for (int m = 0; m < R; ++m) {
                 Cx<T> y = v[brev<R>(m)];
-                const int t = q * m;  // < L
-                if (m != 0) y = INV ? cmulc(y, twL[t]) : cmul(y, twL[t]);
+                if (m != 0) y = INV ? cmulc(y, twq[q * TWS + m]) : cmul(y, twq[q * TWS + m]);
                 scratch[xslot<TPL>(m, q) * ss] = y;
             }
             __syncwarp();
@@ -112,7 +125,7 @@ struct LineFFT {
     // split -> natural (the reverse of natural_to_split's data movement)
     template <bool INV>
     __device__ __forceinline__ static void split_to_natural(Cx<T> (&o)[J][TPL], Cx<T> (&v)[R], Cx<T>* scratch,
-                                                            int ss, const Cx<T>* twL, int q) {
+                                                            int ss, const Cx<T>* twq, int q) {
         if constexpr (TPL == 1) {
 #pragma unroll
             for (int m = 0; m < R; ++m) v[m] = o[m][0];
@@ -129,8 +142,7 @@ struct LineFFT {
                 for (int i = 0; i < TPL; ++i) {
                     const int p = brev<TPL>(i);
                     Cx<T> z = w[i];
-                    const int t = p * m;
-                    if (t != 0) z = INV ? cmulc(z, twL[t]) : cmul(z, twL[t]);
+                    if (p * m != 0) z = INV ? cmulc(z, twq[p * TWS + m]) : cmul(z, twq[p * TWS + m]);
                     scratch[xslot<TPL>(m, p) * ss] = z;
                 }
             }

@@ -36,13 +36,22 @@ struct DmDev {
     int iters, space_mode, data_mode;
 };
 
+// Shared memory of one CTA: the plane buffer, t1's real part (row pitch L + 4
+// so that the 4-byte accesses of a warp's 8 rows fall on distinct banks), the
+// twiddle table, and the support as a bit mask (SpaceConstraint's threshold
+// test, evaluated once per launch: bit set where the value is kept).
 template <int L>
 struct DmPlan {
     using P = Plane<float, L>;
+    static constexpr int T1S = L + 4;
+    static constexpr int MASK_WORDS = L * L / 32;
+    static constexpr size_t t1_bytes() { return sizeof(float) * (size_t)L * T1S; }
     static constexpr size_t smem_bytes() {
-        return P::buf_bytes() + sizeof(float) * (size_t)L * L + sizeof(Cx<float>) * L;
+        return P::buf_bytes() + t1_bytes() + P::tw_bytes() + sizeof(uint32_t) * MASK_WORDS;
     }
 };
+
+__device__ __forceinline__ bool mask_keep(const uint32_t* mask, int idx) { return (mask[idx >> 5] >> (idx & 31)) & 1u; }
 
 // column forward transform, modulus projection, column inverse transform
 template <int L>
@@ -64,18 +73,33 @@ __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>*
 template <int L>
 __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     using P = Plane<float, L>;
+    using D = DmPlan<L>;
+    constexpr int T1S = D::T1S;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
-    float* t1r = reinterpret_cast<float*>(buf + L * P::LS);
-    Cx<float>* tw = reinterpret_cast<Cx<float>*>(t1r + L * L);
+    float* t1r = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::t1_bytes());
+    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::t1_bytes() + P::tw_bytes());
     const int t = threadIdx.x, line = t >> 2, q = t & 3;
-    for (int i = t; i < L; i += P::NT) tw[i] = p.tw[i];
+    P::F::fill_twiddles(tw, p.tw, t, P::NT);
     const size_t base = (size_t)blockIdx.x * L * L;
     Cx<float>* __restrict__ X = p.x + base;
     Cx<float>* __restrict__ T1 = p.t1 + base;
     Cx<float>* __restrict__ T2 = p.t2 + base;
     const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
+    const bool use_mask = (p.space_mode == SPACE_THRESHOLD);
+    if (use_mask) {
+        for (int i = t; i < L * L; i += P::NT) {
+            const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
+            if ((i & 31) == 0) mask[i >> 5] = keep;
+        }
+    }
+    // SpaceConstraint of element idx, from the mask or the support plane
+    auto space = [&](Cx<float> z, int idx) -> Cx<float> {
+        if (use_mask) return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
+        return space_apply(z, S[idx], p.space_mode);
+    };
     __syncthreads();
 
     for (int it = 0; it < p.iters; ++it) {
@@ -87,7 +111,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
             for (int k = 0; k < P::R; ++k) {
                 const int n = q + P::TPL * k;
                 const int idx = line * L + n;
-                const Cx<float> z = (it == 0) ? T1[idx] : Cx<float>{t1r[idx], 0.0f};
+                const Cx<float> z = (it == 0) ? T1[idx] : Cx<float>{t1r[line * T1S + n], 0.0f};
                 v[k] = csign(z, line + n);
             }
             P::template rows_to_buf<false>(v, buf, tw, line, q);
@@ -106,8 +130,8 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
                     const int idx = line * L + f;
                     const Cx<float> val = csign(cscale(o[j][s], p.scale), line + f);
                     Cx<float> m = merge_apply(X[idx], val, p.a1, p.b1);
-                    m = space_apply(m, S[idx], p.space_mode);
-                    t1r[idx] = m.x;
+                    m = space(m, idx);
+                    t1r[line * T1S + f] = m.x;
                     if (last) T1[idx] = m;
                 }
         }
@@ -119,7 +143,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
             for (int k = 0; k < P::R; ++k) {
                 const int n = q + P::TPL * k;
                 const int idx = line * L + n;
-                Cx<float> z = space_apply(T2[idx], S[idx], p.space_mode);
+                Cx<float> z = space(T2[idx], idx);
                 z = merge_apply(X[idx], z, p.a2, p.b2);
                 v[k] = csign(z, line + n);
             }
@@ -139,7 +163,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
                     const int idx = line * L + f;
                     const Cx<float> t2n = csign(cscale(o[j][s], p.scale), line + f);
                     T2[idx] = t2n;
-                    const Cx<float> x1 = merge_apply(Cx<float>{t1r[idx], 0.0f}, X[idx], p.a3, p.b3);
+                    const Cx<float> x1 = merge_apply(Cx<float>{t1r[line * T1S + f], 0.0f}, X[idx], p.a3, p.b3);
                     X[idx] = merge_apply(t2n, x1, p.a4, p.b4);
                 }
         }

@@ -18,30 +18,59 @@ constexpr int EW_THREADS = 256;
 __device__ __forceinline__ uint64_t gtid() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
 
+// Broadcast kernels: blockIdx.x walks the plane, blockIdx.y a chunk of
+// `reps_per_y` repetitions (element i = r * plane + j), so that the grid covers
+// the whole batch while each thread keeps its plane value in a register.
 template <typename T>
-__global__ void k_space(Cx<T>* __restrict__ x, const T* __restrict__ s, uint64_t num, uint64_t plane, int mode) {
+__global__ void k_space(Cx<T>* __restrict__ x, const T* __restrict__ s, uint64_t num, uint64_t plane,
+                        uint64_t reps_per_y, int mode) {
+    const uint64_t r0 = blockIdx.y * reps_per_y;
     for (uint64_t j = gtid(); j < plane; j += gstride()) {
         const T sv = s[j];
-        for (uint64_t i = j; i < num; i += plane) x[i] = space_apply(x[i], sv, mode);
+        for (uint64_t r = r0, i = r0 * plane + j; r < r0 + reps_per_y && i < num; ++r, i += plane)
+            x[i] = space_apply(x[i], sv, mode);
     }
 }
 
 template <typename T>
 __global__ void k_data_real(Cx<T>* __restrict__ x, const T* __restrict__ a, uint64_t num, uint64_t plane,
-                            int mode) {
+                            uint64_t reps_per_y, int mode) {
+    const uint64_t r0 = blockIdx.y * reps_per_y;
     for (uint64_t j = gtid(); j < plane; j += gstride()) {
         const T av = a[j];
-        for (uint64_t i = j; i < num; i += plane) x[i] = data_apply(x[i], av, mode);
+        for (uint64_t r = r0, i = r0 * plane + j; r < r0 + reps_per_y && i < num; ++r, i += plane)
+            x[i] = data_apply(x[i], av, mode);
     }
 }
 
 template <typename T>
-__global__ void k_data_complex(Cx<T>* __restrict__ x, const Cx<T>* __restrict__ c, uint64_t num,
-                               uint64_t plane) {
+__global__ void k_data_complex(Cx<T>* __restrict__ x, const Cx<T>* __restrict__ c, uint64_t num, uint64_t plane,
+                               uint64_t reps_per_y) {
+    const uint64_t r0 = blockIdx.y * reps_per_y;
     for (uint64_t j = gtid(); j < plane; j += gstride()) {
         const Cx<T> cv = c[j];
-        for (uint64_t i = j; i < num; i += plane) x[i] = data_apply_complex(x[i], cv);
+        for (uint64_t r = r0, i = r0 * plane + j; r < r0 + reps_per_y && i < num; ++r, i += plane)
+            x[i] = data_apply_complex(x[i], cv);
     }
+}
+
+// grid of a broadcast kernel: x covers the plane (capped at a wave of CTAs),
+// y splits the repetitions so that the whole grid is about 8 CTAs per SM
+struct BroadcastGrid {
+    dim3 grid;
+    uint64_t reps_per_y;
+};
+BroadcastGrid broadcast_grid(uint64_t num, uint64_t plane) {
+    const uint64_t reps = (num + plane - 1) / plane;
+    const uint64_t target = (uint64_t)sm_count() * 8;
+    const uint64_t gx = ew_grid(plane, EW_THREADS);
+    uint64_t gy = target / gx;
+    if (gy < 1) gy = 1;
+    if (gy > reps) gy = reps;
+    if (gy > 65535) gy = 65535;
+    const uint64_t per = (reps + gy - 1) / gy;
+    gy = (reps + per - 1) / per;
+    return {dim3((unsigned)gx, (unsigned)gy), per};
 }
 
 // src may alias dst exactly (test/unitest_mkl.cpp:33 calls MergeAddData(x, x, ...))
@@ -255,33 +284,38 @@ __global__ void k_complex2d_to_3d(const Cx<T>* __restrict__ src, Cx<T>* __restri
 
 cudaError_t launch_space_constraint(bool dbl, void* x, const void* s, uint64_t num, uint64_t plane, int mode,
                                     cudaStream_t st) {
-    const unsigned g = ew_grid(plane, EW_THREADS);
+    const BroadcastGrid g = broadcast_grid(num, plane);
     if (dbl)
-        k_space<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)s, num, plane, mode);
+        k_space<double><<<g.grid, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)s, num, plane, g.reps_per_y,
+                                                       mode);
     else
-        k_space<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)s, num, plane, mode);
+        k_space<float><<<g.grid, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)s, num, plane, g.reps_per_y, mode);
     count_launches();
     return cudaGetLastError();
 }
 
 cudaError_t launch_data_constraint_real(bool dbl, void* x, const void* a, uint64_t num, uint64_t plane, int mode,
                                         cudaStream_t st) {
-    const unsigned g = ew_grid(plane, EW_THREADS);
+    const BroadcastGrid g = broadcast_grid(num, plane);
     if (dbl)
-        k_data_real<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)a, num, plane, mode);
+        k_data_real<double><<<g.grid, EW_THREADS, 0, st>>>((Cx<double>*)x, (const double*)a, num, plane,
+                                                           g.reps_per_y, mode);
     else
-        k_data_real<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)a, num, plane, mode);
+        k_data_real<float><<<g.grid, EW_THREADS, 0, st>>>((Cx<float>*)x, (const float*)a, num, plane, g.reps_per_y,
+                                                          mode);
     count_launches();
     return cudaGetLastError();
 }
 
 cudaError_t launch_data_constraint_complex(bool dbl, void* x, const void* c, uint64_t num, uint64_t plane,
                                            cudaStream_t st) {
-    const unsigned g = ew_grid(plane, EW_THREADS);
+    const BroadcastGrid g = broadcast_grid(num, plane);
     if (dbl)
-        k_data_complex<double><<<g, EW_THREADS, 0, st>>>((Cx<double>*)x, (const Cx<double>*)c, num, plane);
+        k_data_complex<double><<<g.grid, EW_THREADS, 0, st>>>((Cx<double>*)x, (const Cx<double>*)c, num, plane,
+                                                              g.reps_per_y);
     else
-        k_data_complex<float><<<g, EW_THREADS, 0, st>>>((Cx<float>*)x, (const Cx<float>*)c, num, plane);
+        k_data_complex<float><<<g.grid, EW_THREADS, 0, st>>>((Cx<float>*)x, (const Cx<float>*)c, num, plane,
+                                                             g.reps_per_y);
     count_launches();
     return cudaGetLastError();
 }

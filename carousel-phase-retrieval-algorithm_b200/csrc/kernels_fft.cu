@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, c
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
     Cx<T>* tw = buf + L * P::LS;
     const int t = threadIdx.x, line = t >> 2, q = t & 3;
-    for (int i = t; i < L; i += P::NT) tw[i] = twg[i];
+    P::F::fill_twiddles(tw, twg, t, P::NT);
     Cx<T>* g = data + (size_t)blockIdx.x * L * L;
     __syncthreads();
     if constexpr (!INV) {
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, c
 template <typename T, int L>
 cudaError_t plane_fft(void* x, uint64_t batch, bool inverse, T scale, int s_neg, const void* tw, cudaStream_t st) {
     using P = Plane<T, L>;
-    const size_t smem = P::buf_bytes() + sizeof(Cx<T>) * L;
+    const size_t smem = P::buf_bytes() + P::tw_bytes();
     auto kf = inverse ? k_plane_fft<T, L, true> : k_plane_fft<T, L, false>;
     cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
     Cx<T>* tw = buf + LINES * LSX;
     const int t = threadIdx.x;
-    for (int i = t; i < L; i += AXIS_THREADS) tw[i] = twg[i];
+    F::fill_twiddles(tw, twg, t, AXIS_THREADS);
 
     const uint64_t tile = blockIdx.x;
     const bool contig = (Bi == 1);
@@ -181,7 +181,7 @@ cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shi
                        bool do_scale, const void* tw, cudaStream_t st) {
     constexpr int LINES = AXIS_THREADS / TPL;
     constexpr int PADL = TPL < 16 ? TPL : 0;
-    const size_t smem = sizeof(Cx<T>) * ((size_t)LINES * (L + PADL) + L);
+    const size_t smem = sizeof(Cx<T>) * ((size_t)LINES * (L + PADL) + LineFFT<T, L, TPL>::TW_ENTRIES);
     auto kf = k_axis_fft<T, L, TPL>;
     cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

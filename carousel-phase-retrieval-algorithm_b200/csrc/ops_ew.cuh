@@ -26,17 +26,21 @@ __device__ __forceinline__ Cx<T> space_apply(Cx<T> z, T s, int mode) {
     return {z.x < T(0) ? T(0) : mul_rn(z.x, s), T(0)};
 }
 
+__device__ __forceinline__ float rsqrt_fast(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double rsqrt_fast(double a) { return rsqrt(a); }
+
 // DataConstraint (real modulus): MKL_Impl.inl:86-106.  A == 0 leaves the value
 // unconstrained (DATA_SKIP_ZERO; the CUDA kernel, CUDA_Impl_Kernel.cuh:30-38,
 // has no such skip: DATA_ALWAYS); |z|^2 == 0 leaves it unchanged; otherwise
-// z <- A * z / |z|, which is std::polar(A, std::arg(z)) up to rounding.
+// z <- A * z / |z|, which is std::polar(A, std::arg(z)) up to rounding (the
+// reciprocal square root is CUDA's rsqrt, a few ulp like the reference's
+// atan2/cos/sin; |z|^2 overflowing to infinity takes the hypot route).
 template <typename T>
 __device__ __forceinline__ Cx<T> data_apply(Cx<T> z, T a, int mode) {
     if (mode == DATA_SKIP_ZERO && a == T(0)) return z;
     const T n = add_rn(mul_rn(z.x, z.x), mul_rn(z.y, z.y));
     if (!(n > T(0))) return z;
-    const T mag = isinf(n) ? hypot(z.x, z.y) : sqrt_rn(n);
-    const T r = div_rn(a, mag);
+    const T r = isinf(n) ? div_rn(a, hypot(z.x, z.y)) : mul_rn(a, rsqrt_fast(n));
     return {mul_rn(z.x, r), mul_rn(z.y, r)};
 }
 
