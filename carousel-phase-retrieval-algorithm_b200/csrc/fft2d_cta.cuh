@@ -7,8 +7,10 @@
 //
 // The per-operator transforms (Forward2D / Backward2D) and the fused
 // difference-map kernel are built from the same four steps below, so they
-// perform identical arithmetic:
-//   forward : rows natural->split (to buf), columns natural->split (registers)
+// perform identical arithmetic.  A row thread always sees its row in the
+// split layout (elements q + 4j + R s), both as transform input and output,
+// so the fused kernel can keep a row's values in registers across passes:
+//   forward : rows split->natural (to buf), columns natural->split (registers)
 //   inverse : columns split->natural (to buf), rows natural->split (registers)
 #pragma once
 #include "fft_line.cuh"
@@ -41,6 +43,16 @@ struct Plane {
         for (int j = 0; j < J; ++j)
 #pragma unroll
             for (int s = 0; s < TPL; ++s) buf[r * LS + split_pos(q, j, s)] = o[j][s];
+    }
+
+    // rows: split registers of row r -> transformed row, natural, in buf
+    template <bool INV>
+    __device__ __forceinline__ static void rows_split_to_buf(Cx<T> (&o)[J][TPL], Cx<T>* buf, const Cx<T>* tw, int r,
+                                                             int q) {
+        Cx<T> v[R];
+        F::template split_to_natural<INV>(o, v, buf + r * LS, 1, tw, q);
+#pragma unroll
+        for (int i = 0; i < R; ++i) buf[r * LS + q + TPL * brev<R>(i)] = v[i];
     }
 
     // columns: column c natural in buf -> transformed column in split registers

@@ -3,13 +3,19 @@
 //   t1 <- Forward2D; DataConstraint(A); Backward2D; t1 <- a1*x + b1*t1; SpaceConstraint(S)
 //   t2 <- SpaceConstraint(S); t2 <- a2*x + b2*t2; Forward2D; DataConstraint(A); Backward2D
 //   x  <- a3*t1 + b3*x;  x <- a4*t2 + b4*x
-// as one kernel with one CTA per pattern.  The pattern's plane stays in shared
-// memory for all four transforms; t1 (real after SpaceConstraint) stays in
-// shared memory across iterations; x, t2, A and S are read from global memory
-// (L2) where each step needs them.  The fftshifts cancel in pairs around the
-// modulus step (DataConstraint commutes with the (-1)^(i+j) sign pattern), so
-// only the sign flips on the input of each forward and the output of each
-// inverse transform remain.
+// as one kernel with one CTA per pattern and `iters` iterations per launch.
+//
+// On chip for the whole launch: the plane buffer of the transforms, the
+// modulus plane A and the support (as a bit mask) in shared memory, and t1 --
+// real after SpaceConstraint -- in registers: every row thread reads and
+// writes its row in the same split positions (fft2d_cta.cuh), so the value a
+// thread produces for t1 is the value it consumes next.  Only x and t2 travel
+// through global memory (L2): the second half of each iteration already forms
+// the next iteration's a2*x + b2*S(t2), so each iteration reads x twice and
+// that one plane, and writes x and t2 once.  The fftshifts cancel in pairs
+// around the modulus step (DataConstraint commutes with the (-1)^(i+j) sign
+// pattern), leaving sign flips on the input of each forward and the output of
+// each inverse transform.
 //
 // The arithmetic is the per-operator kernels' arithmetic step for step
 // (Plane<> passes, ops_ew.cuh operators), so one launch with `iters`
@@ -36,18 +42,18 @@ struct DmDev {
     int iters, space_mode, data_mode;
 };
 
-// Shared memory of one CTA: the plane buffer, t1's real part (row pitch L + 4
-// so that the 4-byte accesses of a warp's 8 rows fall on distinct banks), the
-// twiddle table, and the support as a bit mask (SpaceConstraint's threshold
-// test, evaluated once per launch: bit set where the value is kept).
+// Shared memory of one CTA: the plane buffer, A with row pitch L + 8 (the
+// column pass reads A[f][c] for 4 rows f and 8 columns c per warp: distinct
+// banks), the twiddle table, and the support as a bit mask (SpaceConstraint's
+// threshold test evaluated once per launch: bit set where the value is kept).
 template <int L>
 struct DmPlan {
     using P = Plane<float, L>;
-    static constexpr int T1S = L + 4;
+    static constexpr int AP = L + 8;
     static constexpr int MASK_WORDS = L * L / 32;
-    static constexpr size_t t1_bytes() { return sizeof(float) * (size_t)L * T1S; }
+    static constexpr size_t a_bytes() { return sizeof(float) * (size_t)L * AP; }
     static constexpr size_t smem_bytes() {
-        return P::buf_bytes() + t1_bytes() + P::tw_bytes() + sizeof(uint32_t) * MASK_WORDS;
+        return P::buf_bytes() + a_bytes() + P::tw_bytes() + sizeof(uint32_t) * MASK_WORDS;
     }
 };
 
@@ -55,9 +61,10 @@ __device__ __forceinline__ bool mask_keep(const uint32_t* mask, int idx) { retur
 
 // column forward transform, modulus projection, column inverse transform
 template <int L>
-__device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>* tw, const float* __restrict__ A,
-                                                int c, int q, int data_mode) {
+__device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>* tw, const float* As, int c, int q,
+                                                int data_mode) {
     using P = Plane<float, L>;
+    constexpr int AP = DmPlan<L>::AP;
     Cx<float> o[P::J][P::TPL];
     P::template col_from_buf<false>(o, buf, tw, c, q);
 #pragma unroll
@@ -65,7 +72,7 @@ __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>*
 #pragma unroll
         for (int s = 0; s < P::TPL; ++s) {
             const int f = P::split_pos(q, j, s);
-            o[j][s] = data_apply(o[j][s], A[f * L + c], data_mode);
+            o[j][s] = data_apply(o[j][s], As[f * AP + c], data_mode);
         }
     P::template col_to_buf<true>(o, buf, tw, c, q);
 }
@@ -74,12 +81,12 @@ template <int L>
 __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     using P = Plane<float, L>;
     using D = DmPlan<L>;
-    constexpr int T1S = D::T1S;
+    constexpr int J = P::J, TPL = P::TPL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
-    float* t1r = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
-    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::t1_bytes());
-    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::t1_bytes() + P::tw_bytes());
+    float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::a_bytes());
+    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::a_bytes() + P::tw_bytes());
     const int t = threadIdx.x, line = t >> 2, q = t & 3;
     P::F::fill_twiddles(tw, p.tw, t, P::NT);
     const size_t base = (size_t)blockIdx.x * L * L;
@@ -88,6 +95,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     Cx<float>* __restrict__ T2 = p.t2 + base;
     const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
+    for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
     const bool use_mask = (p.space_mode == SPACE_THRESHOLD);
     if (use_mask) {
         for (int i = t; i < L * L; i += P::NT) {
@@ -100,74 +108,64 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
         if (use_mask) return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
         return space_apply(z, S[idx], p.space_mode);
     };
+    // every element this thread touches has index line*L + split_pos(q, j, s)
+    auto at = [&](int j, int s) { return line * L + P::split_pos(q, j, s); };
+    // (-1)^(row + col) is the same for all of them
+    const bool neg = ((line + q) & 1) != 0;
+    auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
+    float t1r[J][TPL];
     __syncthreads();
 
     for (int it = 0; it < p.iters; ++it) {
         const bool last = (it == p.iters - 1);
+        Cx<float> o[J][TPL];
         // ---- t1 <- S( a1*x + b1*Backward2D(DataConstraint(Forward2D(t1))) )
-        {
-            Cx<float> v[P::R];
 #pragma unroll
-            for (int k = 0; k < P::R; ++k) {
-                const int n = q + P::TPL * k;
-                const int idx = line * L + n;
-                const Cx<float> z = (it == 0) ? T1[idx] : Cx<float>{t1r[line * T1S + n], 0.0f};
-                v[k] = csign(z, line + n);
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn((it == 0) ? T1[at(j, s)] : Cx<float>{t1r[j][s], 0.0f});
+        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+        __syncthreads();
+        modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, line, q);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const Cx<float> val = sgn(cscale(o[j][s], p.scale));
+                const Cx<float> m = space(merge_apply(X[at(j, s)], val, p.a1, p.b1), at(j, s));
+                t1r[j][s] = m.x;
+                if (last) T1[at(j, s)] = m;
             }
-            P::template rows_to_buf<false>(v, buf, tw, line, q);
-        }
-        __syncthreads();
-        modulus_columns<L>(buf, tw, A, line, q, p.data_mode);
-        __syncthreads();
-        {
-            Cx<float> o[P::J][P::TPL];
-            P::template row_from_buf<true>(o, buf, tw, line, q);
-#pragma unroll
-            for (int j = 0; j < P::J; ++j)
-#pragma unroll
-                for (int s = 0; s < P::TPL; ++s) {
-                    const int f = P::split_pos(q, j, s);
-                    const int idx = line * L + f;
-                    const Cx<float> val = csign(cscale(o[j][s], p.scale), line + f);
-                    Cx<float> m = merge_apply(X[idx], val, p.a1, p.b1);
-                    m = space(m, idx);
-                    t1r[line * T1S + f] = m.x;
-                    if (last) T1[idx] = m;
-                }
-        }
-        __syncthreads();
         // ---- t2 <- Backward2D(DataConstraint(Forward2D( a2*x + b2*S(t2) )))
-        {
-            Cx<float> v[P::R];
+        // (from the second iteration on, T2 already holds a2*x + b2*S(t2))
 #pragma unroll
-            for (int k = 0; k < P::R; ++k) {
-                const int n = q + P::TPL * k;
-                const int idx = line * L + n;
-                Cx<float> z = space(T2[idx], idx);
-                z = merge_apply(X[idx], z, p.a2, p.b2);
-                v[k] = csign(z, line + n);
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                Cx<float> z = T2[at(j, s)];
+                if (it == 0) z = merge_apply(X[at(j, s)], space(z, at(j, s)), p.a2, p.b2);
+                o[j][s] = sgn(z);
             }
-            P::template rows_to_buf<false>(v, buf, tw, line, q);
-        }
+        __syncthreads();  // every thread is done reading the plane buffer
+        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
         __syncthreads();
-        modulus_columns<L>(buf, tw, A, line, q, p.data_mode);
+        modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
         __syncthreads();
-        {
-            Cx<float> o[P::J][P::TPL];
-            P::template row_from_buf<true>(o, buf, tw, line, q);
+        P::template row_from_buf<true>(o, buf, tw, line, q);
 #pragma unroll
-            for (int j = 0; j < P::J; ++j)
+        for (int j = 0; j < J; ++j)
 #pragma unroll
-                for (int s = 0; s < P::TPL; ++s) {
-                    const int f = P::split_pos(q, j, s);
-                    const int idx = line * L + f;
-                    const Cx<float> t2n = csign(cscale(o[j][s], p.scale), line + f);
-                    T2[idx] = t2n;
-                    const Cx<float> x1 = merge_apply(Cx<float>{t1r[line * T1S + f], 0.0f}, X[idx], p.a3, p.b3);
-                    X[idx] = merge_apply(t2n, x1, p.a4, p.b4);
-                }
-        }
-        __syncthreads();
+            for (int s = 0; s < TPL; ++s) {
+                const int idx = at(j, s);
+                const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
+                const Cx<float> x1 = merge_apply(Cx<float>{t1r[j][s], 0.0f}, X[idx], p.a3, p.b3);
+                const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
+                X[idx] = xn;
+                T2[idx] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+            }
+        __syncthreads();  // every thread is done reading the plane buffer
     }
 }
 
@@ -182,7 +180,7 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     d.S = (const float*)a.S;
     d.s_stride = a.s_stride;
     d.tw = (const Cx<float>*)tw;
-    d.scale = 1.0f / (float)(a.M * a.N);
+    d.scale = 1.0f / (float)(a.M * a.N);  // DFTI_BACKWARD_SCALE (include/MKL_Impl.hpp:40)
     d.a1 = (float)a.c.a1;
     d.b1 = (float)a.c.b1;
     d.a2 = (float)a.c.a2;

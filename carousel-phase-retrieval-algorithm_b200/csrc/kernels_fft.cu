@@ -32,15 +32,16 @@ __global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, c
     Cx<T>* g = data + (size_t)blockIdx.x * L * L;
     __syncthreads();
     if constexpr (!INV) {
-        Cx<T> v[P::R];
-#pragma unroll
-        for (int k = 0; k < P::R; ++k) {
-            const int n = q + P::TPL * k;
-            v[k] = csign(g[line * L + n], line + n);
-        }
-        P::template rows_to_buf<false>(v, buf, tw, line, q);
-        __syncthreads();
         Cx<T> o[P::J][P::TPL];
+#pragma unroll
+        for (int j = 0; j < P::J; ++j)
+#pragma unroll
+            for (int s = 0; s < P::TPL; ++s) {
+                const int n = P::split_pos(q, j, s);
+                o[j][s] = csign(g[line * L + n], line + n);
+            }
+        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+        __syncthreads();
         P::template col_from_buf<false>(o, buf, tw, line, q);
 #pragma unroll
         for (int j = 0; j < P::J; ++j)
