@@ -257,8 +257,13 @@ int exec_op(cpra_b200_ctx* c, const Op& op) {
     return fail(CPRA_B200_EARG, "unknown operator");
 }
 
-int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters) {
+int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_NONE, const void* xprev = nullptr,
+                 const void* xnext = nullptr, int init_from_x = 0) {
     DmArgs a;
+    a.mix = mix;
+    a.xprev = xprev;
+    a.xnext = xnext;
+    a.init_from_x = init_from_x;
     a.x = p.x;
     a.t1 = p.t1;
     a.t2 = p.t2;
@@ -903,23 +908,34 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
     // Step B (:59-124)
     for (int e = 0; e < epi; ++e) {
         for (uint64_t p = 0; p < P; ++p) {
-            if (p == P - 1) {
-                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
-            } else if (p == 0) {
-                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
-            } else {
-                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.0, MNB, c->stream), "cpra_run");
-                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 1.0, MNB, c->stream), "cpra_run");
-            }
-            CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
-            CPRA_CHECK_CUDA(copy(t2, xp(p)), "cpra_run");
             const DmPattern pat = pattern(p, p);
             const bool err_here = want_err && e == epi - 1;
-            if (!err_here) {
-                if ((r = dm_any(c, pat, iters))) return r;
-                continue;
+            const bool fused = iters > 0 && dm_fused_supported(c->dbl, c->m, c->n);
+            if (fused && (!err_here || iters >= 2)) {
+                // carousel mix, t1 = t2 = x and the angle's iterations (all but
+                // the last one on an error-reporting angle) in one launch
+                const int mix = (p == 0) ? MIX_FIRST : (p == P - 1) ? MIX_LAST : MIX_MIDDLE;
+                if ((r = launch_fused(c, pat, err_here ? iters - 1 : iters, mix, p > 0 ? xp(p - 1) : nullptr,
+                                      p + 1 < P ? xp(p + 1) : nullptr, 1)))
+                    return r;
+                if (!err_here) continue;
+            } else {
+                if (p == P - 1) {
+                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
+                } else if (p == 0) {
+                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
+                } else {
+                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.0, MNB, c->stream), "cpra_run");
+                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 1.0, MNB, c->stream), "cpra_run");
+                }
+                CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+                CPRA_CHECK_CUDA(copy(t2, xp(p)), "cpra_run");
+                if (!err_here) {
+                    if ((r = dm_any(c, pat, iters))) return r;
+                    continue;
+                }
+                if ((r = dm_any(c, pat, iters - 1))) return r;
             }
-            if ((r = dm_any(c, pat, iters - 1))) return r;
             CPRA_CHECK_CUDA(copy(old, xp(p)), "cpra_run");
             if ((r = dm_any(c, pat, 1))) return r;
             CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");

@@ -69,10 +69,18 @@ struct DmCoef {
     double a3, b3;  // t1 -> x
     double a4, b4;  // t2 -> x
 };
+// Carousel mix applied to x before the first iteration (src/CPRA_MKL.cpp:64-76):
+// MIX_FIRST x <- 0.5*next + 0.5*x; MIX_LAST x <- 0.5*prev + 0.5*x;
+// MIX_MIDDLE x <- 0.5*prev + 0*x, then x <- 0.5*next + 1*x.
+enum MixMode : int { MIX_NONE = 0, MIX_FIRST = 1, MIX_LAST = 2, MIX_MIDDLE = 3 };
 struct DmArgs {
     void* x;
     void* t1;
     void* t2;
+    const void* xprev = nullptr;  // neighbouring angles' planes for the mix
+    const void* xnext = nullptr;
+    int mix = MIX_NONE;
+    int init_from_x = 0;  // t1 = t2 = x (after the mix) instead of the t1/t2 buffers' contents
     const void* A;       // modulus constraint plane(s)
     uint64_t a_stride;   // elements between consecutive patterns' planes (0: shared)
     const void* S;       // support plane(s)

@@ -32,6 +32,9 @@ struct DmDev {
     Cx<float>* x;
     Cx<float>* t1;
     Cx<float>* t2;
+    const Cx<float>* xprev;
+    const Cx<float>* xnext;
+    int mix, init_from_x;
     const float* A;
     uint64_t a_stride;
     const float* S;
@@ -93,6 +96,8 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     Cx<float>* __restrict__ X = p.x + base;
     Cx<float>* __restrict__ T1 = p.t1 + base;
     Cx<float>* __restrict__ T2 = p.t2 + base;
+    const Cx<float>* __restrict__ XP = p.xprev + (p.xprev ? base : 0);
+    const Cx<float>* __restrict__ XN = p.xnext + (p.xnext ? base : 0);
     const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
     for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
@@ -116,56 +121,96 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     float t1r[J][TPL];
     __syncthreads();
 
+    // Both halves of an iteration run through one loop body, so each transform
+    // pass exists once in the binary (the fully unrolled passes are large and
+    // duplicating them overflows the instruction cache).  Between halves no
+    // block barrier is needed: a row's slots in the plane buffer are only
+    // touched by the four threads of that row, which share a warp.
     for (int it = 0; it < p.iters; ++it) {
         const bool last = (it == p.iters - 1);
-        Cx<float> o[J][TPL];
-        // ---- t1 <- S( a1*x + b1*Backward2D(DataConstraint(Forward2D(t1))) )
+#pragma unroll 1
+        for (int ph = 0; ph < 2; ++ph) {
+            Cx<float> o[J][TPL];
+            if (ph == 0) {
+                // t1 <- S( a1*x + b1*Backward2D(DataConstraint(Forward2D(t1))) )
+                if (it > 0) {
 #pragma unroll
-        for (int j = 0; j < J; ++j)
+                    for (int j = 0; j < J; ++j)
 #pragma unroll
-            for (int s = 0; s < TPL; ++s) o[j][s] = sgn((it == 0) ? T1[at(j, s)] : Cx<float>{t1r[j][s], 0.0f});
-        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
-        __syncthreads();
-        modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
-        __syncthreads();
-        P::template row_from_buf<true>(o, buf, tw, line, q);
+                        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(Cx<float>{t1r[j][s], 0.0f});
+                } else if (!p.init_from_x) {
 #pragma unroll
-        for (int j = 0; j < J; ++j)
+                    for (int j = 0; j < J; ++j)
 #pragma unroll
-            for (int s = 0; s < TPL; ++s) {
-                const Cx<float> val = sgn(cscale(o[j][s], p.scale));
-                const Cx<float> m = space(merge_apply(X[at(j, s)], val, p.a1, p.b1), at(j, s));
-                t1r[j][s] = m.x;
-                if (last) T1[at(j, s)] = m;
+                        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(T1[at(j, s)]);
+                } else {
+                    // the angle's start: carousel mix of x, then t1 = t2 = x (:64-80)
+#pragma unroll
+                    for (int j = 0; j < J; ++j)
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) {
+                            const int idx = at(j, s);
+                            Cx<float> xv = X[idx];
+                            if (p.mix == MIX_FIRST) {
+                                xv = merge_apply(XN[idx], xv, 0.5f, 0.5f);
+                            } else if (p.mix == MIX_LAST) {
+                                xv = merge_apply(XP[idx], xv, 0.5f, 0.5f);
+                            } else if (p.mix == MIX_MIDDLE) {
+                                xv = merge_apply(XP[idx], xv, 0.5f, 0.0f);
+                                xv = merge_apply(XN[idx], xv, 0.5f, 1.0f);
+                            }
+                            if (p.mix != MIX_NONE) X[idx] = xv;
+                            o[j][s] = sgn(xv);
+                        }
+                }
+            } else {
+                // t2 <- Backward2D(DataConstraint(Forward2D( a2*x + b2*S(t2) )))
+                // (from the second iteration on, T2 already holds a2*x + b2*S(t2);
+                // on an angle's start t2 = x)
+#pragma unroll
+                for (int j = 0; j < J; ++j)
+#pragma unroll
+                    for (int s = 0; s < TPL; ++s) {
+                        const int idx = at(j, s);
+                        Cx<float> z;
+                        if (it > 0) {
+                            z = T2[idx];
+                        } else {
+                            const Cx<float> xv = X[idx];
+                            z = merge_apply(xv, space(p.init_from_x ? xv : T2[idx], idx), p.a2, p.b2);
+                        }
+                        o[j][s] = sgn(z);
+                    }
             }
-        // ---- t2 <- Backward2D(DataConstraint(Forward2D( a2*x + b2*S(t2) )))
-        // (from the second iteration on, T2 already holds a2*x + b2*S(t2))
+            P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+            __syncthreads();
+            modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
+            __syncthreads();
+            P::template row_from_buf<true>(o, buf, tw, line, q);
+            if (ph == 0) {
 #pragma unroll
-        for (int j = 0; j < J; ++j)
+                for (int j = 0; j < J; ++j)
 #pragma unroll
-            for (int s = 0; s < TPL; ++s) {
-                Cx<float> z = T2[at(j, s)];
-                if (it == 0) z = merge_apply(X[at(j, s)], space(z, at(j, s)), p.a2, p.b2);
-                o[j][s] = sgn(z);
+                    for (int s = 0; s < TPL; ++s) {
+                        const Cx<float> val = sgn(cscale(o[j][s], p.scale));
+                        const Cx<float> m = space(merge_apply(X[at(j, s)], val, p.a1, p.b1), at(j, s));
+                        t1r[j][s] = m.x;
+                        if (last) T1[at(j, s)] = m;
+                    }
+            } else {
+#pragma unroll
+                for (int j = 0; j < J; ++j)
+#pragma unroll
+                    for (int s = 0; s < TPL; ++s) {
+                        const int idx = at(j, s);
+                        const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
+                        const Cx<float> x1 = merge_apply(Cx<float>{t1r[j][s], 0.0f}, X[idx], p.a3, p.b3);
+                        const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
+                        X[idx] = xn;
+                        T2[idx] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                    }
             }
-        __syncthreads();  // every thread is done reading the plane buffer
-        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
-        __syncthreads();
-        modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
-        __syncthreads();
-        P::template row_from_buf<true>(o, buf, tw, line, q);
-#pragma unroll
-        for (int j = 0; j < J; ++j)
-#pragma unroll
-            for (int s = 0; s < TPL; ++s) {
-                const int idx = at(j, s);
-                const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
-                const Cx<float> x1 = merge_apply(Cx<float>{t1r[j][s], 0.0f}, X[idx], p.a3, p.b3);
-                const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
-                X[idx] = xn;
-                T2[idx] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
-            }
-        __syncthreads();  // every thread is done reading the plane buffer
+        }
     }
 }
 
@@ -175,6 +220,10 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     d.x = (Cx<float>*)a.x;
     d.t1 = (Cx<float>*)a.t1;
     d.t2 = (Cx<float>*)a.t2;
+    d.xprev = (const Cx<float>*)a.xprev;
+    d.xnext = (const Cx<float>*)a.xnext;
+    d.mix = a.mix;
+    d.init_from_x = a.init_from_x;
     d.A = (const float*)a.A;
     d.a_stride = a.a_stride;
     d.S = (const float*)a.S;

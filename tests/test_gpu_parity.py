@@ -434,3 +434,39 @@ def test_real2d_to_3d_vs_oracle(tb):
     got = host(dst)
     np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
     assert (want != 0).sum() > 0.05 * want.size
+
+
+@pytest.mark.parametrize("L,P,B,epi,it,pre", [(32, 4, 2, 2, 3, 4), (128, 5, 3, 2, 3, 2), (64, 3, 2, 1, 1, 0)])
+def test_cpra_run_equals_driver_bitwise(tb, L, P, B, epi, it, pre):
+    """cpra_b200_cpra_run (carousel mix and t1 = t2 = x fused into each angle's
+    launch) writes the same bits as the reference driver's call sequence issued
+    one call at a time (src/CPRA_MKL.cpp:35-140)."""
+    torch, cb = tb
+    rng = np.random.default_rng(L * 7 + P)
+    A = (rng.uniform(0, 30, (P, L * L)) * (rng.uniform(0, 1, (P, L * L)) > 0.1)).astype(np.float32)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(np.float32)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(np.complex64)
+    Ad, Sd = dev(torch, A.ravel()), dev(torch, S.ravel())
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    ref.set_option(cb.OPT_FUSION, 0)
+    xr = dev(torch, x0)
+    err_r = np.zeros(P * B, np.float32)
+    cpra_driver(ref, torch, L, L, 1, P, B, Ad, Sd, xr, epi, it, pre, 0.9, err_r)
+    run = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    xf = dev(torch, x0)
+    err_f = np.zeros(P * B, np.float32)
+    assert run.cpra_run(xf, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=True, err=err_f) and run.Sync()
+    np.testing.assert_array_equal(host(xf), host(xr))
+    np.testing.assert_array_equal(err_f, err_r)
+
+
+def test_cpra_run_vs_reference(tb):
+    torch, cb = tb
+    M, N, L, P, B, epi, it, pre = (int(v) for v in G["cpra_cfg"])
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B)
+    x = dev(torch, G["cpra_x0"])
+    assert impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), P, B, epi, it, pre, 0.9) and impl.Sync()
+    assert O.rel_l2(host(x), G["cpra_x"]) < 1e-3
+    # argument errors of the driver entry
+    assert not impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), 1, B, epi, it, pre, 0.9)
+    assert not impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), P, B + 1, epi, it, pre, 0.9)
