@@ -470,3 +470,39 @@ def test_cpra_run_vs_reference(tb):
     # argument errors of the driver entry
     assert not impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), 1, B, epi, it, pre, 0.9)
     assert not impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), P, B + 1, epi, it, pre, 0.9)
+
+
+def _drop_in_binaries():
+    from conftest import REPO
+    d = REPO / "tests" / "cpp" / "_bin"
+    return [p for p in (d / "drop_in_ref_iface", d / "drop_in_standalone") if p.exists()]
+
+
+@pytest.mark.parametrize("exe", _drop_in_binaries(), ids=lambda p: p.name)
+def test_cpp_drop_in_driver(tb, tmp_path, exe):
+    """The reference driver's call sequence through CpraImpl<float>* on
+    B200Impl<float> (C++, managed memory, recorder fusion on) writes the same
+    bits as the per-call Python driver, and matches the reference build."""
+    import subprocess
+    torch, cb = tb
+    M, N, L, P, B, epi, it, pre = (int(v) for v in G["cpra_cfg"])
+    (tmp_path / "cfg.txt").write_text(f"{M} {N} {L} {P} {B} {epi} {it} {pre} 0.9\n")
+    G["cpra_A"].astype(np.float32).tofile(tmp_path / "A.f32")
+    G["cpra_S"].astype(np.float32).tofile(tmp_path / "S.f32")
+    G["cpra_x0"].astype(np.complex64).tofile(tmp_path / "x0.c64")
+    out = tmp_path / "out.bin"
+    r = subprocess.run([str(exe), str(tmp_path), str(out)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(out, dtype=np.uint8)
+    nx = P * B * M * N
+    x = raw[: nx * 8].view(np.complex64)
+    err = raw[nx * 8:].view(np.float32)
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B)
+    ref.set_option(cb.OPT_FUSION, 0)
+    xr = dev(torch, G["cpra_x0"])
+    err_r = np.zeros(P * B, np.float32)
+    cpra_driver(ref, torch, M, N, L, P, B, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), xr, epi, it, pre, 0.9,
+                err_r)
+    np.testing.assert_array_equal(x, host(xr))
+    np.testing.assert_array_equal(err, err_r)
+    assert O.rel_l2(x, G["cpra_x"]) < 1e-3
