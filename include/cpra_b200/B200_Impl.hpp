@@ -8,9 +8,11 @@
 // CUDA failures throw CPRA::b200_error, a std::runtime_error like the
 // reference's CPRA::cuda_error (include/CUDA_Error_Check.hpp:29).
 //
-// Inside the reference tree, include it after "CPRA_Impl.hpp" (it includes it
-// itself) and register it as INTEGRATION.md describes.  Without the reference
-// tree, define CPRA_B200_STANDALONE to use this project's restatement of the
+// Inside the reference tree it includes the tree's own "CPRA_Impl.hpp"; a
+// backend is registered there by adding B200 to enum IMPL_TYPE
+// (include/CPRA_Impl.hpp:15) and a case returning NewB200Impl<T> to
+// NewCpraImpl (include/Impl_Factory.hpp:14-30).  Without the reference tree,
+// define CPRA_B200_STANDALONE to use this project's restatement of the
 // interface (cpra_impl_interface.hpp).
 #pragma once
 #include <complex>

@@ -14,7 +14,7 @@ from conftest import GOLDEN
 G = np.load(GOLDEN / "ref_golden.npz")
 
 FP32_FFT_TOL = 1e-6   # one FP32 transform vs the float64-rounded oracle
-FP32_DM_TOL = 1e-5    # the north-star per-iteration bound
+FP32_DM_TOL = 1e-5    # per difference-map iteration, relative L2
 
 
 # ---- test/unitest_mkl.cpp -------------------------------------------------------
