@@ -78,6 +78,8 @@ _SIGS = {
     "cpra_b200_cpra_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                            C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "cpra_b200_converge_error_noalloc": [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
+                                        + [C.c_void_p],
 }
 
 

@@ -56,6 +56,12 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+void cpra_b200::set_last_error(const std::string& msg) { g_last_error = msg; }
+
+namespace {
+
 int cuda_fail(cudaError_t e, const char* where) {
     return fail(CPRA_B200_ECUDA, std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }

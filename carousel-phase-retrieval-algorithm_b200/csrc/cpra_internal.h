@@ -4,6 +4,7 @@
 // the C-ABI layer before any launcher is called.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 namespace cpra_b200 {
@@ -11,6 +12,8 @@ namespace cpra_b200 {
 // Process-wide count of kernels this library has launched (every launcher
 // calls count_launches after its launches; read by cpra_b200_kernels_launched).
 void count_launches(uint64_t n = 1);
+// Sets the calling thread's message returned by cpra_b200_last_error().
+void set_last_error(const std::string& msg);
 
 // ---- transforms (kernels_fft.cu) ---------------------------------------
 // Shifted 2D transform of `batch` MxN planes in place:

@@ -150,6 +150,25 @@ int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S
  * iterations they processed.  Synchronises the stream.  Resets the counters. */
 int cpra_b200_kernel_timing(cpra_b200_ctx* ctx, double* ms, uint64_t* launches, uint64_t* pattern_iters);
 
+/* ConvergeError for callers that cannot allocate GPU memory while they run
+ * (device memory already reserved by another allocator or pool, loops that
+ * must not be stalled by cudaFree's device-wide synchronisation, runs that must
+ * not fail halfway on an allocation).  No counterpart in the reference: it is
+ * the reference's ConvergeError (include/CPRA_Impl.hpp:56, CUDA_Impl.inl:145-172)
+ * with the same result as cpra_b200_converge_error, but it needs no context and
+ * calls no allocator: its partial sums live in a fixed scratch array compiled
+ * into the library (a file-scope __device__ array of about 264 KiB that every
+ * GPU loading the library holds until exit).  batch_size is limited to
+ * CPRA_B200_NOALLOC_MAX_BATCH; larger batches are refused with CPRA_B200_EARG.
+ * The scratch address is looked up on the first call made on each device, so
+ * make that first call before any stream capture.  All calls share the scratch:
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * dtype is CPRA_B200_F32 or CPRA_B200_F64; stream is a cudaStream_t (NULL: the
+ * default stream); the call returns after err_host is written. */
+#define CPRA_B200_NOALLOC_MAX_BATCH 256
+int cpra_b200_converge_error_noalloc(int dtype, void* flat_old, const void* flat_new, void* err_host, uint64_t m,
+                                     uint64_t n, uint64_t l, uint64_t batch_size, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
