@@ -12,7 +12,7 @@
 // iterations, the per-operator kernels for a partial prefix -- and then runs
 // normally.  Program order is preserved, so results are the per-operator
 // results; the fused kernel performs the same arithmetic.
-#include "../../include/cpra_b200.h"
+#include "cpra_b200.h"
 #include "cpra_internal.h"
 
 #include <atomic>

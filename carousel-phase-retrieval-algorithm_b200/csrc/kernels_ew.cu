@@ -212,7 +212,7 @@ __global__ void k_real2d_to_3d(const T* __restrict__ src, T* __restrict__ dst, c
         const int64_t y = (int64_t)(idx % M);
         const int64_t x = (int64_t)((idx / M) % N);
         const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
-        const int64_t j = L / 2 - z, k = x - N / 2, l = M / 2 - y;
+        const int64_t j = L / 2 - z, l = M / 2 - y;
         double acc = 0.0, wsum = 0.0;
         for (int64_t p = 0; p < P; ++p) {
             const double a = (double)ang[p];

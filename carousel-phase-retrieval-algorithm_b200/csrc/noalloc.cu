@@ -20,7 +20,7 @@
 // full by every call before they are read, so nothing has to start at zero, but
 // two calls that overlap on the GPU (on different streams, or from different
 // host threads) race on it.
-#include "../../include/cpra_b200.h"
+#include "cpra_b200.h"
 #include "cpra_internal.h"
 
 #include <cmath>
