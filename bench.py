@@ -166,15 +166,17 @@ def cpu_reference_rate(A, S, size, iters, seconds, threads):
 
 # ---------------------------------------------------------------------------
 # plain per-operator path on the GPU: torch.fft (cuFFT) + element-wise kernels
-# in the reference CUDA backend's call order (CUDA_Impl.inl), for comparison
+# in the reference CUDA backend's call order (CUDA_Impl.inl), for comparison;
+# both paths run the same iterations from the same start so that their
+# R-factors can be compared
 # ---------------------------------------------------------------------------
-def per_op_rate(torch, A, S, B, size, iters, reps=2):
+def per_op_compare(torch, cpra_b200, A, S, B, size, iters, reps=2):
     dev = torch.device("cuda")
     M = N = size
     Ad = torch.from_numpy(A[0]).to(dev)
     Sd = torch.from_numpy(S[0]).to(dev)
-    x = torch.rand(B, M, N, dtype=torch.complex64, device=dev)
-    t1, t2 = x.clone(), x.clone()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x0 = torch.rand(B, M, N, dtype=torch.complex64, device=dev, generator=g)
     beta = float(np.float32(0.9))
 
     def fwd(t):
@@ -205,8 +207,10 @@ def per_op_rate(torch, A, S, B, size, iters, reps=2):
         x = -beta * t2 + x
         return x, t1, t2
 
+    x, t1, t2 = x0.clone(), x0.clone(), x0.clone()
     for _ in range(3):
         x, t1, t2 = it(x, t1, t2)
+    x, t1, t2 = x0.clone(), x0.clone(), x0.clone()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -215,7 +219,19 @@ def per_op_rate(torch, A, S, B, size, iters, reps=2):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return B * reps * iters / (ms / 1e3)
+    impl = cpra_b200.B200Impl(M, N, 1, B)
+    xf, t1f, t2f = x0.clone().ravel(), x0.clone().ravel(), x0.clone().ravel()
+    impl.dm_iterations(xf, t1f, t2f, Ad, Sd, B, 0.9, reps * iters)
+    impl.Sync()
+    r_perop = impl.rfactor(x.contiguous().ravel(), Ad, B)
+    r_fused = impl.rfactor(xf, Ad, B)
+    impl.close()
+    return {"value": B * reps * iters / (ms / 1e3), "unit": METRIC,
+            "impl": "torch.fft (cuFFT) + torch element-wise kernels, reference CUDA backend call order, same GPU",
+            "iterations_compared": reps * iters,
+            "rfactor_median_per_op": float(np.median(r_perop)),
+            "rfactor_median_b200_same_start": float(np.median(r_fused)),
+            "rfactor_max_rel_diff": float(np.max(np.abs(r_perop - r_fused) / r_perop))}
 
 
 def read_traffic(kernel_key):
@@ -404,6 +420,8 @@ def main():
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
                 "share_of_step": kms / ms}
 
+    # R-factor of the result of the last step, per pattern, against its angle's modulus
+    rf = np.concatenate([impl.rfactor(x[p * B * MN:(p + 1) * B * MN], A[p * MN:(p + 1) * MN], B) for p in range(P)])
     result = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -411,13 +429,14 @@ def main():
         "config": workload_config(a, ws), "e2e": e2e, "gpu_launches": int(launches), "roofline": roof,
         "clocks": clocks,
         "convergence_error_median": float(np.median(err)),
+        "rfactor": {"median": float(np.median(rf)), "p10": float(np.percentile(rf, 10)),
+                    "p90": float(np.percentile(rf, 90)), "patterns": int(rf.size),
+                    "definition": "sum | |Forward2D(x)| - A | / sum A, float64"},
     }
 
     if rank == 0 and ws == 1 and not a.no_extras:
         try:
-            result["per_op_path"] = {"value": per_op_rate(torch, d["A"], d["S"], B, M, IT), "unit": METRIC,
-                                     "impl": "torch.fft (cuFFT) + torch element-wise kernels, reference CUDA "
-                                             "backend call order, same GPU"}
+            result["per_op_path"] = per_op_compare(torch, cpra_b200, d["A"], d["S"], B, M, IT)
         except Exception as ex:  # the comparison must not sink the line
             result["per_op_path"] = {"error": str(ex)[:200]}
         try:

@@ -78,6 +78,7 @@ _SIGS = {
     "cpra_b200_cpra_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                            C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "cpra_b200_rfactor": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p],
     "cpra_b200_converge_error_noalloc": [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                         + [C.c_void_p],
 }
@@ -265,6 +266,15 @@ class B200Impl:
         return _check(lib().cpra_b200_cpra_run(self._h, _addr(x), _addr(A), _addr(S), int(P), int(batch), int(epi),
                                                int(iters), int(pre_iter), float(beta), 1 if final_step else 0,
                                                _host_addr(err) if err is not None else 0), "cpra_run")
+
+    def rfactor(self, x, A, batch, a_stride=0):
+        """R-factor per pattern, sum | |Forward2D(x_b)| - A_b | / sum A_b in
+        double (project-defined metric); returns a numpy float64 array."""
+        import numpy as np
+        out = np.zeros(int(batch), np.float64)
+        _check(lib().cpra_b200_rfactor(self._h, _addr(x), _addr(A), int(a_stride), int(batch),
+                                       out.ctypes.data_as(C.c_void_p)), "rfactor")
+        return out
 
     def kernel_timing(self):
         """(ms, launches, pattern_iterations) of the fused launches timed since

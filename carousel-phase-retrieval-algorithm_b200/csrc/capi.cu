@@ -815,6 +815,38 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* c, void* x, void* t1, void* t2, const
     return CPRA_B200_OK;
 }
 
+int cpra_b200_rfactor(cpra_b200_ctx* c, const void* x, const void* A, uint64_t a_stride, uint64_t batch,
+                      double* r_host) {
+    CTX_OR_RETURN(c);
+    if (!x || !A || !r_host) return fail(CPRA_B200_EARG, "rfactor: null pointer");
+    if (batch == 0) return fail(CPRA_B200_EARG, "rfactor: batch must be positive");
+    if (batch > 65535) return fail(CPRA_B200_EUNSUP, "rfactor: batch above 65535");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "rfactor: each plane size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t plane = c->plane();
+    // the spectra go to a work buffer (the input stays untouched); the
+    // non-power-of-two transform path needs a second one of the same size
+    const uint64_t bytes = batch * plane * c->csize();
+    r = ensure_work(c, 2 * bytes);
+    if (r) return r;
+    r = ensure_reduction(c, batch);
+    if (r) return r;
+    char* F = static_cast<char*>(c->work);
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(F, x, bytes, cudaMemcpyDefault, c->stream), "rfactor");
+    CPRA_CHECK_CUDA(launch_fft2d(c->dbl, F, c->m, c->n, batch, false, 1.0, twiddles(c, c->m), twiddles(c, c->n),
+                                 F + bytes, c->stream),
+                    "rfactor");
+    CPRA_CHECK_CUDA(launch_rfactor_sums(c->dbl, F, A, a_stride, plane, batch, c->partials, c->sums, c->stream),
+                    "rfactor");
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost, c->stream),
+                    "rfactor");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "rfactor");
+    for (uint64_t i = 0; i < batch; ++i) r_host[i] = c->host_sums[2 * i] / c->host_sums[2 * i + 1];
+    return CPRA_B200_OK;
+}
+
 int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, uint64_t* pattern_iters) {
     CTX_OR_RETURN(c);
     int r = flush(c);

@@ -58,6 +58,12 @@ cudaError_t launch_uniform(bool dbl, void* x, uint64_t num, uint64_t seed, uint6
 constexpr int CONVERGE_BLOCKS = 64;
 cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t span, uint64_t stride,
                               uint64_t batch, double* partials, double* sums, cudaStream_t st);
+// R-factor sums of `batch` centred spectra F (the Forward2D of each pattern):
+// sums[2b] = sum_px | |F_b| - A_b |, sums[2b+1] = sum_px A_b, in double, with
+// A_b = A + b * a_stride; deterministic two-level reduction through `partials`
+// (>= batch * CONVERGE_BLOCKS * 2 doubles).
+cudaError_t launch_rfactor_sums(bool dbl, const void* F, const void* A, uint64_t a_stride, uint64_t plane,
+                                uint64_t batch, double* partials, double* sums, cudaStream_t st);
 cudaError_t launch_real2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m, uint64_t n,
                                 uint64_t p, uint64_t l, cudaStream_t st);
 cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m,

@@ -192,6 +192,40 @@ __global__ void k_norm_final(const double* __restrict__ partials, double* __rest
     }
 }
 
+// R-factor stage 1: grid (CONVERGE_BLOCKS, batch); |F| and the differences in
+// double, one partial pair per block
+template <typename T>
+__global__ void k_rfactor_partial(const Cx<T>* __restrict__ F, const T* __restrict__ A, uint64_t a_stride,
+                                  uint64_t plane, double* __restrict__ partials) {
+    __shared__ double sd[EW_THREADS], sa[EW_THREADS];
+    const uint64_t b = blockIdx.y;
+    const Cx<T>* f = F + b * plane;
+    const T* a = A + b * a_stride;
+    double accD = 0.0, accA = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)EW_THREADS + threadIdx.x; i < plane;
+         i += (uint64_t)gridDim.x * EW_THREADS) {
+        const Cx<T> z = f[i];
+        const double mag = sqrt(fma((double)z.x, (double)z.x, (double)z.y * (double)z.y));
+        const double av = (double)a[i];
+        accD += fabs(mag - av);
+        accA += av;
+    }
+    sd[threadIdx.x] = accD;
+    sa[threadIdx.x] = accA;
+    __syncthreads();
+    for (int h = EW_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            sd[threadIdx.x] += sd[threadIdx.x + h];
+            sa[threadIdx.x] += sa[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partials[(b * gridDim.x + blockIdx.x) * 2 + 0] = sd[0];
+        partials[(b * gridDim.x + blockIdx.x) * 2 + 1] = sa[0];
+    }
+}
+
 // C round(): halfway cases away from zero
 __device__ __forceinline__ double round_away(double v) { return round(v); }
 
@@ -389,6 +423,24 @@ cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t s
     else
         k_norm_partial<float><<<grid, EW_THREADS, 0, st>>>((const Cx<float>*)a, (const Cx<float>*)b, span, stride,
                                                            partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_norm_final<<<ew_grid(batch, 64), 64, 0, st>>>(partials, sums, batch, CONVERGE_BLOCKS);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rfactor_sums(bool dbl, const void* F, const void* A, uint64_t a_stride, uint64_t plane,
+                                uint64_t batch, double* partials, double* sums, cudaStream_t st) {
+    if (batch == 0) return cudaSuccess;
+    if (batch > 65535) return cudaErrorInvalidValue;
+    dim3 grid(CONVERGE_BLOCKS, (unsigned)batch);
+    if (dbl)
+        k_rfactor_partial<double><<<grid, EW_THREADS, 0, st>>>((const Cx<double>*)F, (const double*)A, a_stride, plane,
+                                                               partials);
+    else
+        k_rfactor_partial<float><<<grid, EW_THREADS, 0, st>>>((const Cx<float>*)F, (const float*)A, a_stride, plane,
+                                                              partials);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_norm_final<<<ew_grid(batch, 64), 64, 0, st>>>(partials, sums, batch, CONVERGE_BLOCKS);

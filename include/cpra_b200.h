@@ -144,6 +144,14 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* ctx, void* x, void* t1, void* t2, con
 int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S, uint64_t P, uint64_t batch,
                        int epi, int iters, int pre_iter, double beta, int final_step, void* err_host);
 
+/* Extension (project-defined, no counterpart in the reference): R-factor of
+ * `batch` patterns x ([batch][m][n], the context's plane size) against their
+ * modulus planes A (pattern b uses A + b*a_stride; 0: one shared plane):
+ *   r_host[b] = sum | |Forward2D(x_b)| - A_b | / sum A_b,
+ * with |F| and both sums in double.  x is not modified.  Synchronous. */
+int cpra_b200_rfactor(cpra_b200_ctx* ctx, const void* x, const void* A, uint64_t a_stride, uint64_t batch,
+                      double* r_host);
+
 /* With CPRA_B200_OPT_KERNEL_TIMING on: total device time (ms) and number of
  * the fused difference-map launches since the last call, measured with CUDA
  * events on the context's stream; `pattern_iters` gets the patterns times

@@ -425,3 +425,67 @@ def real2d_to_3d(T, src, angles, m, n, p, l):
     nz = wt > 0
     out[nz] = (acc[nz] / wt[nz]).astype(T)
     return out
+
+
+def rfactor(x, A, M, N, batch, a_stride=0):
+    """Project-defined R-factor (no counterpart in the reference, whose only
+    metric is ConvergeError): for pattern b,
+        R_b = sum | |Forward2D(x_b)| - A_b | / sum A_b
+    with Forward2D the reference's shift-DFT-shift (MKL_Impl.inl:128-139),
+    evaluated here entirely in float64."""
+    x = np.asarray(x).astype(np.complex128).ravel()[: batch * M * N].copy()
+    impl = OracleImpl(np.float64, M, N, 1, batch)
+    impl.Forward2D(x)
+    F = np.abs(x.reshape(batch, M * N))
+    A = np.asarray(A, np.float64).ravel()
+    out = np.zeros(batch)
+    for b in range(batch):
+        a = A[b * a_stride: b * a_stride + M * N]
+        out[b] = np.abs(F[b] - a).sum() / a.sum()
+    return out
+
+
+def complex2d_to_3d(T, src, angles, m, n, p, l):
+    """Project-defined trilinear gather merge of P complex central slices into
+    a [L][N][M] volume (the reference's Complex2DTo3DInterpolation is a stub,
+    include/CUDA_Impl.cuh:89), in the geometry of the real merge
+    (CUDA_Impl_Kernel.cuh:68-119): voxel (z, x, y) is the point
+    (j, k, l) = (L/2 - z, x - N/2, M/2 - y); slice p at angle a sees it at
+    in-plane row yIn = M/2 - (j sin a + l cos a), column xIn = x, and at
+    distance d = j cos a - l sin a from its plane.  Slices with |d| < 1 add
+    (1 - |d|) times the slice sampled linearly in yIn; the voxel is the
+    weight-normalised sum (0 where nothing reaches it)."""
+    T = np.dtype(T).type
+    M, N, P, L = int(m), int(n), int(p), int(l)
+    src = np.asarray(src).astype(np.complex128).reshape(P, N, M)
+    ang = np.asarray(angles, T).astype(np.float64)[:P]
+    z, x, y = np.meshgrid(np.arange(L), np.arange(N), np.arange(M), indexing="ij")
+    j = (L // 2 - z).astype(np.float64)
+    ll = (M // 2 - y).astype(np.float64)
+    acc = np.zeros((L, N, M), np.complex128)
+    wsum = np.zeros((L, N, M))
+    for q in range(P):
+        sa, ca = np.sin(ang[q]), np.cos(ang[q])
+        d = j * ca - ll * sa
+        wd = 1.0 - np.abs(d)
+        yin = (M // 2) - (j * sa + ll * ca)
+        y0 = np.floor(yin)
+        fy = yin - y0
+        y0 = y0.astype(np.int64)
+        s = np.zeros_like(acc)
+        sw = np.zeros_like(wsum)
+        for dy in (0, 1):
+            yy = y0 + dy
+            wy = fy if dy else 1.0 - fy
+            ok = (yy >= 0) & (yy < M) & (wy != 0)
+            v = np.zeros_like(acc)
+            v[ok] = src[q, x[ok], yy[ok]]
+            s += np.where(ok, wy, 0.0) * v
+            sw += np.where(ok, wy, 0.0)
+        use = (wd > 0) & (sw > 0)
+        acc[use] += wd[use] * s[use]
+        wsum[use] += wd[use] * sw[use]
+    out = np.zeros((L, N, M), np.complex128)
+    nz = wsum > 0
+    out[nz] = acc[nz] / wsum[nz]
+    return out.astype(complex_dtype(T)).ravel()

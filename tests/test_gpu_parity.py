@@ -506,3 +506,35 @@ def test_cpp_drop_in_driver(tb, tmp_path, exe):
     np.testing.assert_array_equal(x, host(xr))
     np.testing.assert_array_equal(err, err_r)
     assert O.rel_l2(x, G["cpra_x"]) < 1e-3
+
+
+@pytest.mark.parametrize("L,B,shared", [(128, 3, True), (64, 4, False), (160, 2, False)])
+def test_rfactor_vs_oracle(tb, L, B, shared):
+    """Project-defined R-factor (FP64 sums on the GPU) against the float64 oracle."""
+    torch, cb = tb
+    rng = np.random.default_rng(L + B)
+    x = (rng.standard_normal(B * L * L) + 1j * rng.standard_normal(B * L * L)).astype(np.complex64)
+    A = rng.uniform(0, 20, (1 if shared else B) * L * L).astype(np.float32)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    xd = dev(torch, x)
+    r = impl.rfactor(xd, dev(torch, A), B, a_stride=0 if shared else L * L)
+    want = O.rfactor(x, A, L, L, B, a_stride=0 if shared else L * L)
+    np.testing.assert_allclose(r, want, rtol=1e-5)
+    np.testing.assert_array_equal(host(xd), x)   # input untouched
+
+
+def test_complex_merge_vs_oracle(tb):
+    """Project-defined trilinear gather merge (Complex2DTo3DInterpolation)."""
+    torch, cb = tb
+    rng = np.random.default_rng(21)
+    M = N = L = 24
+    P = 10
+    src = (rng.standard_normal(P * M * N) + 1j * rng.standard_normal(P * M * N)).astype(np.complex64)
+    ang = np.deg2rad(np.linspace(0, 170, P) + 0.37).astype(np.float32)
+    want = O.complex2d_to_3d(np.float32, src, ang, M, N, P, L)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, 1)
+    dst = torch.zeros(M * N * L, dtype=torch.complex64, device="cuda")
+    assert impl.Complex2DTo3DInterpolation(dev(torch, src), dst, dev(torch, ang), M, N, P, L) and impl.Sync()
+    got = host(dst)
+    assert O.rel_l2(got, want) < 1e-6
+    assert (np.abs(want) > 0).mean() > 0.3
