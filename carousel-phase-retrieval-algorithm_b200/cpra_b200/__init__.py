@@ -78,6 +78,9 @@ _SIGS = {
     "cpra_b200_cpra_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                            C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+    "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
+                                 C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                 C.c_void_p],
     "cpra_b200_rfactor": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p],
     "cpra_b200_converge_error_noalloc": [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                         + [C.c_void_p],
@@ -266,6 +269,20 @@ class B200Impl:
         return _check(lib().cpra_b200_cpra_run(self._h, _addr(x), _addr(A), _addr(S), int(P), int(batch), int(epi),
                                                int(iters), int(pre_iter), float(beta), 1 if final_step else 0,
                                                _host_addr(err) if err is not None else 0), "cpra_run")
+
+    def hio_shrinkwrap(self, x, A, S, batch, iters, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5,
+                       threshold=0.1, positivity=False, a_stride=None, s_stride=None, estimate=None) -> bool:
+        """Fused HIO iterations with shrinkwrap support updates (project-defined);
+        per-pattern planes by default (stride m*n); ``estimate`` (optional
+        device buffer) receives S (.) P_M(x) of the final x."""
+        plane = self.m * self.n
+        a_stride = plane if a_stride is None else a_stride
+        s_stride = plane if s_stride is None else s_stride
+        return _check(lib().cpra_b200_hio_shrinkwrap(self._h, _addr(x), _addr(A), int(a_stride), _addr(S),
+                                                     int(s_stride), int(batch), int(iters), float(beta),
+                                                     int(sw_every), float(sigma_start), float(sigma_end),
+                                                     float(threshold), 1 if positivity else 0, _addr(estimate)),
+                      "hio_shrinkwrap")
 
     def rfactor(self, x, A, batch, a_stride=0):
         """R-factor per pattern, sum | |Forward2D(x_b)| - A_b | / sum A_b in

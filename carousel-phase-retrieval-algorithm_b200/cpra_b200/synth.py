@@ -104,3 +104,23 @@ def r_factor(x_plane, A_plane):
     F = np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(np.asarray(x_plane, np.complex128))))
     A = np.asarray(A_plane, np.float64)
     return float(np.abs(np.abs(F) - A).sum() / max(A.sum(), 1e-300))
+
+
+def autocorrelation_support(A, frac=0.04):
+    """Initial support from the autocorrelation |IFFT(A^2)| > frac * max, per
+    plane ([count][n][n] float32 of 0/1): the autocorrelation's extent bounds
+    twice the object's."""
+    A = np.asarray(A, np.float64)
+    ac = np.abs(np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(A * A, axes=(-2, -1))), axes=(-2, -1)))
+    mx = ac.reshape(ac.shape[0], -1).max(axis=1)[:, None, None]
+    return (ac > frac * mx).astype(np.float32)
+
+
+def random_phase_start(A, seed=0):
+    """Starting guesses: the centred inverse transform of A with uniform random
+    phases, [count][n][n] complex64 (seeded)."""
+    rng = np.random.default_rng(seed)
+    A = np.asarray(A, np.float64)
+    ph = np.exp(2j * np.pi * rng.uniform(size=A.shape))
+    x = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(A * ph, axes=(-2, -1))), axes=(-2, -1))
+    return x.astype(np.complex64)

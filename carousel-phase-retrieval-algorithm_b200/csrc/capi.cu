@@ -15,6 +15,7 @@
 #include "cpra_b200.h"
 #include "cpra_internal.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -153,6 +154,9 @@ struct cpra_b200_ctx {
     double* err_sums = nullptr;
     double* host_err = nullptr;
     uint64_t err_cap = 0;
+    // shrinkwrap blur tables
+    void* blur = nullptr;
+    uint64_t blur_bytes = 0;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -521,6 +525,7 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     if (c->sums) cudaFree(c->sums);
     if (c->host_sums) cudaFreeHost(c->host_sums);
     if (c->drv) cudaFree(c->drv);
+    if (c->blur) cudaFree(c->blur);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -844,6 +849,82 @@ int cpra_b200_rfactor(cpra_b200_ctx* c, const void* x, const void* A, uint64_t a
                     "rfactor");
     CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "rfactor");
     for (uint64_t i = 0; i < batch; ++i) r_host[i] = c->host_sums[2 * i] / c->host_sums[2 * i + 1];
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t a_stride, void* S, uint64_t s_stride,
+                             uint64_t batch, int iters, double beta, int sw_every, double sigma_start,
+                             double sigma_end, double threshold, int positivity, void* estimate) {
+    CTX_OR_RETURN(c);
+    if (!x || !A || !S) return fail(CPRA_B200_EARG, "hio_shrinkwrap: null pointer");
+    if (batch == 0 || iters < 0) return fail(CPRA_B200_EARG, "hio_shrinkwrap: batch must be positive, iters >= 0");
+    if (!hio_fused_supported(c->dbl, c->m, c->n))
+        return fail(CPRA_B200_EUNSUP, "hio_shrinkwrap: needs float and square 32, 64 or 128 planes");
+    const int updates = (sw_every > 0) ? iters / sw_every : 0;
+    if (updates > 0 && s_stride < c->plane())
+        return fail(CPRA_B200_EARG, "hio_shrinkwrap: shrinkwrap updates each pattern's support: s_stride >= m*n");
+    if (updates > 0 && !(sigma_start > 0.0 && sigma_end > 0.0))
+        return fail(CPRA_B200_EARG, "hio_shrinkwrap: sigma must be positive");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    if (iters == 0 && !estimate) return CPRA_B200_OK;
+    const uint64_t L = c->m;
+    if (updates > 0) {
+        // g(f) for a normalised periodic Gaussian of width sigma: its DFT, real
+        // and even; entry i is the value at the frequency (i + L/2) mod L that
+        // the sign-modulated transform puts at index i
+        std::vector<float> tab((size_t)updates * L);
+        for (int k = 0; k < updates; ++k) {
+            const double sg = updates > 1 ? sigma_start + (sigma_end - sigma_start) * k / (updates - 1) : sigma_start;
+            std::vector<double> g(L);
+            double sum = 0.0;
+            for (uint64_t n = 0; n < L; ++n) {
+                const double d = (double)std::min<uint64_t>(n, L - n);
+                g[n] = std::exp(-d * d / (2.0 * sg * sg));
+                sum += g[n];
+            }
+            for (uint64_t f = 0; f < L; ++f) {
+                const uint64_t fu = (f + L / 2) % L;
+                double acc = 0.0;
+                for (uint64_t n = 0; n < L; ++n) {
+                    const uint64_t ph = (n * fu) % L;
+                    acc += g[n] * std::cos(2.0 * 3.141592653589793238462643383279502884 * (double)ph / (double)L);
+                }
+                tab[(size_t)k * L + f] = (float)(acc / sum);
+            }
+        }
+        const uint64_t bytes = tab.size() * sizeof(float);
+        if (c->blur_bytes < bytes) {
+            if (c->blur) {
+                cudaStreamSynchronize(c->stream);
+                cudaFree(c->blur);
+                c->blur = nullptr;
+                c->blur_bytes = 0;
+            }
+            CPRA_CHECK_CUDA(cudaMalloc(&c->blur, bytes), "cudaMalloc(blur tables)");
+            c->blur_bytes = bytes;
+        }
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(c->blur, tab.data(), bytes, cudaMemcpyHostToDevice, c->stream), "hio_shrinkwrap");
+        CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "hio_shrinkwrap");  // tab leaves scope
+    }
+    HioArgs a;
+    a.x = x;
+    a.estimate = estimate;
+    a.A = A;
+    a.a_stride = a_stride;
+    a.S = S;
+    a.s_stride = s_stride;
+    a.blur = updates > 0 ? c->blur : nullptr;
+    a.M = c->m;
+    a.N = c->n;
+    a.batch = batch;
+    a.iters = iters;
+    a.sw_every = updates > 0 ? sw_every : 0;
+    a.positivity = positivity ? 1 : 0;
+    a.data_mode = c->data_mode;
+    a.beta = c->round_t(beta);
+    a.threshold = threshold;
+    CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "hio_shrinkwrap");
     return CPRA_B200_OK;
 }
 

@@ -103,4 +103,20 @@ struct DmArgs {
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
 
+// ---- fused HIO + shrinkwrap iterations (kernels_hio.cu) -----------------------
+struct HioArgs {
+    void* x;            // [batch][M][N] complex, in/out
+    void* estimate;     // optional [batch][M][N] complex out: S (.) P_M(x) after the last iteration
+    const void* A;      // modulus planes, pattern b at A + b*a_stride
+    uint64_t a_stride;
+    void* S;            // support planes (float, > 0.5 = inside), in/out, pattern b at S + b*s_stride
+    uint64_t s_stride;
+    const void* blur;   // [updates][M] Gaussian transfer tables (device), or null
+    uint64_t M, N, batch;
+    int iters, sw_every, positivity, data_mode;
+    double beta, threshold;
+};
+bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N);
+cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st);
+
 }  // namespace cpra_b200

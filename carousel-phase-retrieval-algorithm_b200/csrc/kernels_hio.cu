@@ -1,0 +1,236 @@
+// Hybrid input-output iterations with shrinkwrap support updates, fused: one
+// CTA per pattern, `iters` iterations per launch.  Project-defined (the
+// reference's "shrinkwrap" drivers run the difference map with a fixed
+// support, src/CPRA_MKL.cpp:94-110; it has no HIO and no support update).
+//
+// Per iteration, with y = P_M(x) = Backward2D(DataConstraint(Forward2D(x)))
+// (the reference operators' composition, modulus plane A):
+//   x <- y            where the pixel is in the support (and Re y >= 0 with
+//                     positivity on),
+//   x <- x - beta*y   elsewhere.
+// Every `sw_every` iterations the support becomes { v > threshold * max v }
+// with v = |x| blurred by a normalised periodic Gaussian (circular
+// convolution, evaluated exactly through the DFT: the separable transfer
+// function g(f_row) g(f_col) is a table per update, sigma moving linearly from
+// sigma_start at the first update to sigma_end at the last).
+//
+// On chip: the plane buffer of the transforms, A and the support (a bit mask)
+// in shared memory; x goes through L2 (read twice, written once per iteration).
+// Optionally the kernel also writes the estimate S (.) P_M(x) of the final x.
+#include "cpra_internal.h"
+#include "fft2d_cta.cuh"
+#include "ops_ew.cuh"
+
+namespace cpra_b200 {
+
+namespace {
+
+struct HioDev {
+    Cx<float>* x;
+    Cx<float>* est;  // optional: S (.) P_M(x) after the last iteration
+    const float* A;
+    uint64_t a_stride;
+    float* S;
+    uint64_t s_stride;
+    const Cx<float>* tw;
+    const float* blur;  // [updates][L]: g at the frequency of each (D-shifted) row/column index
+    float scale, beta, thresh;
+    int iters, sw_every, positivity, data_mode;
+};
+
+template <int L>
+struct HioPlan {
+    using P = Plane<float, L>;
+    static constexpr int AP = L + 8;
+    static constexpr int MASK_WORDS = L * L / 32;
+    static constexpr int WARPS = P::NT / 32;
+    static constexpr size_t a_bytes() { return sizeof(float) * (size_t)L * AP; }
+    static constexpr size_t smem_bytes() {
+        return P::buf_bytes() + a_bytes() + P::tw_bytes() + sizeof(uint32_t) * MASK_WORDS + sizeof(float) * L +
+               sizeof(float) * WARPS;
+    }
+};
+
+// column forward transform, a per-frequency operation, column inverse transform
+template <int L, class Op>
+__device__ __forceinline__ void spectral_columns(Cx<float>* buf, const Cx<float>* tw, int c, int q, Op op) {
+    using P = Plane<float, L>;
+    Cx<float> o[P::J][P::TPL];
+    P::template col_from_buf<false>(o, buf, tw, c, q);
+#pragma unroll
+    for (int j = 0; j < P::J; ++j)
+#pragma unroll
+        for (int s = 0; s < P::TPL; ++s) o[j][s] = op(o[j][s], P::split_pos(q, j, s), c);
+    P::template col_to_buf<true>(o, buf, tw, c, q);
+}
+
+template <int L>
+__global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
+    using P = Plane<float, L>;
+    using H = HioPlan<L>;
+    constexpr int J = P::J, TPL = P::TPL, AP = H::AP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
+    float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + H::a_bytes());
+    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + H::a_bytes() + P::tw_bytes());
+    float* gt = reinterpret_cast<float*>(mask + H::MASK_WORDS);
+    float* red = gt + L;
+    const int t = threadIdx.x, line = t >> 2, q = t & 3;
+    P::F::fill_twiddles(tw, p.tw, t, P::NT);
+    Cx<float>* __restrict__ X = p.x + (size_t)blockIdx.x * L * L;
+    const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
+    float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
+    for (int i = t; i < L * L; i += P::NT) As[(i / L) * AP + (i % L)] = A[i];
+    for (int i = t; i < L * L; i += P::NT) {
+        const unsigned in = __ballot_sync(0xffffffffu, S[i] > 0.5f);
+        if ((i & 31) == 0) mask[i >> 5] = in;
+    }
+    auto at = [&](int j, int s) { return line * L + P::split_pos(q, j, s); };
+    const bool neg = ((line + q) & 1) != 0;
+    auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
+    auto inside = [&](int idx) { return (mask[idx >> 5] >> (idx & 31)) & 1u; };
+    const int dmode = p.data_mode;
+    __syncthreads();
+
+    int update = 0;
+    for (int it = 0; it < p.iters; ++it) {
+        Cx<float> o[J][TPL];
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(X[at(j, s)]);
+        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+        __syncthreads();
+        spectral_columns<L>(buf, tw, line, q, [&](Cx<float> z, int f, int c) {
+            return data_apply(z, As[f * AP + c], dmode);
+        });
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, line, q);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const int idx = at(j, s);
+                const Cx<float> y = sgn(cscale(o[j][s], p.scale));
+                const Cx<float> xv = X[idx];
+                const bool keep = inside(idx) && (!p.positivity || y.x >= 0.0f);
+                const Cx<float> xn = keep ? y : merge_apply(y, xv, -p.beta, 1.0f);
+                X[idx] = xn;
+                o[j][s] = xn;
+            }
+        if (p.sw_every <= 0 || !p.blur || (it + 1) % p.sw_every != 0) continue;
+
+        // ---- shrinkwrap: v = |x| blurred, support = { v > thresh * max v } ----
+        if (t < L) gt[t] = p.blur[(size_t)update * L + t];
+        ++update;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const Cx<float> z = o[j][s];
+                o[j][s] = sgn(Cx<float>{sqrtf(fmaf(z.x, z.x, z.y * z.y)), 0.0f});
+            }
+        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+        __syncthreads();
+        spectral_columns<L>(buf, tw, line, q, [&](Cx<float> z, int f, int c) { return cscale(z, gt[f] * gt[c]); });
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, line, q);
+        float vmax = -INFINITY;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                o[j][s].x = sgn(cscale(o[j][s], p.scale)).x;
+                vmax = fmaxf(vmax, o[j][s].x);
+            }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+        if ((t & 31) == 0) red[t >> 5] = vmax;
+        __syncthreads();
+        float m = red[0];
+        for (int w = 1; w < H::WARPS; ++w) m = fmaxf(m, red[w]);
+        const float thr = p.thresh * m;
+        // this row's mask words are read and written only by its four threads
+        for (int w = q; w < L / 32; w += TPL) mask[line * (L / 32) + w] = 0u;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s)
+                if (o[j][s].x > thr) {
+                    const int idx = at(j, s);
+                    atomicOr(&mask[idx >> 5], 1u << (idx & 31));
+                }
+        __syncthreads();  // red[] is reused by the next update
+    }
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) S[at(j, s)] = inside(at(j, s)) ? 1.0f : 0.0f;
+    if (!p.est) return;
+    // the estimate: the modulus projection of the final x, restricted to the support
+    Cx<float>* __restrict__ E = p.est + (size_t)blockIdx.x * L * L;
+    Cx<float> o[J][TPL];
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(X[at(j, s)]);
+    P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+    __syncthreads();
+    spectral_columns<L>(buf, tw, line, q, [&](Cx<float> z, int f, int c) {
+        return data_apply(z, As[f * AP + c], dmode);
+    });
+    __syncthreads();
+    P::template row_from_buf<true>(o, buf, tw, line, q);
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) {
+            const int idx = at(j, s);
+            E[idx] = inside(idx) ? sgn(cscale(o[j][s], p.scale)) : Cx<float>{0.0f, 0.0f};
+        }
+}
+
+template <int L>
+cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
+    HioDev d;
+    d.x = (Cx<float>*)a.x;
+    d.est = (Cx<float>*)a.estimate;
+    d.A = (const float*)a.A;
+    d.a_stride = a.a_stride;
+    d.S = (float*)a.S;
+    d.s_stride = a.s_stride;
+    d.tw = (const Cx<float>*)tw;
+    d.blur = (const float*)a.blur;
+    d.scale = 1.0f / (float)(a.M * a.N);
+    d.beta = (float)a.beta;
+    d.thresh = (float)a.threshold;
+    d.iters = a.iters;
+    d.sw_every = a.sw_every;
+    d.positivity = a.positivity;
+    d.data_mode = a.data_mode;
+    const size_t smem = HioPlan<L>::smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_hio<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_hio<L><<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
+    count_launches();
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N) { return dm_fused_supported(dbl, M, N); }
+
+cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st) {
+    if (!hio_fused_supported(dbl, a.M, a.N)) return cudaErrorInvalidValue;
+    if (a.batch == 0 || (a.iters <= 0 && !a.estimate)) return cudaSuccess;
+    switch (a.M) {
+        case 32: return hio_launch<32>(a, tw, st);
+        case 64: return hio_launch<64>(a, tw, st);
+        case 128: return hio_launch<128>(a, tw, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace cpra_b200

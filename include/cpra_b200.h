@@ -152,6 +152,22 @@ int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S
 int cpra_b200_rfactor(cpra_b200_ctx* ctx, const void* x, const void* A, uint64_t a_stride, uint64_t batch,
                       double* r_host);
 
+/* Extension (project-defined, no counterpart in the reference): `iters`
+ * hybrid input-output iterations with shrinkwrap, fused, for `batch` patterns
+ * x ([batch][m][n] complex, in/out) with modulus planes A (pattern b at
+ * A + b*a_stride) and supports S (float, > 0.5 = inside; in/out, pattern b at
+ * S + b*s_stride).  With y = Backward2D(DataConstraint(Forward2D(x))):
+ * x <- y inside the support (and Re y >= 0 if positivity != 0), else
+ * x <- x - beta*y.  Every sw_every iterations (0: never) the support becomes
+ * { v > threshold * max v }, v = |x| circularly blurred by a normalised
+ * Gaussian whose sigma moves linearly from sigma_start (first update) to
+ * sigma_end (last).  If estimate is not null it receives S (.) y of the final
+ * x (the reconstruction).  Square float planes of 32, 64 or 128. */
+int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* ctx, void* x, const void* A, uint64_t a_stride, void* S,
+                             uint64_t s_stride, uint64_t batch, int iters, double beta, int sw_every,
+                             double sigma_start, double sigma_end, double threshold, int positivity,
+                             void* estimate);
+
 /* With CPRA_B200_OPT_KERNEL_TIMING on: total device time (ms) and number of
  * the fused difference-map launches since the last call, measured with CUDA
  * events on the context's stream; `pattern_iters` gets the patterns times

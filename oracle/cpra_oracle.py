@@ -489,3 +489,61 @@ def complex2d_to_3d(T, src, angles, m, n, p, l):
     nz = wsum > 0
     out[nz] = acc[nz] / wsum[nz]
     return out.astype(complex_dtype(T)).ravel()
+
+
+def gaussian_transfer(L, sigma):
+    """DFT of the normalised periodic Gaussian g[n] ~ exp(-min(n, L-n)^2 /
+    (2 sigma^2)), real and even (float64)."""
+    n = np.arange(L)
+    d = np.minimum(n, L - n).astype(np.float64)
+    g = np.exp(-d * d / (2.0 * sigma * sigma))
+    g /= g.sum()
+    return np.real(np.fft.fft(g))
+
+
+def hio_shrinkwrap(x0, A, S0, L, batch, iters, beta, sw_every=0, sigma_start=3.0, sigma_end=1.5, threshold=0.1,
+                   positivity=False, a_stride=None, s_stride=None):
+    """Project-defined hybrid input-output with shrinkwrap, float64 (the
+    reference has neither; its operator composition supplies the modulus
+    projection y = Backward2D(DataConstraint(Forward2D(x))),
+    MKL_Impl.inl:86-152).  Per iteration: x <- y inside the support (and
+    Re y >= 0 with positivity), x <- x - beta*y elsewhere.  Every sw_every
+    iterations the support becomes {v > threshold * max v}, v = |x| circularly
+    blurred by a normalised periodic Gaussian, sigma linear from sigma_start at
+    the first update to sigma_end at the last.  Returns (x, S, estimate) with
+    estimate = S (.) y of the final x."""
+    plane = L * L
+    a_stride = plane if a_stride is None else a_stride
+    s_stride = plane if s_stride is None else s_stride
+    x0 = np.asarray(x0).astype(np.complex128).ravel()
+    A = np.asarray(A, np.float64).ravel()
+    S0 = np.asarray(S0, np.float64).ravel()
+    updates = iters // sw_every if sw_every else 0
+    impl = OracleImpl(np.float64, L, L, 1, 1)
+    xs, ss, es = [], [], []
+    for b in range(batch):
+        x = x0[b * plane:(b + 1) * plane].copy()
+        a = A[b * a_stride: b * a_stride + plane]
+        S = S0[b * s_stride: b * s_stride + plane] > 0.5
+        k = 0
+        for it in range(iters):
+            y = x.copy()
+            impl.Forward2D(y)
+            impl.DataConstraint(y, a, plane, 1)
+            impl.Backward2D(y)
+            inside = S & (y.real >= 0) if positivity else S
+            x = np.where(inside, y, x - beta * y)
+            if updates and (it + 1) % sw_every == 0:
+                sg = sigma_start + (sigma_end - sigma_start) * k / (updates - 1) if updates > 1 else sigma_start
+                k += 1
+                g = gaussian_transfer(L, sg)
+                v = np.real(np.fft.ifft2(np.fft.fft2(np.abs(x).reshape(L, L)) * np.outer(g, g))).ravel()
+                S = v > threshold * v.max()
+        y = x.copy()
+        impl.Forward2D(y)
+        impl.DataConstraint(y, a, plane, 1)
+        impl.Backward2D(y)
+        xs.append(x)
+        ss.append(S.astype(np.float64))
+        es.append(np.where(S, y, 0))
+    return np.concatenate(xs), np.concatenate(ss), np.concatenate(es)
