@@ -81,6 +81,9 @@ _SIGS = {
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_void_p],
+    "cpra_b200_slice": [C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 + [C.c_void_p],
+    "cpra_b200_slice_loss_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
+                                 + [C.c_void_p, C.c_void_p, C.c_void_p],
     "cpra_b200_rfactor": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p],
     "cpra_b200_converge_error_noalloc": [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                         + [C.c_void_p],
@@ -283,6 +286,22 @@ class B200Impl:
                                                      int(sw_every), float(sigma_start), float(sigma_end),
                                                      float(threshold), 1 if positivity else 0, _addr(estimate)),
                       "hio_shrinkwrap")
+
+    def slice(self, V, angles, m, n, p, l, out) -> bool:
+        """Central slices of the Fourier volume V at the given angles (project-defined)."""
+        return _check(lib().cpra_b200_slice(self._h, _addr(V), _addr(angles), int(m), int(n), int(p), int(l),
+                                            _addr(out)), "slice")
+
+    def slice_loss_grad(self, V, angles, A, m, n, p, l, grad_V):
+        """Amplitude loss of the slices against A and its adjoints; returns
+        (loss, dL/dangles as a numpy float64 array); grad_V is written."""
+        import numpy as np
+        loss = np.zeros(1, np.float64)
+        ga = np.zeros(int(p), np.float64)
+        _check(lib().cpra_b200_slice_loss_grad(self._h, _addr(V), _addr(angles), _addr(A), int(m), int(n), int(p),
+                                               int(l), _addr(grad_V), loss.ctypes.data_as(C.c_void_p),
+                                               ga.ctypes.data_as(C.c_void_p)), "slice_loss_grad")
+        return float(loss[0]), ga
 
     def rfactor(self, x, A, batch, a_stride=0):
         """R-factor per pattern, sum | |Forward2D(x_b)| - A_b | / sum A_b in

@@ -928,6 +928,45 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
     return CPRA_B200_OK;
 }
 
+int cpra_b200_slice(cpra_b200_ctx* c, const void* V, const void* angles, uint64_t m, uint64_t n, uint64_t p,
+                    uint64_t l, void* slices) {
+    CTX_OR_RETURN(c);
+    if (!V || !angles || !slices) return fail(CPRA_B200_EARG, "slice: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "slice: zero size");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    CPRA_CHECK_CUDA(launch_slice(c->dbl, V, angles, slices, m, n, p, l, c->stream), "slice");
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_slice_loss_grad(cpra_b200_ctx* c, const void* V, const void* angles, const void* A, uint64_t m,
+                              uint64_t n, uint64_t p, uint64_t l, void* grad_V, double* loss_host,
+                              double* grad_angles_host) {
+    CTX_OR_RETURN(c);
+    if (!V || !angles || !A || !grad_V) return fail(CPRA_B200_EARG, "slice_loss_grad: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "slice_loss_grad: zero size");
+    if (p > 65535) return fail(CPRA_B200_EUNSUP, "slice_loss_grad: more than 65535 slices");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    r = ensure_work(c, p * n * m * c->csize());  // G = dL/ds
+    if (r) return r;
+    r = ensure_reduction(c, p);
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, grad_V, m, n, p, l, c->partials, c->sums,
+                                           c->stream),
+                    "slice_loss_grad");
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * p, cudaMemcpyDeviceToHost, c->stream),
+                    "slice_loss_grad");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "slice_loss_grad");
+    double loss = 0.0;
+    for (uint64_t i = 0; i < p; ++i) {
+        loss += c->host_sums[2 * i];
+        if (grad_angles_host) grad_angles_host[i] = c->host_sums[2 * i + 1];
+    }
+    if (loss_host) *loss_host = loss;
+    return CPRA_B200_OK;
+}
+
 int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, uint64_t* pattern_iters) {
     CTX_OR_RETURN(c);
     int r = flush(c);

@@ -58,6 +58,9 @@ cudaError_t launch_uniform(bool dbl, void* x, uint64_t num, uint64_t seed, uint6
 constexpr int CONVERGE_BLOCKS = 64;
 cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t span, uint64_t stride,
                               uint64_t batch, double* partials, double* sums, cudaStream_t st);
+// stage 2 of the two-level reductions: sums[2b], sums[2b+1] from the
+// CONVERGE_BLOCKS partial pairs of each of `batch` members, in index order
+cudaError_t launch_norm_final(const double* partials, double* sums, uint64_t batch, cudaStream_t st);
 // R-factor sums of `batch` centred spectra F (the Forward2D of each pattern):
 // sums[2b] = sum_px | |F_b| - A_b |, sums[2b+1] = sum_px A_b, in double, with
 // A_b = A + b * a_stride; deterministic two-level reduction through `partials`
@@ -102,6 +105,16 @@ struct DmArgs {
 };
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
+
+// ---- central slices and the amplitude-loss adjoints (kernels_adj.cu) --------
+// slices out[p] ([P][N][M]) of the [L][N][M] volume V at angles ang[p]
+cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, uint64_t m, uint64_t n, uint64_t p,
+                         uint64_t l, cudaStream_t st);
+// G = dL/ds (scratch, [P][N][M]), gV = dL/dV, sums[2p] = loss of slice p,
+// sums[2p+1] = dL/d ang[p] (partials: >= P * CONVERGE_BLOCKS * 2 doubles)
+cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
+                                   uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
+                                   cudaStream_t st);
 
 // ---- fused HIO + shrinkwrap iterations (kernels_hio.cu) -----------------------
 struct HioArgs {

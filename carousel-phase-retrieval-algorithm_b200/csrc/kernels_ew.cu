@@ -430,6 +430,12 @@ cudaError_t launch_norm_pairs(bool dbl, const void* a, const void* b, uint64_t s
     return cudaGetLastError();
 }
 
+cudaError_t launch_norm_final(const double* partials, double* sums, uint64_t batch, cudaStream_t st) {
+    k_norm_final<<<ew_grid(batch, 64), 64, 0, st>>>(partials, sums, batch, CONVERGE_BLOCKS);
+    count_launches();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rfactor_sums(bool dbl, const void* F, const void* A, uint64_t a_stride, uint64_t plane,
                                 uint64_t batch, double* partials, double* sums, cudaStream_t st) {
     if (batch == 0) return cudaSuccess;

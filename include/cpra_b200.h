@@ -168,6 +168,23 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* ctx, void* x, const void* A, uint64_
                              double sigma_start, double sigma_end, double threshold, int positivity,
                              void* estimate);
 
+/* Extension (project-defined): central slices of a Fourier volume.  V is
+ * [l][n][m] complex (y fastest), slices are [p][n][m]; slice pixel (xIn, yIn)
+ * at angle a (radians, element type) samples V bilinearly at z = l/2 - yr sin a,
+ * x = xIn, y = m/2 - yr cos a, yr = m/2 - yIn (the merges' geometry); points
+ * outside the volume read 0. */
+int cpra_b200_slice(cpra_b200_ctx* ctx, const void* V, const void* angles, uint64_t m, uint64_t n, uint64_t p,
+                    uint64_t l, void* slices);
+/* Extension (project-defined): the amplitude loss L = sum (|slice(V, a_p)| - A_p)^2
+ * (A: [p][n][m] element type) with its hand-written adjoints: grad_V (device,
+ * [l][n][m] complex) receives dL/dRe V + i dL/dIm V, computed as the exact
+ * transpose of the slice operator in gather form (deterministic);
+ * grad_angles_host[p] (host, double, may be null) receives dL/da_p; loss_host
+ * (double, may be null) receives L.  Sums are in double.  Synchronous. */
+int cpra_b200_slice_loss_grad(cpra_b200_ctx* ctx, const void* V, const void* angles, const void* A, uint64_t m,
+                              uint64_t n, uint64_t p, uint64_t l, void* grad_V, double* loss_host,
+                              double* grad_angles_host);
+
 /* With CPRA_B200_OPT_KERNEL_TIMING on: total device time (ms) and number of
  * the fused difference-map launches since the last call, measured with CUDA
  * events on the context's stream; `pattern_iters` gets the patterns times

@@ -547,3 +547,66 @@ def hio_shrinkwrap(x0, A, S0, L, batch, iters, beta, sw_every=0, sigma_start=3.0
         ss.append(S.astype(np.float64))
         es.append(np.where(S, y, 0))
     return np.concatenate(xs), np.concatenate(ss), np.concatenate(es)
+
+
+def _slice_weights(M, N, L, a):
+    """Bilinear sampling of one slice (the merges' geometry): for every slice
+    pixel (xIn, yIn) the (z, y) of its up to four voxels on the plane x = xIn,
+    their weights and the weights' derivatives in the angle (float64)."""
+    yIn = np.arange(M)
+    yr = (M // 2 - yIn).astype(np.float64)
+    zf = (L // 2) - yr * np.sin(a)
+    yf = (M // 2) - yr * np.cos(a)
+    dz, dy = -yr * np.cos(a), yr * np.sin(a)
+    z0, y0 = np.floor(zf).astype(np.int64), np.floor(yf).astype(np.int64)
+    fz, fy = zf - z0, yf - y0
+    out = []
+    for da in (0, 1):
+        for db in (0, 1):
+            z, y = z0 + da, y0 + db
+            wz, dwz = (fz, dz) if da else (1 - fz, -dz)
+            wy, dwy = (fy, dy) if db else (1 - fy, -dy)
+            ok = (z >= 0) & (z < L) & (y >= 0) & (y < M)
+            out.append((z, y, ok, wz * wy, dwz * wy + wz * dwy))
+    return out
+
+
+def slice_volume(V, angles, M, N, P, L):
+    """Project-defined central slices ([P][N][M] complex128) of the [L][N][M]
+    Fourier volume V: pixel (xIn, yIn) of angle a samples V bilinearly at
+    z = L/2 - yr sin a, x = xIn, y = M/2 - yr cos a, yr = M/2 - yIn."""
+    V = np.asarray(V).astype(np.complex128).reshape(L, N, M)
+    out = np.zeros((P, N, M), np.complex128)
+    for p in range(P):
+        for z, y, ok, w, _ in _slice_weights(M, N, L, float(angles[p])):
+            zz, yy = np.where(ok, z, 0), np.where(ok, y, 0)
+            out[p] += np.where(ok, w, 0.0)[None, :] * V[zz, :, yy].T
+    return out
+
+
+def slice_loss_grad(V, angles, A, M, N, P, L):
+    """Loss sum (|slice| - A)^2 and its gradients in float64:
+    (loss, dL/dRe V + i dL/dIm V as [L][N][M], dL/da as [P])."""
+    V = np.asarray(V).astype(np.complex128).reshape(L, N, M)
+    A = np.asarray(A, np.float64).reshape(P, N, M)
+    gV = np.zeros_like(V)
+    ga = np.zeros(P)
+    loss = 0.0
+    for p in range(P):
+        ws = _slice_weights(M, N, L, float(angles[p]))
+        s = np.zeros((N, M), np.complex128)
+        ds = np.zeros((N, M), np.complex128)
+        for z, y, ok, w, dw in ws:
+            zz, yy = np.where(ok, z, 0), np.where(ok, y, 0)
+            vals = V[zz, :, yy].T
+            s += np.where(ok, w, 0.0)[None, :] * vals
+            ds += np.where(ok, dw, 0.0)[None, :] * vals
+        mag = np.abs(s)
+        d = mag - A[p]
+        loss += float((d * d).sum())
+        G = np.where(mag > 0, 2 * d * s / np.where(mag > 0, mag, 1), 0)
+        ga[p] = float(np.real(np.conj(G) * ds).sum())
+        for z, y, ok, w, _ in ws:
+            for yi in np.nonzero(ok)[0]:
+                gV[z[yi], :, y[yi]] += w[yi] * G[:, yi]
+    return loss, gV, ga

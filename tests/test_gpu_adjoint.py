@@ -1,0 +1,135 @@
+"""Hand-written adjoints of the amplitude loss through the slice operator
+(project-defined): against the float64 oracle, against central finite
+differences, and through a test-side torch.autograd.Function."""
+import numpy as np
+import pytest
+
+import cpra_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tb(cuda):
+    import torch
+    import cpra_b200
+    return torch, cpra_b200
+
+
+def _problem(M, P, L, seed, dtype=np.complex64):
+    rng = np.random.default_rng(seed)
+    N = M
+    V = (rng.standard_normal(L * N * M) + 1j * rng.standard_normal(L * N * M)).astype(dtype)
+    ang = np.deg2rad(rng.uniform(3, 177, P)).astype(np.float64 if dtype == np.complex128 else np.float32)
+    A = rng.uniform(0.2, 2.0, P * N * M).astype(np.float64 if dtype == np.complex128 else np.float32)
+    return V, ang, A
+
+
+def test_slice_vs_oracle(tb):
+    torch, cb = tb
+    M, P, L = 16, 5, 16
+    V, ang, _ = _problem(M, P, L, 1)
+    impl = cb.B200Impl(M, M, L, 1)
+    out = torch.zeros(P * M * M, dtype=torch.complex64, device="cuda")
+    assert impl.slice(torch.from_numpy(V).cuda(), torch.from_numpy(ang).cuda(), M, M, P, L, out) and impl.Sync()
+    want = O.slice_volume(V, ang, M, M, P, L).ravel()
+    assert O.rel_l2(out.cpu().numpy(), want) < 1e-6
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_loss_grad_vs_oracle(tb, dtype):
+    torch, cb = tb
+    M, P, L = 16, 6, 16
+    cdt = np.complex64 if dtype == "float32" else np.complex128
+    V, ang, A = _problem(M, P, L, 2, cdt)
+    impl = cb.B200Impl(M, M, L, 1, dtype=dtype)
+    gV = torch.zeros(V.size, dtype=torch.complex64 if dtype == "float32" else torch.complex128, device="cuda")
+    loss, ga = impl.slice_loss_grad(torch.from_numpy(V).cuda(), torch.from_numpy(ang).cuda(),
+                                    torch.from_numpy(A).cuda(), M, M, P, L, gV)
+    lo, gVo, gao = O.slice_loss_grad(V, ang, A, M, M, P, L)
+    tol = 1e-5 if dtype == "float32" else 1e-12
+    assert abs(loss - lo) / lo < tol
+    assert O.rel_l2(gV.cpu().numpy(), gVo.ravel()) < tol
+    np.testing.assert_allclose(ga, gao, rtol=10 * tol, atol=10 * tol * np.abs(gao).max())
+
+
+def test_loss_grad_vs_finite_differences(tb):
+    """Central differences in float64: h = 1e-3 on the volume (the loss is smooth
+    where |s| > 0); h = 1e-6 on the angles (bilinear weights have kinks where a
+    sample point crosses a voxel plane, so a small step keeps both evaluations
+    on one side of them).  Relative agreement 1e-4."""
+    torch, cb = tb
+    M, P, L = 12, 4, 12
+    V, ang, A = _problem(M, P, L, 3, np.complex128)
+    impl = cb.B200Impl(M, M, L, 1, dtype="float64")
+    Vd, Ad = torch.from_numpy(V).cuda(), torch.from_numpy(A).cuda()
+    gV = torch.zeros_like(Vd)
+    _, ga = impl.slice_loss_grad(Vd, torch.from_numpy(ang).cuda(), Ad, M, M, P, L, gV)
+    g = gV.cpu().numpy()
+
+    def loss_at(Vh, angh):
+        tmp = torch.zeros_like(Vd)
+        l, _ = impl.slice_loss_grad(torch.from_numpy(Vh).cuda(), torch.from_numpy(angh).cuda(), Ad, M, M, P, L, tmp)
+        return l
+
+    rng = np.random.default_rng(0)
+    # voxels that some slice samples (others have a zero gradient)
+    touched = np.nonzero(np.abs(g) > 1e-6 * np.abs(g).max())[0]
+    for k in rng.choice(touched, 8, replace=False):
+        for unit, part in ((1.0, np.real), (1j, np.imag)):
+            h = 1e-3
+            Vp, Vm = V.copy(), V.copy()
+            Vp[k] += unit * h
+            Vm[k] -= unit * h
+            fd = (loss_at(Vp, ang) - loss_at(Vm, ang)) / (2 * h)
+            assert abs(fd - part(g[k])) <= 1e-4 * max(abs(fd), 1e-3 * np.abs(g).max()), (k, fd, part(g[k]))
+    for p in range(P):
+        h = 1e-6
+        ap, am = ang.copy(), ang.copy()
+        ap[p] += h
+        am[p] -= h
+        fd = (loss_at(V, ap) - loss_at(V, am)) / (2 * h)
+        assert abs(fd - ga[p]) <= 1e-4 * abs(fd), (p, fd, ga[p])
+
+
+def test_autograd_function_and_refinement(tb):
+    """A test-side torch.autograd.Function over the C ABI; a few gradient steps
+    on the volume and the angles lower the loss of perturbed orientations."""
+    torch, cb = tb
+    M, P, L = 16, 8, 16
+    impl = cb.B200Impl(M, M, L, 1)
+
+    class SliceLoss(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, Vr, ang, A):
+            V = torch.view_as_complex(Vr.contiguous())
+            gV = torch.zeros_like(V)
+            loss, ga = impl.slice_loss_grad(V, ang.contiguous(), A, M, M, P, L, gV)
+            ctx.save_for_backward(torch.view_as_real(gV), torch.from_numpy(ga).to(ang))
+            return Vr.new_tensor(loss)
+
+        @staticmethod
+        def backward(ctx, gout):
+            gVr, ga = ctx.saved_tensors
+            return gout * gVr, gout * ga, None
+
+    rng = np.random.default_rng(5)
+    Vt = (rng.standard_normal(L * M * M) + 1j * rng.standard_normal(L * M * M)).astype(np.complex64)
+    ang_t = np.deg2rad(np.linspace(10, 170, P)).astype(np.float32)
+    out = torch.zeros(P * M * M, dtype=torch.complex64, device="cuda")
+    impl.slice(torch.from_numpy(Vt).cuda(), torch.from_numpy(ang_t).cuda(), M, M, P, L, out)
+    impl.Sync()
+    A = out.abs().contiguous()
+    Vr = torch.view_as_real(torch.from_numpy(Vt).cuda()).clone().requires_grad_(True)
+    ang = (torch.from_numpy(ang_t).cuda() + torch.from_numpy(np.deg2rad(rng.normal(0, 0.5, P)).astype(np.float32)).cuda())
+    ang.requires_grad_(True)
+    opt = torch.optim.Adam([{"params": [ang], "lr": 1e-3}, {"params": [Vr], "lr": 1e-3}])
+    losses = []
+    for _ in range(25):
+        opt.zero_grad()
+        loss = SliceLoss.apply(Vr, ang, A)
+        loss.backward()
+        assert ang.grad is not None and Vr.grad is not None
+        opt.step()
+        losses.append(loss.item())
+    assert losses[-1] < 0.5 * losses[0], losses
