@@ -157,6 +157,8 @@ struct cpra_b200_ctx {
     // shrinkwrap blur tables
     void* blur = nullptr;
     uint64_t blur_bytes = 0;
+    // patterns per chunk of the large-plane HIO passes (0: the whole batch)
+    uint64_t hio_chunk = 0;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -554,6 +556,10 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
             break;
         case CPRA_B200_OPT_SEED: c->seed = (uint64_t)value; c->init_calls = 0; break;
         case CPRA_B200_OPT_KERNEL_TIMING: c->timing = value != 0; break;
+        case CPRA_B200_OPT_HIO_CHUNK:
+            if (value < 0) return fail(CPRA_B200_EARG, "hio chunk must be >= 0");
+            c->hio_chunk = (uint64_t)value;
+            break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -858,8 +864,9 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
     CTX_OR_RETURN(c);
     if (!x || !A || !S) return fail(CPRA_B200_EARG, "hio_shrinkwrap: null pointer");
     if (batch == 0 || iters < 0) return fail(CPRA_B200_EARG, "hio_shrinkwrap: batch must be positive, iters >= 0");
-    if (!hio_fused_supported(c->dbl, c->m, c->n))
-        return fail(CPRA_B200_EUNSUP, "hio_shrinkwrap: needs float and square 32, 64 or 128 planes");
+    const bool large = !hio_fused_supported(c->dbl, c->m, c->n);
+    if (large && !hio_large_supported(c->dbl, c->m, c->n))
+        return fail(CPRA_B200_EUNSUP, "hio_shrinkwrap: needs float and square 32, 64, 128, 256 or 512 planes");
     const int updates = (sw_every > 0) ? iters / sw_every : 0;
     if (updates > 0 && s_stride < c->plane())
         return fail(CPRA_B200_EARG, "hio_shrinkwrap: shrinkwrap updates each pattern's support: s_stride >= m*n");
@@ -924,7 +931,23 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
     a.data_mode = c->data_mode;
     a.beta = c->round_t(beta);
     a.threshold = threshold;
-    CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "hio_shrinkwrap");
+    if (!large) {
+        CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "hio_shrinkwrap");
+        return CPRA_B200_OK;
+    }
+    // line passes over chunks of patterns (default: one chunk); the work
+    // buffer holds one chunk's Y (complex), blurred values, support mask and
+    // per-pattern maxima
+    const uint64_t chunk = (c->hio_chunk == 0) ? batch : std::min(c->hio_chunk, batch);
+    // Y, V, the support mask (multiples of 256 bytes) and the maxima
+    const uint64_t ybytes = chunk * c->plane() * 8, vbytes = chunk * c->plane() * 4, mbytes = chunk * c->plane() / 8;
+    r = ensure_work(c, ybytes + vbytes + mbytes + chunk * 4);
+    if (r) return r;
+    char* w = static_cast<char*>(c->work);
+    CPRA_CHECK_CUDA(launch_hio_large(a, twiddles(c, c->m), w, w + ybytes,
+                                     reinterpret_cast<unsigned int*>(w + ybytes + vbytes + mbytes),
+                                     reinterpret_cast<uint32_t*>(w + ybytes + vbytes), chunk, c->stream),
+                    "hio_shrinkwrap");
     return CPRA_B200_OK;
 }
 

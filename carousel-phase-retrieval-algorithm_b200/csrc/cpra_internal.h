@@ -132,4 +132,13 @@ struct HioArgs {
 bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st);
 
+// ---- the same HIO iteration as line passes through L2 (kernels_large.cu) ----
+// Float square planes of 256 or 512; patterns run in chunks of `chunk`, each
+// chunk through all iterations.  Scratch, 16-byte aligned: Y (chunk planes,
+// complex), V (chunk planes, float), vmax (chunk unsigned ints), mask (chunk
+// planes of bits).
+bool hio_large_supported(bool dbl, uint64_t M, uint64_t N);
+cudaError_t launch_hio_large(const HioArgs& a, const void* tw, void* Y, void* V, unsigned int* vmax, uint32_t* mask,
+                             uint64_t chunk, cudaStream_t st);
+
 }  // namespace cpra_b200

@@ -53,6 +53,8 @@ extern "C" {
 #define CPRA_B200_OPT_DATA_MODE 3  /* 0 (default): MKL_Impl.inl:86-106 (A==0 unconstrained); 1: CUDA kernel */
 #define CPRA_B200_OPT_SEED 4       /* seed of cpra_b200_initialize's counter-based stream */
 #define CPRA_B200_OPT_KERNEL_TIMING 5 /* 1: bracket each fused launch with CUDA events (cpra_b200_kernel_timing) */
+#define CPRA_B200_OPT_HIO_CHUNK 6  /* patterns per chunk of the 256/512 HIO line passes (bounds their scratch,
+                                    12.125 bytes per pixel); 0 (default): the whole batch */
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 
@@ -162,7 +164,11 @@ int cpra_b200_rfactor(cpra_b200_ctx* ctx, const void* x, const void* A, uint64_t
  * { v > threshold * max v }, v = |x| circularly blurred by a normalised
  * Gaussian whose sigma moves linearly from sigma_start (first update) to
  * sigma_end (last).  If estimate is not null it receives S (.) y of the final
- * x (the reconstruction).  Square float planes of 32, 64 or 128. */
+ * x (the reconstruction).  Square float planes of 32, 64 or 128 run one CTA
+ * per pattern, all iterations in one launch; 256 and 512 run two line passes
+ * per iteration (columns with the modulus step; rows with the update and the
+ * next forward row transform) over chunks of patterns
+ * (CPRA_B200_OPT_HIO_CHUNK). */
 int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* ctx, void* x, const void* A, uint64_t a_stride, void* S,
                              uint64_t s_stride, uint64_t batch, int iters, double beta, int sw_every,
                              double sigma_start, double sigma_end, double threshold, int positivity,
