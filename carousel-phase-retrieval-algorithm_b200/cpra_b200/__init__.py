@@ -49,6 +49,12 @@ class IMPL_TYPE(enum.IntEnum):
 _lib = None
 
 # name -> (argtypes) ; every entry point returns int
+class HioBucket(C.Structure):
+    """cpra_b200_hio_bucket (include/cpra_b200.h)."""
+    _fields_ = [("side", C.c_uint64), ("count", C.c_uint64), ("x", C.c_void_p), ("A", C.c_void_p),
+                ("S", C.c_void_p), ("estimate", C.c_void_p)]
+
+
 _SIGS = {
     "cpra_b200_create": [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64],
     "cpra_b200_destroy": [C.c_void_p],
@@ -81,6 +87,8 @@ _SIGS = {
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_void_p],
+    "cpra_b200_hio_batched": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double,
+                              C.c_double, C.c_double, C.c_int],
     "cpra_b200_slice": [C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 + [C.c_void_p],
     "cpra_b200_slice_loss_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                  + [C.c_void_p, C.c_void_p, C.c_void_p],
@@ -286,6 +294,20 @@ class B200Impl:
                                                      int(sw_every), float(sigma_start), float(sigma_end),
                                                      float(threshold), 1 if positivity else 0, _addr(estimate)),
                       "hio_shrinkwrap")
+
+    def hio_batched(self, buckets, iters, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5, threshold=0.1,
+                    positivity=False) -> bool:
+        """HIO + shrinkwrap over patterns of uneven sizes in one call
+        (project-defined): ``buckets`` is a list of dicts with keys side,
+        count, x, A, S and optionally estimate (device buffers, per-pattern
+        contiguous); each bucket runs on its own stream."""
+        arr = (HioBucket * len(buckets))()
+        for i, b in enumerate(buckets):
+            arr[i] = HioBucket(int(b["side"]), int(b["count"]), _addr(b["x"]), _addr(b["A"]), _addr(b["S"]),
+                               _addr(b.get("estimate")))
+        return _check(lib().cpra_b200_hio_batched(self._h, C.cast(arr, C.c_void_p), len(buckets), int(iters),
+                                                  float(beta), int(sw_every), float(sigma_start), float(sigma_end),
+                                                  float(threshold), 1 if positivity else 0), "hio_batched")
 
     def slice(self, V, angles, m, n, p, l, out) -> bool:
         """Central slices of the Fourier volume V at the given angles (project-defined)."""

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -121,6 +122,13 @@ std::vector<T> twiddle_table(uint64_t L) {
 
 }  // namespace
 
+struct BucketLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    void* scratch = nullptr;
+    uint64_t scratch_bytes = 0;
+};
+
 struct cpra_b200_ctx {
     bool dbl = false;
     uint64_t m = 1, n = 1, l = 1, batch = 1;
@@ -154,9 +162,11 @@ struct cpra_b200_ctx {
     double* err_sums = nullptr;
     double* host_err = nullptr;
     uint64_t err_cap = 0;
-    // shrinkwrap blur tables
-    void* blur = nullptr;
-    uint64_t blur_bytes = 0;
+    // shrinkwrap blur tables per (side, updates, sigma_start, sigma_end)
+    std::map<std::tuple<uint64_t, int, double, double>, void*> blur_cache;
+    // streams, join events and scratch of cpra_b200_hio_batched's buckets
+    std::vector<BucketLane> bucket_streams;
+    cudaEvent_t fork_event = nullptr;
     // patterns per chunk of the large-plane HIO passes (0: the whole batch)
     uint64_t hio_chunk = 0;
 
@@ -527,7 +537,14 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     if (c->sums) cudaFree(c->sums);
     if (c->host_sums) cudaFreeHost(c->host_sums);
     if (c->drv) cudaFree(c->drv);
-    if (c->blur) cudaFree(c->blur);
+    for (auto& kv : c->blur_cache) cudaFree(kv.second);
+    for (BucketLane& lane : c->bucket_streams) {
+        if (lane.stream) cudaStreamSynchronize(lane.stream);
+        if (lane.scratch) cudaFree(lane.scratch);
+        if (lane.done) cudaEventDestroy(lane.done);
+        if (lane.stream) cudaStreamDestroy(lane.stream);
+    }
+    if (c->fork_event) cudaEventDestroy(c->fork_event);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -858,96 +875,224 @@ int cpra_b200_rfactor(cpra_b200_ctx* c, const void* x, const void* A, uint64_t a
     return CPRA_B200_OK;
 }
 
+namespace {
+
+// Device tables of the shrinkwrap blur: for update k of `updates`, sigma moves
+// linearly from s0 to s1; entry i of a table is the DFT of a normalised
+// periodic Gaussian (real and even) at the frequency (i + L/2) mod L that the
+// sign-modulated transform puts at index i.  Cached per (L, updates, s0, s1).
+int blur_tables(cpra_b200_ctx* c, uint64_t L, int updates, double s0, double s1, const void** out) {
+    const auto key = std::make_tuple(L, updates, s0, s1);
+    auto it = c->blur_cache.find(key);
+    if (it != c->blur_cache.end()) {
+        *out = it->second;
+        return CPRA_B200_OK;
+    }
+    std::vector<double> cs(L);
+    for (uint64_t ph = 0; ph < L; ++ph) cs[ph] = std::cos(2.0 * 3.141592653589793238462643383279502884 * (double)ph / (double)L);
+    std::vector<float> tab((size_t)updates * L);
+    std::vector<double> g(L);
+    for (int k = 0; k < updates; ++k) {
+        const double sg = updates > 1 ? s0 + (s1 - s0) * k / (updates - 1) : s0;
+        double sum = 0.0;
+        for (uint64_t n = 0; n < L; ++n) {
+            const double d = (double)std::min<uint64_t>(n, L - n);
+            g[n] = std::exp(-d * d / (2.0 * sg * sg));
+            sum += g[n];
+        }
+        for (uint64_t f = 0; f < L; ++f) {
+            const uint64_t fu = (f + L / 2) % L;
+            double acc = 0.0;
+            for (uint64_t n = 0; n < L; ++n) acc += g[n] * cs[(n * fu) % L];
+            tab[(size_t)k * L + f] = (float)(acc / sum);
+        }
+    }
+    void* d = nullptr;
+    const size_t bytes = tab.size() * sizeof(float);
+    CPRA_CHECK_CUDA(cudaMalloc(&d, bytes), "cudaMalloc(blur tables)");
+    const cudaError_t e = cudaMemcpy(d, tab.data(), bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(e, "cudaMemcpy(blur tables)");
+    }
+    c->blur_cache[key] = d;
+    *out = d;
+    return CPRA_B200_OK;
+}
+
+struct HioJob {
+    uint64_t L, batch;
+    void* x;
+    const void* A;
+    uint64_t a_stride;
+    void* S;
+    uint64_t s_stride;
+    void* estimate;
+};
+struct HioParams {
+    int iters, sw_every, positivity;
+    double beta, sigma_start, sigma_end, threshold;
+    int updates() const { return sw_every > 0 ? iters / sw_every : 0; }
+};
+
+bool hio_side_supported(bool dbl, uint64_t L) {
+    return hio_fused_supported(dbl, L, L) || hio_large_supported(dbl, L, L);
+}
+
+// scratch bytes of one job: Y, V, the support mask and the maxima of a chunk
+uint64_t hio_scratch_bytes(bool dbl, uint64_t L, uint64_t chunk) {
+    if (hio_fused_supported(dbl, L, L)) return 0;
+    return chunk * L * L * 8 + chunk * L * L * 4 + chunk * L * L / 8 + chunk * 4;
+}
+
+// enqueue one job on `st` (arguments already checked); `scratch` holds
+// hio_scratch_bytes(L, chunk)
+int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t chunk, void* scratch,
+                cudaStream_t st) {
+    const int updates = h.updates();
+    HioArgs a;
+    a.x = j.x;
+    a.estimate = j.estimate;
+    a.A = j.A;
+    a.a_stride = j.a_stride;
+    a.S = j.S;
+    a.s_stride = j.s_stride;
+    a.blur = nullptr;
+    if (updates > 0) {
+        int r = blur_tables(c, j.L, updates, h.sigma_start, h.sigma_end, &a.blur);
+        if (r) return r;
+    }
+    a.M = a.N = j.L;
+    a.batch = j.batch;
+    a.iters = h.iters;
+    a.sw_every = updates > 0 ? h.sw_every : 0;
+    a.positivity = h.positivity ? 1 : 0;
+    a.data_mode = c->data_mode;
+    a.beta = c->round_t(h.beta);
+    a.threshold = h.threshold;
+    int r = ensure_twiddles(c, j.L);
+    if (r) return r;
+    if (hio_fused_supported(c->dbl, j.L, j.L)) {
+        CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, j.L), st), "hio_shrinkwrap");
+        return CPRA_B200_OK;
+    }
+    const uint64_t plane = j.L * j.L;
+    char* w = static_cast<char*>(scratch);
+    const uint64_t yb = chunk * plane * 8, vb = chunk * plane * 4, mb = chunk * plane / 8;  // multiples of 256
+    CPRA_CHECK_CUDA(launch_hio_large(a, twiddles(c, j.L), w, w + yb, reinterpret_cast<unsigned int*>(w + yb + vb + mb),
+                                     reinterpret_cast<uint32_t*>(w + yb + vb), chunk, st),
+                    "hio_shrinkwrap");
+    return CPRA_B200_OK;
+}
+
+int hio_check_params(const HioParams& h, const char* who) {
+    if (h.iters < 0) return fail(CPRA_B200_EARG, std::string(who) + ": iters must be >= 0");
+    if (h.updates() > 0 && !(h.sigma_start > 0.0 && h.sigma_end > 0.0))
+        return fail(CPRA_B200_EARG, std::string(who) + ": sigma must be positive");
+    return CPRA_B200_OK;
+}
+
+int ensure_buffer(cpra_b200_ctx* c, void** buf, uint64_t* have, uint64_t bytes, const char* what) {
+    if (*have >= bytes) return CPRA_B200_OK;
+    if (*buf) {
+        cudaDeviceSynchronize();
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
+    }
+    CPRA_CHECK_CUDA(cudaMalloc(buf, bytes), what);
+    *have = bytes;
+    return CPRA_B200_OK;
+}
+
+}  // namespace
+
 int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t a_stride, void* S, uint64_t s_stride,
                              uint64_t batch, int iters, double beta, int sw_every, double sigma_start,
                              double sigma_end, double threshold, int positivity, void* estimate) {
     CTX_OR_RETURN(c);
     if (!x || !A || !S) return fail(CPRA_B200_EARG, "hio_shrinkwrap: null pointer");
     if (batch == 0 || iters < 0) return fail(CPRA_B200_EARG, "hio_shrinkwrap: batch must be positive, iters >= 0");
-    const bool large = !hio_fused_supported(c->dbl, c->m, c->n);
-    if (large && !hio_large_supported(c->dbl, c->m, c->n))
+    if (c->m != c->n || !hio_side_supported(c->dbl, c->m))
         return fail(CPRA_B200_EUNSUP, "hio_shrinkwrap: needs float and square 32, 64, 128, 256 or 512 planes");
-    const int updates = (sw_every > 0) ? iters / sw_every : 0;
-    if (updates > 0 && s_stride < c->plane())
+    const HioParams h{iters, sw_every, positivity, beta, sigma_start, sigma_end, threshold};
+    int r = hio_check_params(h, "hio_shrinkwrap");
+    if (r) return r;
+    if (h.updates() > 0 && s_stride < c->plane())
         return fail(CPRA_B200_EARG, "hio_shrinkwrap: shrinkwrap updates each pattern's support: s_stride >= m*n");
-    if (updates > 0 && !(sigma_start > 0.0 && sigma_end > 0.0))
-        return fail(CPRA_B200_EARG, "hio_shrinkwrap: sigma must be positive");
-    int r = flush(c);
+    r = flush(c);
     if (r) return take_deferred(c);
     if (iters == 0 && !estimate) return CPRA_B200_OK;
-    const uint64_t L = c->m;
-    if (updates > 0) {
-        // g(f) for a normalised periodic Gaussian of width sigma: its DFT, real
-        // and even; entry i is the value at the frequency (i + L/2) mod L that
-        // the sign-modulated transform puts at index i
-        std::vector<float> tab((size_t)updates * L);
-        for (int k = 0; k < updates; ++k) {
-            const double sg = updates > 1 ? sigma_start + (sigma_end - sigma_start) * k / (updates - 1) : sigma_start;
-            std::vector<double> g(L);
-            double sum = 0.0;
-            for (uint64_t n = 0; n < L; ++n) {
-                const double d = (double)std::min<uint64_t>(n, L - n);
-                g[n] = std::exp(-d * d / (2.0 * sg * sg));
-                sum += g[n];
-            }
-            for (uint64_t f = 0; f < L; ++f) {
-                const uint64_t fu = (f + L / 2) % L;
-                double acc = 0.0;
-                for (uint64_t n = 0; n < L; ++n) {
-                    const uint64_t ph = (n * fu) % L;
-                    acc += g[n] * std::cos(2.0 * 3.141592653589793238462643383279502884 * (double)ph / (double)L);
-                }
-                tab[(size_t)k * L + f] = (float)(acc / sum);
-            }
-        }
-        const uint64_t bytes = tab.size() * sizeof(float);
-        if (c->blur_bytes < bytes) {
-            if (c->blur) {
-                cudaStreamSynchronize(c->stream);
-                cudaFree(c->blur);
-                c->blur = nullptr;
-                c->blur_bytes = 0;
-            }
-            CPRA_CHECK_CUDA(cudaMalloc(&c->blur, bytes), "cudaMalloc(blur tables)");
-            c->blur_bytes = bytes;
-        }
-        CPRA_CHECK_CUDA(cudaMemcpyAsync(c->blur, tab.data(), bytes, cudaMemcpyHostToDevice, c->stream), "hio_shrinkwrap");
-        CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "hio_shrinkwrap");  // tab leaves scope
-    }
-    HioArgs a;
-    a.x = x;
-    a.estimate = estimate;
-    a.A = A;
-    a.a_stride = a_stride;
-    a.S = S;
-    a.s_stride = s_stride;
-    a.blur = updates > 0 ? c->blur : nullptr;
-    a.M = c->m;
-    a.N = c->n;
-    a.batch = batch;
-    a.iters = iters;
-    a.sw_every = updates > 0 ? sw_every : 0;
-    a.positivity = positivity ? 1 : 0;
-    a.data_mode = c->data_mode;
-    a.beta = c->round_t(beta);
-    a.threshold = threshold;
-    if (!large) {
-        CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "hio_shrinkwrap");
-        return CPRA_B200_OK;
-    }
-    // line passes over chunks of patterns (default: one chunk); the work
-    // buffer holds one chunk's Y (complex), blurred values, support mask and
-    // per-pattern maxima
     const uint64_t chunk = (c->hio_chunk == 0) ? batch : std::min(c->hio_chunk, batch);
-    // Y, V, the support mask (multiples of 256 bytes) and the maxima
-    const uint64_t ybytes = chunk * c->plane() * 8, vbytes = chunk * c->plane() * 4, mbytes = chunk * c->plane() / 8;
-    r = ensure_work(c, ybytes + vbytes + mbytes + chunk * 4);
+    r = ensure_work(c, hio_scratch_bytes(c->dbl, c->m, chunk));
     if (r) return r;
-    char* w = static_cast<char*>(c->work);
-    CPRA_CHECK_CUDA(launch_hio_large(a, twiddles(c, c->m), w, w + ybytes,
-                                     reinterpret_cast<unsigned int*>(w + ybytes + vbytes + mbytes),
-                                     reinterpret_cast<uint32_t*>(w + ybytes + vbytes), chunk, c->stream),
-                    "hio_shrinkwrap");
+    return hio_enqueue(c, HioJob{c->m, batch, x, A, a_stride, S, s_stride, estimate}, h, chunk, c->work, c->stream);
+}
+
+int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets, int n_buckets, int iters,
+                          double beta, int sw_every, double sigma_start, double sigma_end, double threshold,
+                          int positivity) {
+    CTX_OR_RETURN(c);
+    if (!buckets || n_buckets <= 0) return fail(CPRA_B200_EARG, "hio_batched: no buckets");
+    if (n_buckets > CPRA_B200_MAX_BUCKETS) return fail(CPRA_B200_EARG, "hio_batched: too many buckets");
+    const HioParams h{iters, sw_every, positivity, beta, sigma_start, sigma_end, threshold};
+    int r = hio_check_params(h, "hio_batched");
+    if (r) return r;
+    for (int i = 0; i < n_buckets; ++i) {
+        const cpra_b200_hio_bucket& b = buckets[i];
+        if (!b.x || !b.A || !b.S || b.count == 0) return fail(CPRA_B200_EARG, "hio_batched: bucket without data");
+        if (!hio_side_supported(c->dbl, b.side))
+            return fail(CPRA_B200_EUNSUP, "hio_batched: sides must be 32, 64, 128, 256 or 512 (float context)");
+    }
+    r = flush(c);
+    if (r) return take_deferred(c);
+    if (iters == 0) {
+        bool any_estimate = false;
+        for (int i = 0; i < n_buckets; ++i) any_estimate |= buckets[i].estimate != nullptr;
+        if (!any_estimate) return CPRA_B200_OK;
+    }
+    // one stream per bucket, forked from and joined back into the context's
+    // stream; the most work (pixels x patterns) is enqueued first
+    std::vector<int> order(n_buckets);
+    for (int i = 0; i < n_buckets; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return buckets[a].side * buckets[a].side * buckets[a].count > buckets[b].side * buckets[b].side * buckets[b].count;
+    });
+    while ((int)c->bucket_streams.size() < n_buckets) {
+        BucketLane lane;
+        CPRA_CHECK_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&lane.done, cudaEventDisableTiming), "cudaEventCreate");
+        c->bucket_streams.push_back(lane);
+    }
+    if (!c->fork_event) CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&c->fork_event, cudaEventDisableTiming), "cudaEventCreate");
+    for (int k = 0; k < n_buckets; ++k) {
+        const cpra_b200_hio_bucket& b = buckets[order[k]];
+        BucketLane& lane = c->bucket_streams[k];
+        const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
+        r = ensure_buffer(c, &lane.scratch, &lane.scratch_bytes, hio_scratch_bytes(c->dbl, b.side, chunk),
+                          "cudaMalloc(hio_batched scratch)");
+        if (r) return r;
+        r = ensure_twiddles(c, b.side);
+        if (r) return r;
+        if (h.updates() > 0) {
+            const void* unused;
+            r = blur_tables(c, b.side, h.updates(), sigma_start, sigma_end, &unused);
+            if (r) return r;
+        }
+    }
+    CPRA_CHECK_CUDA(cudaEventRecord(c->fork_event, c->stream), "hio_batched");
+    for (int k = 0; k < n_buckets; ++k) {
+        const cpra_b200_hio_bucket& b = buckets[order[k]];
+        BucketLane& lane = c->bucket_streams[k];
+        const uint64_t plane = b.side * b.side;
+        const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
+        CPRA_CHECK_CUDA(cudaStreamWaitEvent(lane.stream, c->fork_event, 0), "hio_batched");
+        r = hio_enqueue(c, HioJob{b.side, b.count, b.x, b.A, plane, b.S, plane, b.estimate}, h, chunk, lane.scratch,
+                        lane.stream);
+        if (r) return r;
+        CPRA_CHECK_CUDA(cudaEventRecord(lane.done, lane.stream), "hio_batched");
+        CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, lane.done, 0), "hio_batched");
+    }
     return CPRA_B200_OK;
 }
 

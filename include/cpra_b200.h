@@ -174,6 +174,32 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* ctx, void* x, const void* A, uint64_
                              double sigma_start, double sigma_end, double threshold, int positivity,
                              void* estimate);
 
+/* One size bucket of cpra_b200_hio_batched: `count` square side x side
+ * patterns with x ([count][side][side] complex, in/out), A (modulus planes,
+ * float), S (supports, float, in/out) and, optionally, the estimate output,
+ * all contiguous per pattern (strides side*side). */
+typedef struct cpra_b200_hio_bucket {
+    uint64_t side;
+    uint64_t count;
+    void* x;
+    const void* A;
+    void* S;
+    void* estimate;
+} cpra_b200_hio_bucket;
+#define CPRA_B200_MAX_BUCKETS 64
+
+/* Extension (project-defined, no counterpart in the reference): the HIO +
+ * shrinkwrap iterations of cpra_b200_hio_shrinkwrap for patterns of uneven
+ * sizes in one call: each bucket (side 32, 64, 128, 256 or 512; float
+ * context) runs on its own stream, forked from and joined back into the
+ * context's stream, so the buckets' launches overlap on the device.  The
+ * context's m, n, batch do not constrain the buckets.  Asynchronous like the
+ * other operators; same results per bucket as a cpra_b200_hio_shrinkwrap call
+ * with that bucket's patterns. */
+int cpra_b200_hio_batched(cpra_b200_ctx* ctx, const cpra_b200_hio_bucket* buckets, int n_buckets, int iters,
+                          double beta, int sw_every, double sigma_start, double sigma_end, double threshold,
+                          int positivity);
+
 /* Extension (project-defined): central slices of a Fourier volume.  V is
  * [l][n][m] complex (y fastest), slices are [p][n][m]; slice pixel (xIn, yIn)
  * at angle a (radians, element type) samples V bilinearly at z = l/2 - yr sin a,

@@ -685,3 +685,43 @@ def test_hio_large_full_run_rfactor(tb):
     assert np.median(rel) < 0.03 and np.max(rel) < 0.25, (r, ro)
     e = host(est).reshape(B, -1)
     assert np.all(e[host(S).reshape(B, -1) < 0.5] == 0)
+
+
+# ---- uneven sizes in one call --------------------------------------------------------------
+def test_hio_batched_matches_per_size_calls(tb):
+    """Each bucket of the uneven-size call gives the same bits as a
+    single-size call with the same patterns (the buckets only share the
+    device, not data)."""
+    torch, cb = tb
+    sizes = [(64, 3), (128, 2), (256, 2), (512, 1)]
+    iters, sw = 12, 5
+    data = {L: _hio_inputs(L, B, seed=L) for L, B in sizes}
+    buckets, keep = [], []
+    for L, B in sizes:
+        A, S0, x0 = data[L]
+        b = {"side": L, "count": B, "x": dev(torch, x0.ravel()), "A": dev(torch, A.ravel()),
+             "S": dev(torch, S0.ravel())}
+        b["estimate"] = torch.empty_like(b["x"])
+        buckets.append(b)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
+    assert impl.hio_batched(buckets, iters, beta=0.9, sw_every=sw) and impl.Sync()
+    for (L, B), b in zip(sizes, buckets):
+        A, S0, x0 = data[L]
+        one = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        est = torch.empty_like(x)
+        assert one.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=sw, estimate=est)
+        assert one.Sync()
+        np.testing.assert_array_equal(host(b["x"]), host(x))
+        np.testing.assert_array_equal(host(b["S"]), host(S))
+        np.testing.assert_array_equal(host(b["estimate"]), host(est))
+
+
+def test_hio_batched_rejects_bad_buckets(tb):
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
+    x = torch.zeros(96 * 96, dtype=torch.complex64, device="cuda")
+    A = torch.zeros(96 * 96, dtype=torch.float32, device="cuda")
+    with pytest.raises(cb.CpraB200Error):
+        impl.hio_batched([{"side": 96, "count": 1, "x": x, "A": A, "S": A}], 2)
+    assert not impl.hio_batched([], 2)
