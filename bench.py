@@ -443,6 +443,10 @@ def main():
             result["episode3d"] = episode_3d(torch, cpra_b200, d, dev)
         except Exception as ex:
             result["episode3d"] = {"error": str(ex)[:200]}
+        try:
+            result["uneven_batch"] = uneven_batch(torch, cpra_b200, dev)
+        except Exception as ex:
+            result["uneven_batch"] = {"error": str(ex)[:200]}
 
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         rate, sample, cores = cpu_reference_rate(d["A"], d["S"], M, IT, a.cpu_seconds, os.cpu_count() or 1)
@@ -492,6 +496,126 @@ def episode_3d(torch, cpra_b200, d, dev, iters3d=10):
         torch.cuda.synchronize()
     return {"merge_ms": e[0].elapsed_time(e[1]), "iters3d": iters3d, "loop3d_ms": e[1].elapsed_time(e[2]),
             "total_ms": e[0].elapsed_time(e[2]), "volume": [n, n, n], "slices": P}
+
+
+UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns): 512 patterns, 18,612,224 pixels
+HIO_BYTES_PER_PIXEL = 24  # read+write x (complex64) + read A, S (float32) per HIO pattern-iteration
+
+
+def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
+    """The uneven-size configuration: 192 x 64^2, 192 x 128^2, 96 x 256^2 and
+    32 x 512^2 patterns (objects as in the plain 2D configuration, support
+    radius 0.19 of the side), 100 HIO iterations (beta 0.9) with shrinkwrap
+    every 20 (sigma 3 -> 1.5, threshold 0.1) from random-phase starts, in one
+    cpra_b200_hio_batched call; device time by CUDA events on the context's
+    stream.  Beside it the plain per-op path on the same GPU (torch.fft =
+    cuFFT plus torch element-wise kernels, same iteration, same starts) and
+    the mean R-factor of both paths' reconstructions per size."""
+    from cpra_b200 import synth
+    data = {}
+    for L, B in UNEVEN_SIZES:
+        d = synth.patterns_2d(count=B, n=L, radius=int(0.19 * L), seed=L)
+        data[L] = (d["A"], synth.autocorrelation_support(d["A"]), synth.random_phase_start(d["A"], seed=L + 1))
+    pixels = sum(L * L * B for L, B in UNEVEN_SIZES)
+    patterns = sum(B for _, B in UNEVEN_SIZES)
+    impl = cpra_b200.B200Impl(64, 64, 1, 1)
+    st = torch.cuda.ExternalStream(impl.stream(), device=dev)
+
+    def make():
+        out = []
+        for L, B in UNEVEN_SIZES:
+            A, S0, x0 = data[L]
+            b = {"side": L, "count": B, "x": torch.from_numpy(x0.ravel()).to(dev),
+                 "A": torch.from_numpy(A.ravel()).to(dev), "S": torch.from_numpy(S0.ravel()).to(dev)}
+            b["estimate"] = torch.empty_like(b["x"])
+            out.append(b)
+        torch.cuda.synchronize()
+        return out
+
+    impl.hio_batched(make(), sw_every, sw_every=sw_every)
+    impl.Sync()
+    best = None
+    for _ in range(reps):
+        bk = make()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = cpra_b200.kernels_launched()
+        e0.record(st)
+        impl.hio_batched(bk, iters, beta=0.9, sw_every=sw_every, sigma_start=3.0, sigma_end=1.5, threshold=0.1)
+        e1.record(st)
+        impl.Sync()
+        ms = e0.elapsed_time(e1)
+        if best is None or ms < best[0]:
+            best = (ms, bk, cpra_b200.kernels_launched() - n0)
+    ms, bk, launches = best
+    r_b200 = {}
+    for (L, B), b in zip(UNEVEN_SIZES, bk):
+        one = cpra_b200.B200Impl(L, L, 1, B)
+        r_b200[L] = float(np.mean(one.rfactor(b["estimate"], b["A"], B, a_stride=L * L)))
+        one.close()
+
+    # ---- the per-op path: same iteration with torch.fft and element-wise kernels ----
+    def per_op_run():
+        rs = {}
+        for L, B in UNEVEN_SIZES:
+            A, S0, x0 = data[L]
+            Ad = torch.from_numpy(A).to(dev)
+            S = torch.from_numpy(S0).to(dev) > 0.5
+            x = torch.from_numpy(x0).to(dev)
+            f = torch.fft.fftfreq(L, device=dev).abs() * L
+            n = torch.minimum(torch.arange(L, device=dev), L - torch.arange(L, device=dev)).double()
+            updates = iters // sw_every
+
+            def pm(t):
+                F = torch.fft.fftshift(torch.fft.fft2(torch.fft.ifftshift(t, dim=(-2, -1))), dim=(-2, -1))
+                mag = F.abs()
+                F = torch.where((Ad == 0) | (mag == 0), F, F * (Ad / mag.clamp_min(1e-30)))
+                return torch.fft.fftshift(torch.fft.ifft2(torch.fft.ifftshift(F, dim=(-2, -1))), dim=(-2, -1))
+
+            k = 0
+            for it in range(iters):
+                y = pm(x)
+                x = torch.where(S, y, x - 0.9 * y)
+                if (it + 1) % sw_every == 0:
+                    sg = 3.0 + (1.5 - 3.0) * k / (updates - 1) if updates > 1 else 3.0
+                    k += 1
+                    g = torch.exp(-n * n / (2 * sg * sg))
+                    g = torch.fft.fft(g / g.sum()).real.float()
+                    v = torch.fft.ifft2(torch.fft.fft2(x.abs()) * (g[:, None] * g[None, :])).real
+                    S = v > 0.1 * v.amax(dim=(-2, -1), keepdim=True)
+            est = torch.where(S, pm(x), torch.zeros_like(x))
+            rs[L] = (est, Ad)
+        return rs
+
+    per_op_run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rs = per_op_run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_perop = e0.elapsed_time(e1)
+    r_perop = {}
+    for L, B in UNEVEN_SIZES:
+        est, Ad = rs[L]
+        one = cpra_b200.B200Impl(L, L, 1, B)
+        r_perop[L] = float(np.mean(one.rfactor(est.contiguous().ravel(), Ad.contiguous().ravel(), B, a_stride=L * L)))
+        one.close()
+    impl.close()
+    peak, peak_kind = measured_peak()
+    value = patterns * iters / (ms / 1e3)
+    achieved = HIO_BYTES_PER_PIXEL * pixels * iters / (ms / 1e3) / 1e9
+    return {
+        "workload": "uneven-size HIO + shrinkwrap: 192x64^2, 192x128^2, 96x256^2, 32x512^2 complex64, "
+                    f"{iters} iterations, shrinkwrap every {sw_every}, one call",
+        "value": value, "unit": METRIC, "ms": ms, "gpu_launches": int(launches),
+        "pixel_iterations_per_s": pixels * iters / (ms / 1e3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "algorithmic_bytes": f"{HIO_BYTES_PER_PIXEL} B per pixel-iteration", "peak_kind": peak_kind},
+        "per_op_path": {"value": patterns * iters / (ms_perop / 1e3), "unit": METRIC, "ms": ms_perop,
+                        "impl": "torch.fft (cuFFT) + torch element-wise kernels, same iteration and starts"},
+        "speedup_vs_per_op": ms_perop / ms,
+        "rfactor_mean_b200": r_b200, "rfactor_mean_per_op": r_perop,
+    }
 
 
 if __name__ == "__main__":
