@@ -22,7 +22,7 @@ CSRC = PKG / "csrc"
 OUT_SO = PKG / "cpra_b200" / "libcpra_b200.so"
 BUILD = REPO / "_build" / "cpra_b200"
 
-SOURCES = ["kernels_fft.cu", "kernels_ew.cu", "kernels_dm.cu", "kernels_hio.cu", "kernels_adj.cu", "kernels_large.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["kernels_fft.cu", "kernels_ew.cu", "kernels_dm.cu", "kernels_hio.cu", "kernels_adj.cu", "kernels_large.cu", "kernels_dm_large.cu", "capi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -279,6 +279,23 @@ int exec_op(cpra_b200_ctx* c, const Op& op) {
     return fail(CPRA_B200_EARG, "unknown operator");
 }
 
+// fused difference-map iterations on either path: one CTA per pattern up to
+// 128 x 128, line passes through the work buffer at 256 and 512
+bool dm_fusable(const cpra_b200_ctx* c) {
+    return dm_fused_supported(c->dbl, c->m, c->n) || dm_large_supported(c->dbl, c->m, c->n, c->space_mode);
+}
+
+int run_dm(cpra_b200_ctx* c, const DmArgs& a, const char* what) {
+    if (dm_fused_supported(c->dbl, a.M, a.N)) {
+        CPRA_CHECK_CUDA(launch_dm_iterations(c->dbl, a, twiddles(c, a.M), c->stream), what);
+        return CPRA_B200_OK;
+    }
+    int r = ensure_work(c, dm_large_scratch_bytes(a.M, a.N, a.batch, a.s_stride));
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_dm_large(a, twiddles(c, a.M), c->work, c->stream), what);
+    return CPRA_B200_OK;
+}
+
 int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_NONE, const void* xprev = nullptr,
                  const void* xnext = nullptr, int init_from_x = 0) {
     DmArgs a;
@@ -312,7 +329,8 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
         }
         CPRA_CHECK_CUDA(cudaEventRecord(ev[0], c->stream), "cudaEventRecord");
     }
-    CPRA_CHECK_CUDA(launch_dm_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "fused difference-map iteration");
+    int r = run_dm(c, a, "fused difference-map iteration");
+    if (r) return r;
     if (c->timing) {
         CPRA_CHECK_CUDA(cudaEventRecord(ev[1], c->stream), "cudaEventRecord");
         c->timed.emplace_back(ev[0], ev[1]);
@@ -324,7 +342,7 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
 // `iters` iterations of pattern p: fused when the shape allows, else per call
 int dm_any(cpra_b200_ctx* c, const DmPattern& p, int iters) {
     if (iters <= 0) return CPRA_B200_OK;
-    if (dm_fused_supported(c->dbl, c->m, c->n)) return launch_fused(c, p, iters);
+    if (dm_fusable(c)) return launch_fused(c, p, iters);
     const uint64_t num = p.num;
     const uint64_t B = p.batch;
     for (int i = 0; i < iters; ++i) {
@@ -371,7 +389,7 @@ int take_deferred(cpra_b200_ctx* c) {
     return fail(rc, "deferred launch failed: " + c->deferred_msg);
 }
 
-bool fusable_shape(const cpra_b200_ctx* c) { return c->fusion && dm_fused_supported(c->dbl, c->m, c->n); }
+bool fusable_shape(const cpra_b200_ctx* c) { return c->fusion && dm_fusable(c); }
 
 // Does `op` extend the pending prefix (of length k) of the pattern?
 bool extends(const cpra_b200_ctx* c, const Op& op) {
@@ -817,8 +835,12 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* c, void* x, void* t1, void* t2, const
     if (batch == 0 || iters < 0) return fail(CPRA_B200_EARG, "dm_iterations: batch must be positive, iters >= 0");
     const double b = c->round_t(beta);
     if (b == 0.0) return fail(CPRA_B200_EARG, "dm_iterations: beta == 0");
-    if (!dm_fused_supported(c->dbl, c->m, c->n))
-        return fail(CPRA_B200_EUNSUP, "dm_iterations: fused path needs float and square 32, 64 or 128 planes");
+    if (!dm_fusable(c))
+        return fail(CPRA_B200_EUNSUP,
+                    "dm_iterations: fused path needs float and square 32, 64, 128 planes, or 256 and 512 with the "
+                    "threshold SpaceConstraint");
+    if (!dm_fused_supported(c->dbl, c->m, c->n) && s_stride != 0 && s_stride != c->plane())
+        return fail(CPRA_B200_EARG, "dm_iterations: at 256 and 512 s_stride must be 0 or m*n");
     int r = flush(c);
     if (r) return take_deferred(c);
     if (iters == 0) return CPRA_B200_OK;
@@ -839,8 +861,7 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* c, void* x, void* t1, void* t2, const
     a.data_mode = c->data_mode;
     a.c = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
            c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
-    CPRA_CHECK_CUDA(launch_dm_iterations(c->dbl, a, twiddles(c, c->m), c->stream), "dm_iterations");
-    return CPRA_B200_OK;
+    return run_dm(c, a, "dm_iterations");
 }
 
 int cpra_b200_rfactor(cpra_b200_ctx* c, const void* x, const void* A, uint64_t a_stride, uint64_t batch,
@@ -1236,7 +1257,7 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
         for (uint64_t p = 0; p < P; ++p) {
             const DmPattern pat = pattern(p, p);
             const bool err_here = want_err && e == epi - 1;
-            const bool fused = iters > 0 && dm_fused_supported(c->dbl, c->m, c->n);
+            const bool fused = iters > 0 && dm_fusable(c);
             if (fused && (!err_here || iters >= 2)) {
                 // carousel mix, t1 = t2 = x and the angle's iterations (all but
                 // the last one on an error-reporting angle) in one launch

@@ -106,6 +106,14 @@ struct DmArgs {
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
 
+// ---- the same iterations as line passes at 256 and 512 (kernels_dm_large.cu) ----
+// Float square planes with the threshold SpaceConstraint; S shared
+// (s_stride 0) or per pattern (s_stride M*N).  `scratch` holds
+// dm_large_scratch_bytes (the row spectra of both halves and the support mask).
+bool dm_large_supported(bool dbl, uint64_t M, uint64_t N, int space_mode);
+uint64_t dm_large_scratch_bytes(uint64_t M, uint64_t N, uint64_t batch, uint64_t s_stride);
+cudaError_t launch_dm_large(const DmArgs& a, const void* tw, void* scratch, cudaStream_t st);
+
 // ---- central slices and the amplitude-loss adjoints (kernels_adj.cu) --------
 // slices out[p] ([P][N][M]) of the [L][N][M] volume V at angles ang[p]
 cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, uint64_t m, uint64_t n, uint64_t p,

@@ -264,7 +264,9 @@ cudaError_t axis_pass(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi,
         case 32: return axis_fft_t<T, 32, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 64: return axis_fft_t<T, 64, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 128: return axis_fft_t<T, 128, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 256: return axis_fft_t<T, 256, 8>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        // 256 and 512: 16 threads per line, the split of the fused line passes
+        // (line_pass.cuh LineGeom), so those round exactly like these calls
+        case 256: return axis_fft_t<T, 256, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 512: return axis_fft_t<T, 512, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 1024: return axis_fft_t<T, 1024, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         default: return cudaErrorInvalidValue;

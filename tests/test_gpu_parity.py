@@ -289,7 +289,7 @@ def test_dm_iterations_vs_reference(tb, iters, fusion):
         assert O.rel_l2(host(v), G[f"dm{iters}_{name}"]) < FP32_DM_TOL * iters, name
 
 
-@pytest.mark.parametrize("L,B,iters", [(128, 3, 4), (64, 5, 3), (32, 2, 6)])
+@pytest.mark.parametrize("L,B,iters", [(128, 3, 4), (64, 5, 3), (32, 2, 6), (256, 2, 3), (512, 1, 2)])
 def test_fused_equals_per_call_bitwise(tb, L, B, iters):
     """One fused launch, the recorder-fused call stream and the per-call kernels
     write identical bits."""
@@ -317,11 +317,32 @@ def test_fused_equals_per_call_bitwise(tb, L, B, iters):
             np.testing.assert_array_equal(a, b)
 
 
-def test_fused_per_pattern_constraints(tb):
+@pytest.mark.parametrize("L,B,iters", [(256, 2, 3), (512, 1, 2)])
+def test_dm_large_vs_oracle(tb, L, B, iters):
+    """The 256 / 512 line-pass iterations against the float64-inside oracle:
+    <= 1e-5 relative L2 per iteration for x, t1 and t2."""
+    torch, cb = tb
+    rng = np.random.default_rng(L)
+    num = L * L * B
+    amps = (rng.uniform(0, 40, L * L) * (rng.uniform(0, 1, L * L) > 0.1)).astype(np.float32)
+    sup = (rng.uniform(0, 1, L * L) > 0.5).astype(np.float32)
+    x0 = (rng.uniform(0, 1, num) + 1j * rng.uniform(0, 1, num)).astype(np.complex64)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    x, t1, t2 = (dev(torch, x0) for _ in range(3))
+    assert impl.dm_iterations(x, t1, t2, dev(torch, amps), dev(torch, sup), B, 0.9, iters) and impl.Sync()
+    o = O.OracleImpl(np.float32, L, L, 1, B)
+    xo, t1o, t2o = x0.copy(), x0.copy(), x0.copy()
+    for _ in range(iters):
+        O.dm_iteration(o, xo, t1o, t2o, amps, sup, num, B, 0.9)
+    for got, want in ((x, xo), (t1, t1o), (t2, t2o)):
+        assert O.rel_l2(host(got), want) < FP32_DM_TOL * iters
+
+
+@pytest.mark.parametrize("L,B,iters", [(64, 4, 3), (256, 2, 2)])
+def test_fused_per_pattern_constraints(tb, L, B, iters):
     """dm_iterations with per-pattern modulus/support planes equals running each
     pattern on its own with a shared plane."""
     torch, cb = tb
-    L, B, iters = 64, 4, 3
     rng = np.random.default_rng(5)
     A = rng.uniform(0, 10, (B, L * L)).astype(np.float32)
     S = (rng.uniform(0, 1, (B, L * L)) > 0.4).astype(np.float32)
@@ -436,7 +457,8 @@ def test_real2d_to_3d_vs_oracle(tb):
     assert (want != 0).sum() > 0.05 * want.size
 
 
-@pytest.mark.parametrize("L,P,B,epi,it,pre", [(32, 4, 2, 2, 3, 4), (128, 5, 3, 2, 3, 2), (64, 3, 2, 1, 1, 0)])
+@pytest.mark.parametrize("L,P,B,epi,it,pre", [(32, 4, 2, 2, 3, 4), (128, 5, 3, 2, 3, 2), (64, 3, 2, 1, 1, 0),
+                                              (256, 3, 2, 2, 2, 1)])
 def test_cpra_run_equals_driver_bitwise(tb, L, P, B, epi, it, pre):
     """cpra_b200_cpra_run (carousel mix and t1 = t2 = x fused into each angle's
     launch) writes the same bits as the reference driver's call sequence issued
