@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
+    ap.add_argument("--case", choices=["carousel", "uneven"], default="carousel",
+                    help="uneven: only the uneven-size HIO measurement (one JSON line, for profiling runs)")
+    ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
+    ap.add_argument("--uneven-iters", type=int, default=100)
     return ap.parse_args()
 
 
@@ -324,6 +328,14 @@ def main():
     import cpra_b200
     from cpra_b200 import synth
 
+    if a.case == "uneven":
+        sizes = tuple(zip((64, 128, 256, 512), (int(v) for v in a.uneven_counts.split(","))))
+        out = uneven_batch(torch, cpra_b200, torch.device("cuda", local), iters=a.uneven_iters,
+                           sizes=tuple((L, B) for L, B in sizes if B > 0), per_op=not a.no_extras)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+
     M = N = a.size
     P, B, E, IT = a.angles, a.starts, a.episodes, a.iters
     MN = M * N
@@ -502,7 +514,7 @@ UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns)
 HIO_BYTES_PER_PIXEL = 24  # read+write x (complex64) + read A, S (float32) per HIO pattern-iteration
 
 
-def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
+def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2, sizes=UNEVEN_SIZES, per_op=True):
     """The uneven-size configuration: 192 x 64^2, 192 x 128^2, 96 x 256^2 and
     32 x 512^2 patterns (objects as in the plain 2D configuration, support
     radius 0.19 of the side), 100 HIO iterations (beta 0.9) with shrinkwrap
@@ -513,17 +525,17 @@ def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
     the mean R-factor of both paths' reconstructions per size."""
     from cpra_b200 import synth
     data = {}
-    for L, B in UNEVEN_SIZES:
+    for L, B in sizes:
         d = synth.patterns_2d(count=B, n=L, radius=int(0.19 * L), seed=L)
         data[L] = (d["A"], synth.autocorrelation_support(d["A"]), synth.random_phase_start(d["A"], seed=L + 1))
-    pixels = sum(L * L * B for L, B in UNEVEN_SIZES)
-    patterns = sum(B for _, B in UNEVEN_SIZES)
+    pixels = sum(L * L * B for L, B in sizes)
+    patterns = sum(B for _, B in sizes)
     impl = cpra_b200.B200Impl(64, 64, 1, 1)
     st = torch.cuda.ExternalStream(impl.stream(), device=dev)
 
     def make():
         out = []
-        for L, B in UNEVEN_SIZES:
+        for L, B in sizes:
             A, S0, x0 = data[L]
             b = {"side": L, "count": B, "x": torch.from_numpy(x0.ravel()).to(dev),
                  "A": torch.from_numpy(A.ravel()).to(dev), "S": torch.from_numpy(S0.ravel()).to(dev)}
@@ -548,7 +560,7 @@ def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
             best = (ms, bk, cpra_b200.kernels_launched() - n0)
     ms, bk, launches = best
     r_b200 = {}
-    for (L, B), b in zip(UNEVEN_SIZES, bk):
+    for (L, B), b in zip(sizes, bk):
         one = cpra_b200.B200Impl(L, L, 1, B)
         r_b200[L] = float(np.mean(one.rfactor(b["estimate"], b["A"], B, a_stride=L * L)))
         one.close()
@@ -556,7 +568,7 @@ def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
     # ---- the per-op path: same iteration with torch.fft and element-wise kernels ----
     def per_op_run():
         rs = {}
-        for L, B in UNEVEN_SIZES:
+        for L, B in sizes:
             A, S0, x0 = data[L]
             Ad = torch.from_numpy(A).to(dev)
             S = torch.from_numpy(S0).to(dev) > 0.5
@@ -586,34 +598,37 @@ def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2):
             rs[L] = (est, Ad)
         return rs
 
-    per_op_run()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    rs = per_op_run()
-    e1.record()
-    torch.cuda.synchronize()
-    ms_perop = e0.elapsed_time(e1)
-    r_perop = {}
-    for L, B in UNEVEN_SIZES:
-        est, Ad = rs[L]
-        one = cpra_b200.B200Impl(L, L, 1, B)
-        r_perop[L] = float(np.mean(one.rfactor(est.contiguous().ravel(), Ad.contiguous().ravel(), B, a_stride=L * L)))
-        one.close()
+    ms_perop, r_perop = None, {}
+    if per_op:
+        per_op_run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rs = per_op_run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms_perop = e0.elapsed_time(e1)
+        for L, B in sizes:
+            est, Ad = rs[L]
+            one = cpra_b200.B200Impl(L, L, 1, B)
+            r_perop[L] = float(np.mean(one.rfactor(est.contiguous().ravel(), Ad.contiguous().ravel(), B,
+                                                   a_stride=L * L)))
+            one.close()
     impl.close()
     peak, peak_kind = measured_peak()
     value = patterns * iters / (ms / 1e3)
     achieved = HIO_BYTES_PER_PIXEL * pixels * iters / (ms / 1e3) / 1e9
     return {
-        "workload": "uneven-size HIO + shrinkwrap: 192x64^2, 192x128^2, 96x256^2, 32x512^2 complex64, "
-                    f"{iters} iterations, shrinkwrap every {sw_every}, one call",
+        "workload": "uneven-size HIO + shrinkwrap: " + ", ".join(f"{B}x{L}^2" for L, B in sizes)
+                    + f" complex64, {iters} iterations, shrinkwrap every {sw_every}, one call",
         "value": value, "unit": METRIC, "ms": ms, "gpu_launches": int(launches),
         "pixel_iterations_per_s": pixels * iters / (ms / 1e3),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "algorithmic_bytes": f"{HIO_BYTES_PER_PIXEL} B per pixel-iteration", "peak_kind": peak_kind},
-        "per_op_path": {"value": patterns * iters / (ms_perop / 1e3), "unit": METRIC, "ms": ms_perop,
-                        "impl": "torch.fft (cuFFT) + torch element-wise kernels, same iteration and starts"},
-        "speedup_vs_per_op": ms_perop / ms,
+        "per_op_path": None if ms_perop is None else {
+            "value": patterns * iters / (ms_perop / 1e3), "unit": METRIC, "ms": ms_perop,
+            "impl": "torch.fft (cuFFT) + torch element-wise kernels, same iteration and starts"},
+        "speedup_vs_per_op": None if ms_perop is None else ms_perop / ms,
         "rfactor_mean_b200": r_b200, "rfactor_mean_per_op": r_perop,
     }
 

@@ -140,7 +140,10 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_cols(const DmlDev p) {
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
     Cx<float>* tw = buf + L * CS;
     float* As = reinterpret_cast<float*>(tw + B::F::TW_ENTRIES);
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
+    // two columns per warp, interleaved: each half-warp (which a 64-bit shared
+    // access serves as one unit) reads 8 ranks of both columns, 16 distinct
+    // 8-byte bank pairs at the tile pitch CS
+    const int t = threadIdx.x, line = 2 * (t >> 5) + (t & 1), q = (t & 31) >> 1;
     constexpr int TILES = L / LN;
     const uint64_t pl = blockIdx.x / TILES, b = pl / 2;
     const int c0 = (int)(blockIdx.x % TILES) * LN;

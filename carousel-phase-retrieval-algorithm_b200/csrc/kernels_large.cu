@@ -40,10 +40,11 @@ struct Big {
     // a row tile's Y and x stage in about 70 KB and three CTAs share an SM
     static constexpr int LINES = (L >= 512) ? 8 : 16;
     static constexpr int THREADS = LINES * TPL;
-    // column tile pitches (16-byte rows for the asynchronous copies):
-    // CS = LINES + 2 complex puts the 16 ranks x 2 columns of a warp's reads
-    // on 16 distinct 8-byte bank pairs (two wavefronts, the minimum); the A
-    // tile's AS = LINES + 4 floats costs at most two wavefronts per read
+    // column tile pitches (16-byte rows for the asynchronous copies): with two
+    // columns interleaved per warp (k_big_cols), CS = LINES + 2 complex puts
+    // each half-warp's 8-byte accesses (8 ranks x 2 columns) on 16 distinct
+    // bank pairs; the A tile's AS = LINES + 4 floats costs at most two
+    // wavefronts per read
     static constexpr int CS = LINES + 2;
     static constexpr int AS = LINES + 4;
     using F = LineFFT<float, L, TPL>;
@@ -136,7 +137,10 @@ __global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_cols(Cx<float>* __re
     Cx<float>* tw = buf + L * CS;
     float* As = reinterpret_cast<float*>(tw + B::F::TW_ENTRIES);
     float* gt = As + L * AS;
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
+    // two columns per warp, interleaved: each half-warp (which a 64-bit shared
+    // access serves as one unit) reads 8 ranks of both columns, 16 distinct
+    // 8-byte bank pairs at the tile pitch CS
+    const int t = threadIdx.x, line = 2 * (t >> 5) + (t & 1), q = (t & 31) >> 1;
     constexpr int TILES = L / LN;
     const uint64_t b = blockIdx.x / TILES;
     const int c0 = (int)(blockIdx.x % TILES) * LN;
