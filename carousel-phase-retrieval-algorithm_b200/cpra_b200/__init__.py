@@ -21,12 +21,12 @@ from pathlib import Path
 __all__ = [
     "IMPL_TYPE", "CpraB200Error", "B200Impl", "NewCpraImpl", "library_path", "lib",
     "OK", "EARG", "ECUDA", "EUNSUP", "OPT_FUSION", "OPT_SPACE_MODE", "OPT_DATA_MODE", "OPT_SEED",
-    "OPT_KERNEL_TIMING", "OPT_HIO_CHUNK",
+    "OPT_KERNEL_TIMING", "OPT_HIO_CHUNK", "OPT_GRAPH",
 ]
 
 OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
 F32, F64 = 0, 1
-OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_CHUNK = 1, 2, 3, 4, 5, 6
+OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_CHUNK, OPT_GRAPH = 1, 2, 3, 4, 5, 6, 7
 
 _HERE = Path(__file__).resolve().parent
 

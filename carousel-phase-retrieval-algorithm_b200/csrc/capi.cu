@@ -122,6 +122,13 @@ std::vector<T> twiddle_table(uint64_t L) {
 
 }  // namespace
 
+struct GraphEntry {
+    std::string key;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+    uint64_t epoch = 0;
+};
+
 struct BucketLane {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
@@ -167,6 +174,12 @@ struct cpra_b200_ctx {
     // streams, join events and scratch of cpra_b200_hio_batched's buckets
     std::vector<BucketLane> bucket_streams;
     cudaEvent_t fork_event = nullptr;
+    // CUDA graphs of cpra_run / hio_batched calls (CPRA_B200_OPT_GRAPH): one
+    // per distinct argument set, valid while no context buffer has moved
+    bool graphs = false;
+    bool capturing = false;
+    uint64_t epoch = 0;  // bumped whenever a context buffer is freed or reallocated
+    std::vector<GraphEntry> graph_cache;
     // patterns per chunk of the large-plane HIO passes (0: the whole batch)
     uint64_t hio_chunk = 0;
 
@@ -206,6 +219,7 @@ int ensure_twiddles(cpra_b200_ctx* c, uint64_t L) {
 
 int ensure_work(cpra_b200_ctx* c, uint64_t bytes) {
     if (c->work_bytes >= bytes) return CPRA_B200_OK;
+    ++c->epoch;
     if (c->work) {
         cudaStreamSynchronize(c->stream);
         cudaFree(c->work);
@@ -219,6 +233,7 @@ int ensure_work(cpra_b200_ctx* c, uint64_t bytes) {
 
 int ensure_reduction(cpra_b200_ctx* c, uint64_t members) {
     if (c->red_cap >= members) return CPRA_B200_OK;
+    ++c->epoch;
     if (c->partials) {
         cudaStreamSynchronize(c->stream);
         cudaFree(c->partials);
@@ -318,7 +333,8 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
     a.data_mode = c->data_mode;
     a.c = p.c;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    if (c->timing) {
+    const bool timed = c->timing && !c->capturing;  // graph replays are not timed per launch
+    if (timed) {
         for (cudaEvent_t& e : ev) {
             if (!c->free_events.empty()) {
                 e = c->free_events.back();
@@ -331,7 +347,7 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
     }
     int r = run_dm(c, a, "fused difference-map iteration");
     if (r) return r;
-    if (c->timing) {
+    if (timed) {
         CPRA_CHECK_CUDA(cudaEventRecord(ev[1], c->stream), "cudaEventRecord");
         c->timed.emplace_back(ev[0], ev[1]);
         c->timed_pattern_iters += c->batch * (uint64_t)iters;
@@ -563,6 +579,7 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
     }
     if (c->fork_event) cudaEventDestroy(c->fork_event);
+    for (GraphEntry& g : c->graph_cache) cudaGraphExecDestroy(g.exec);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -591,6 +608,13 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
             break;
         case CPRA_B200_OPT_SEED: c->seed = (uint64_t)value; c->init_calls = 0; break;
         case CPRA_B200_OPT_KERNEL_TIMING: c->timing = value != 0; break;
+        case CPRA_B200_OPT_GRAPH:
+            c->graphs = value != 0;
+            if (!c->graphs) {
+                for (GraphEntry& g : c->graph_cache) cudaGraphExecDestroy(g.exec);
+                c->graph_cache.clear();
+            }
+            break;
         case CPRA_B200_OPT_HIO_CHUNK:
             if (value < 0) return fail(CPRA_B200_EARG, "hio chunk must be >= 0");
             c->hio_chunk = (uint64_t)value;
@@ -1006,6 +1030,60 @@ int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t 
     return CPRA_B200_OK;
 }
 
+extern "C++" {
+// Runs `enqueue` (stream work only: no allocation, no synchronisation) on the
+// context's stream, or, with CPRA_B200_OPT_GRAPH on, replays the CUDA graph
+// captured from it for the same key, capturing it on the first call.  A
+// graph holds the context buffers' addresses, so it is used only while the
+// context's buffer epoch is the one it was captured in.
+template <class Fn>
+int run_maybe_graph(cpra_b200_ctx* c, const std::string& key, Fn enqueue) {
+    if (!c->graphs) return enqueue();
+    for (GraphEntry& g : c->graph_cache) {
+        if (g.key == key && g.epoch == c->epoch) {
+            CPRA_CHECK_CUDA(cudaGraphLaunch(g.exec, c->stream), "cudaGraphLaunch");
+            count_launches(g.launches);
+            return CPRA_B200_OK;
+        }
+    }
+    const uint64_t n0 = g_launches.load(std::memory_order_relaxed);
+    CPRA_CHECK_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    c->capturing = true;
+    const uint64_t epoch0 = c->epoch;
+    int r = enqueue();
+    c->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (r || e != cudaSuccess || c->epoch != epoch0) {
+        if (graph) cudaGraphDestroy(graph);
+        if (r) return r;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        return fail(CPRA_B200_ECUDA, "graph capture: a context buffer moved during capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+    // the capture counted the graph's kernels once, for this first launch
+    const uint64_t launches = g_launches.load(std::memory_order_relaxed) - n0;
+    if (c->graph_cache.size() >= 16) {
+        cudaGraphExecDestroy(c->graph_cache.front().exec);
+        c->graph_cache.erase(c->graph_cache.begin());
+    }
+    c->graph_cache.push_back(GraphEntry{key, exec, launches, c->epoch});
+    CPRA_CHECK_CUDA(cudaGraphLaunch(exec, c->stream), "cudaGraphLaunch");
+    return CPRA_B200_OK;
+}
+
+// a graph cache key: the raw bytes of the values
+template <class... V>
+std::string graph_key(const char* tag, const V&... v) {
+    std::string k(tag);
+    (k.append(reinterpret_cast<const char*>(&v), sizeof(V)), ...);
+    return k;
+}
+}  // extern "C++"
+
 int hio_check_params(const HioParams& h, const char* who) {
     if (h.iters < 0) return fail(CPRA_B200_EARG, std::string(who) + ": iters must be >= 0");
     if (h.updates() > 0 && !(h.sigma_start > 0.0 && h.sigma_end > 0.0))
@@ -1015,6 +1093,7 @@ int hio_check_params(const HioParams& h, const char* who) {
 
 int ensure_buffer(cpra_b200_ctx* c, void** buf, uint64_t* have, uint64_t bytes, const char* what) {
     if (*have >= bytes) return CPRA_B200_OK;
+    ++c->epoch;
     if (*buf) {
         cudaDeviceSynchronize();
         cudaFree(*buf);
@@ -1101,20 +1180,26 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
             if (r) return r;
         }
     }
-    CPRA_CHECK_CUDA(cudaEventRecord(c->fork_event, c->stream), "hio_batched");
-    for (int k = 0; k < n_buckets; ++k) {
-        const cpra_b200_hio_bucket& b = buckets[order[k]];
-        BucketLane& lane = c->bucket_streams[k];
-        const uint64_t plane = b.side * b.side;
-        const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
-        CPRA_CHECK_CUDA(cudaStreamWaitEvent(lane.stream, c->fork_event, 0), "hio_batched");
-        r = hio_enqueue(c, HioJob{b.side, b.count, b.x, b.A, plane, b.S, plane, b.estimate}, h, chunk, lane.scratch,
-                        lane.stream);
-        if (r) return r;
-        CPRA_CHECK_CUDA(cudaEventRecord(lane.done, lane.stream), "hio_batched");
-        CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, lane.done, 0), "hio_batched");
-    }
-    return CPRA_B200_OK;
+    auto enqueue = [&]() -> int {
+        CPRA_CHECK_CUDA(cudaEventRecord(c->fork_event, c->stream), "hio_batched");
+        for (int k = 0; k < n_buckets; ++k) {
+            const cpra_b200_hio_bucket& b = buckets[order[k]];
+            BucketLane& lane = c->bucket_streams[k];
+            const uint64_t plane = b.side * b.side;
+            const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
+            CPRA_CHECK_CUDA(cudaStreamWaitEvent(lane.stream, c->fork_event, 0), "hio_batched");
+            int rr = hio_enqueue(c, HioJob{b.side, b.count, b.x, b.A, plane, b.S, plane, b.estimate}, h, chunk,
+                                 lane.scratch, lane.stream);
+            if (rr) return rr;
+            CPRA_CHECK_CUDA(cudaEventRecord(lane.done, lane.stream), "hio_batched");
+            CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, lane.done, 0), "hio_batched");
+        }
+        return CPRA_B200_OK;
+    };
+    std::string key = graph_key("hio_batched", n_buckets, iters, beta, sw_every, sigma_start, sigma_end, threshold,
+                                positivity, c->hio_chunk, c->data_mode);
+    for (int i = 0; i < n_buckets; ++i) key.append(reinterpret_cast<const char*>(&buckets[i]), sizeof(buckets[i]));
+    return run_maybe_graph(c, key, enqueue);
 }
 
 int cpra_b200_slice(cpra_b200_ctx* c, const void* V, const void* angles, uint64_t m, uint64_t n, uint64_t p,
@@ -1194,6 +1279,7 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
     const uint64_t MN = c->plane(), MNB = MN * batch;
     const uint64_t cb = MNB * c->csize();
     if (c->drv_bytes < 3 * cb) {
+        ++c->epoch;
         if (c->drv) {
             cudaStreamSynchronize(c->stream);
             cudaFree(c->drv);
@@ -1208,6 +1294,7 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
         r = ensure_reduction(c, batch);
         if (r) return r;
         if (c->err_cap < P * batch) {
+            ++c->epoch;
             if (c->err_sums) {
                 cudaStreamSynchronize(c->stream);
                 cudaFree(c->err_sums);
@@ -1220,6 +1307,14 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
             c->err_cap = P * batch;
         }
     }
+    // scratch of the fused large-plane iterations and of non-power-of-two
+    // transforms, reserved before any work is enqueued (and before a capture)
+    if (dm_fusable(c) && !dm_fused_supported(c->dbl, c->m, c->n)) {
+        r = ensure_work(c, dm_large_scratch_bytes(c->m, c->n, batch, 0));
+        if (r) return r;
+    }
+    r = ensure_work(c, batch * MN * c->csize());
+    if (r) return r;
     char* base = static_cast<char*>(x);
     char* t1 = static_cast<char*>(c->drv);
     char* t2 = t1 + cb;
@@ -1246,6 +1341,8 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
     auto copy = [&](void* dst, const void* src) {
         return cudaMemcpyAsync(dst, src, cb, cudaMemcpyDeviceToDevice, c->stream);
     };
+    auto enqueue = [&]() -> int {
+    int r = CPRA_B200_OK;
     // Step A (:35-55): pre-reconstruction of angle 0 with the first constraint planes
     if (pre_iter > 0) {
         CPRA_CHECK_CUDA(copy(t1, xp(0)), "cpra_run");
@@ -1310,10 +1407,18 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
             CPRA_CHECK_CUDA(copy(xp(p), t1), "cpra_run");
         }
     }
-    if (want_err) {
+    if (want_err)
         CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_err, c->err_sums, sizeof(double) * 2 * P * batch,
                                         cudaMemcpyDeviceToHost, c->stream),
                         "cpra_run");
+    return CPRA_B200_OK;
+    };
+    r = run_maybe_graph(c,
+                        graph_key("cpra_run", x, A, S, P, batch, epi, iters, pre_iter, b, final_step, want_err,
+                                  c->space_mode, c->data_mode, c->fusion),
+                        enqueue);
+    if (r) return r;
+    if (want_err) {
         CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "cpra_run");
         for (uint64_t i = 0; i < P * batch; ++i) {
             const double v = std::sqrt(c->host_err[2 * i]) / std::sqrt(c->host_err[2 * i + 1]);

@@ -747,3 +747,90 @@ def test_hio_batched_rejects_bad_buckets(tb):
     with pytest.raises(cb.CpraB200Error):
         impl.hio_batched([{"side": 96, "count": 1, "x": x, "A": A, "S": A}], 2)
     assert not impl.hio_batched([], 2)
+
+
+# ---- CUDA graphs of whole runs --------------------------------------------------------------
+@pytest.mark.parametrize("L", [64, 256])
+def test_cpra_run_graph_replay_bitwise(tb, L):
+    """With CPRA_B200_OPT_GRAPH the first cpra_run call is captured and later
+    identical calls replay the graph: same bits, same error output and the
+    same kernel count as running without graphs."""
+    torch, cb = tb
+    P, B, epi, it, pre = 3, 2, 2, 2, 1
+    rng = np.random.default_rng(L)
+    A = (rng.uniform(0, 30, (P, L * L)) * (rng.uniform(0, 1, (P, L * L)) > 0.1)).astype(np.float32)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(np.float32)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(np.complex64)
+    Ad, Sd = dev(torch, A.ravel()), dev(torch, S.ravel())
+    plain = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    xr = dev(torch, x0)
+    err_r = np.zeros(P * B, np.float32)
+    n0 = cb.kernels_launched()
+    assert plain.cpra_run(xr, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=True, err=err_r) and plain.Sync()
+    n_plain = cb.kernels_launched() - n0
+    g = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert g.set_option(cb.OPT_GRAPH, 1)
+    x = dev(torch, x0)
+    for rep in range(3):
+        x.copy_(dev(torch, x0))
+        err = np.zeros(P * B, np.float32)
+        n0 = cb.kernels_launched()
+        assert g.cpra_run(x, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=True, err=err) and g.Sync()
+        assert cb.kernels_launched() - n0 == n_plain
+        np.testing.assert_array_equal(host(x), host(xr))
+        np.testing.assert_array_equal(err, err_r)
+
+
+def test_graph_recaptured_after_buffers_move(tb):
+    """A call that grows a context buffer invalidates the cached graphs (they
+    hold its old address); the next run captures anew and stays exact."""
+    torch, cb = tb
+    L, P, B = 64, 3, 2
+    rng = np.random.default_rng(3)
+    A = rng.uniform(0, 30, (P, L * L)).astype(np.float32)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(np.float32)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(np.complex64)
+    Ad, Sd = dev(torch, A.ravel()), dev(torch, S.ravel())
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    xr = dev(torch, x0)
+    assert ref.cpra_run(xr, Ad, Sd, P, B, 1, 2, 0, 0.9) and ref.Sync()
+    g = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert g.set_option(cb.OPT_GRAPH, 1)
+    x = dev(torch, x0)
+    assert g.cpra_run(x, Ad, Sd, P, B, 1, 2, 0, 0.9) and g.Sync()
+    # rfactor over many patterns grows the context's work buffer
+    big = torch.zeros(64 * L * L, dtype=torch.complex64, device="cuda")
+    g.rfactor(big, Ad, 64)
+    x.copy_(dev(torch, x0))
+    assert g.cpra_run(x, Ad, Sd, P, B, 1, 2, 0, 0.9) and g.Sync()
+    np.testing.assert_array_equal(host(x), host(xr))
+
+
+def test_hio_batched_graph_replay_bitwise(tb):
+    torch, cb = tb
+    sizes = [(64, 2), (256, 1)]
+    data = {L: _hio_inputs(L, B, seed=L + 3) for L, B in sizes}
+
+    def buckets():
+        out = []
+        for L, B in sizes:
+            A, S0, x0 = data[L]
+            out.append({"side": L, "count": B, "x": dev(torch, x0.ravel()), "A": dev(torch, A.ravel()),
+                        "S": dev(torch, S0.ravel())})
+        return out
+
+    plain = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
+    want = buckets()
+    assert plain.hio_batched(want, 10, sw_every=5) and plain.Sync()
+    g = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
+    assert g.set_option(cb.OPT_GRAPH, 1)
+    bk = buckets()
+    for rep in range(2):
+        for (L, B), b in zip(sizes, bk):
+            A, S0, x0 = data[L]
+            b["x"].copy_(dev(torch, x0.ravel()))
+            b["S"].copy_(dev(torch, S0.ravel()))
+        assert g.hio_batched(bk, 10, sw_every=5) and g.Sync()
+        for b, w in zip(bk, want):
+            np.testing.assert_array_equal(host(b["x"]), host(w["x"]))
+            np.testing.assert_array_equal(host(b["S"]), host(w["S"]))
