@@ -87,6 +87,10 @@ _SIGS = {
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_void_p],
+    "cpra_b200_refine": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 +
+                        [C.c_int, C.c_double, C.c_double, C.c_void_p],
+    "cpra_b200_best_start": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
+                             C.c_void_p],
     "cpra_b200_hio_batched": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_double,
                               C.c_double, C.c_double, C.c_int],
     "cpra_b200_slice": [C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 + [C.c_void_p],
@@ -324,6 +328,28 @@ class B200Impl:
                                                int(l), _addr(grad_V), loss.ctypes.data_as(C.c_void_p),
                                                ga.ctypes.data_as(C.c_void_p)), "slice_loss_grad")
         return float(loss[0]), ga
+
+    def refine(self, V, angles, A, m, n, p, l, steps, lr_volume=1e-3, lr_angle=1e-3):
+        """Adam steps on the volume and the angles against the amplitude loss
+        (project-defined); V and angles are updated in place; returns the loss
+        before each step (numpy float64)."""
+        import numpy as np
+        loss = np.zeros(max(int(steps), 1), np.float64)
+        _check(lib().cpra_b200_refine(self._h, _addr(V), _addr(angles), _addr(A), int(m), int(n), int(p), int(l),
+                                      int(steps), float(lr_volume), float(lr_angle), loss.ctypes.data_as(C.c_void_p)),
+               "refine")
+        return loss[:int(steps)]
+
+    def best_start(self, x, A, P, batch, best_out=None):
+        """(best start index, per-start scores) by the mean R-factor over the
+        P angles (project-defined); best_out (device) receives its planes."""
+        import numpy as np
+        scores = np.zeros(int(batch), np.float64)
+        best = np.zeros(1, np.uint64)
+        _check(lib().cpra_b200_best_start(self._h, _addr(x), _addr(A), int(P), int(batch),
+                                          scores.ctypes.data_as(C.c_void_p), best.ctypes.data_as(C.c_void_p),
+                                          _addr(best_out)), "best_start")
+        return int(best[0]), scores
 
     def rfactor(self, x, A, batch, a_stride=0):
         """R-factor per pattern, sum | |Forward2D(x_b)| - A_b | / sum A_b in

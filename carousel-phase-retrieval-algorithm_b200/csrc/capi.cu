@@ -176,6 +176,11 @@ struct cpra_b200_ctx {
     cudaEvent_t fork_event = nullptr;
     // CUDA graphs of cpra_run / hio_batched calls (CPRA_B200_OPT_GRAPH): one
     // per distinct argument set, valid while no context buffer has moved
+    // cpra_b200_refine: gV, Adam moments, per-step losses; cpra_b200_best_start: sums
+    void* refine_buf = nullptr;
+    uint64_t refine_bytes = 0;
+    void* best_sums = nullptr;
+    uint64_t best_bytes = 0;
     bool graphs = false;
     bool capturing = false;
     uint64_t epoch = 0;  // bumped whenever a context buffer is freed or reallocated
@@ -580,6 +585,8 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     }
     if (c->fork_event) cudaEventDestroy(c->fork_event);
     for (GraphEntry& g : c->graph_cache) cudaGraphExecDestroy(g.exec);
+    if (c->refine_buf) cudaFree(c->refine_buf);
+    if (c->best_sums) cudaFree(c->best_sums);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -1238,6 +1245,103 @@ int cpra_b200_slice_loss_grad(cpra_b200_ctx* c, const void* V, const void* angle
         if (grad_angles_host) grad_angles_host[i] = c->host_sums[2 * i + 1];
     }
     if (loss_host) *loss_host = loss;
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_refine(cpra_b200_ctx* c, void* V, void* angles, const void* A, uint64_t m, uint64_t n, uint64_t p,
+                     uint64_t l, int steps, double lr_volume, double lr_angle, double* loss_host) {
+    CTX_OR_RETURN(c);
+    if (!V || !angles || !A) return fail(CPRA_B200_EARG, "refine: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0 || steps < 0) return fail(CPRA_B200_EARG, "refine: zero size or steps < 0");
+    if (p > 65535) return fail(CPRA_B200_EUNSUP, "refine: more than 65535 slices");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    if (steps == 0) return CPRA_B200_OK;
+    const uint64_t vox = l * n * m;
+    const uint64_t gbytes = vox * c->csize(), mbytes = (4 * vox + 2 * p) * c->esize();
+    const uint64_t mofs = (gbytes + 255) / 256 * 256, lofs = mofs + (mbytes + 255) / 256 * 256;
+    r = ensure_buffer(c, &c->refine_buf, &c->refine_bytes, lofs + sizeof(double) * (uint64_t)steps,
+                      "cudaMalloc(refine buffers)");
+    if (r) return r;
+    r = ensure_work(c, p * n * m * c->csize());  // G = dL/ds
+    if (r) return r;
+    r = ensure_reduction(c, p);
+    if (r) return r;
+    char* buf = static_cast<char*>(c->refine_buf);
+    void* gV = buf;
+    void* mom = buf + mofs;
+    double* loss_dev = reinterpret_cast<double*>(buf + lofs);
+    CPRA_CHECK_CUDA(cudaMemsetAsync(mom, 0, mbytes, c->stream), "refine");
+    for (int k = 1; k <= steps; ++k) {
+        CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, gV, m, n, p, l, c->partials, c->sums,
+                                               c->stream),
+                        "refine");
+        CPRA_CHECK_CUDA(launch_refine_step(c->dbl, V, angles, gV, mom, vox, p, c->sums, lr_volume, lr_angle, k,
+                                           loss_dev + (k - 1), c->stream),
+                        "refine");
+    }
+    if (loss_host) {
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(loss_host, loss_dev, sizeof(double) * steps, cudaMemcpyDeviceToHost, c->stream),
+                        "refine");
+        CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "refine");
+    }
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_best_start(cpra_b200_ctx* c, const void* x, const void* A, uint64_t P, uint64_t batch,
+                         double* scores_host, uint64_t* best_host, void* best_out) {
+    CTX_OR_RETURN(c);
+    if (!x || !A || !best_host) return fail(CPRA_B200_EARG, "best_start: null pointer");
+    if (P == 0 || batch == 0) return fail(CPRA_B200_EARG, "best_start: P and batch must be positive");
+    if (batch > 65535) return fail(CPRA_B200_EUNSUP, "best_start: batch above 65535");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n))
+        return fail(CPRA_B200_EUNSUP, "best_start: each plane size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t plane = c->plane(), bytes = batch * plane * c->csize();
+    r = ensure_reduction(c, batch);
+    if (r) return r;
+    r = ensure_work(c, 2 * bytes);
+    if (r) return r;
+    r = ensure_buffer(c, &c->best_sums, &c->best_bytes, sizeof(double) * 2 * P * batch, "cudaMalloc(best_start sums)");
+    if (r) return r;
+    char* F = static_cast<char*>(c->work);
+    double* sums = static_cast<double*>(c->best_sums);
+    for (uint64_t p = 0; p < P; ++p) {
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(F, static_cast<const char*>(x) + p * bytes, bytes, cudaMemcpyDefault, c->stream),
+                        "best_start");
+        CPRA_CHECK_CUDA(launch_fft2d(c->dbl, F, c->m, c->n, batch, false, 1.0, twiddles(c, c->m), twiddles(c, c->n),
+                                     F + bytes, c->stream),
+                        "best_start");
+        CPRA_CHECK_CUDA(launch_rfactor_sums(c->dbl, F, static_cast<const char*>(A) + p * plane * c->esize(), 0, plane,
+                                            batch, c->partials, sums + 2 * batch * p, c->stream),
+                        "best_start");
+    }
+    std::vector<double> h(2 * P * batch);
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(h.data(), sums, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream),
+                    "best_start");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "best_start");
+    uint64_t best = 0;
+    double best_score = 0.0;
+    for (uint64_t b = 0; b < batch; ++b) {
+        double acc = 0.0;
+        for (uint64_t p = 0; p < P; ++p) acc += h[2 * (batch * p + b)] / h[2 * (batch * p + b) + 1];
+        const double score = acc / (double)P;
+        if (scores_host) scores_host[b] = score;
+        if (b == 0 || score < best_score) {
+            best = b;
+            best_score = score;
+        }
+    }
+    *best_host = best;
+    if (best_out) {
+        const uint64_t pb = plane * c->csize();
+        for (uint64_t p = 0; p < P; ++p)
+            CPRA_CHECK_CUDA(cudaMemcpyAsync(static_cast<char*>(best_out) + p * pb,
+                                            static_cast<const char*>(x) + (p * batch + best) * pb, pb, cudaMemcpyDefault,
+                                            c->stream),
+                            "best_start");
+    }
     return CPRA_B200_OK;
 }
 

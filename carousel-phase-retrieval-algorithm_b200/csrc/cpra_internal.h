@@ -123,6 +123,12 @@ cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, ui
 cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
                                    uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
                                    cudaStream_t st);
+// one Adam step (step >= 1) on the volume (vox complex) and the P angles from
+// gV and the per-slice sums; moments: 4*vox + 2*P elements of the element
+// type, zero before step 1; loss <- sum_p sums[2p]
+cudaError_t launch_refine_step(bool dbl, void* V, void* ang, const void* gV, void* moments, uint64_t vox, uint64_t P,
+                               const double* sums, double lr_volume, double lr_angle, int step, double* loss,
+                               cudaStream_t st);
 
 // ---- fused HIO + shrinkwrap iterations (kernels_hio.cu) -----------------------
 struct HioArgs {

@@ -166,7 +166,61 @@ __global__ void k_slice_adjoint(const Cx<T>* __restrict__ G, const T* __restrict
     }
 }
 
+// Adam (Kingma & Ba, 2015), in the form with bias-corrected step and
+// denominator: m <- b1 m + (1-b1) g, v <- b2 v + (1-b2) g^2,
+// p <- p - (lr / c1) * m / (sqrt(v) / sqrt(c2) + eps), c_k = 1 - b_k^t.
+template <typename T>
+__device__ __forceinline__ void adam_apply(T& p, T g, T& m, T& v, T lr, T b1, T b2, T eps, T c1, T c2) {
+    m = b1 * m + (T(1) - b1) * g;
+    v = b2 * v + (T(1) - b2) * g * g;
+    p -= (lr / c1) * m / (sqrt(v) / sqrt(c2) + eps);
+}
+
+// the volume as 2 * count reals (re, im interleaved), moments alike
+template <typename T>
+__global__ void k_adam_volume(T* __restrict__ V, const T* __restrict__ g, T* __restrict__ m, T* __restrict__ v,
+                              uint64_t n, T lr, T b1, T b2, T eps, T c1, T c2) {
+    for (uint64_t i = tid_g(); i < n; i += str_g()) adam_apply(V[i], g[i], m[i], v[i], lr, b1, b2, eps, c1, c2);
+}
+
+// angles from the per-slice sums (sums[2p + 1] = dL/d ang[p]); loss[step] =
+// sum_p sums[2p] in index order (one thread: P is small)
+template <typename T>
+__global__ void k_adam_angles(T* __restrict__ ang, const double* __restrict__ sums, T* __restrict__ m,
+                              T* __restrict__ v, uint64_t P, T lr, T b1, T b2, T eps, T c1, T c2,
+                              double* __restrict__ loss) {
+    for (uint64_t i = tid_g(); i < P; i += str_g())
+        adam_apply(ang[i], (T)sums[2 * i + 1], m[i], v[i], lr, b1, b2, eps, c1, c2);
+    if (tid_g() == 0) {
+        double acc = 0.0;
+        for (uint64_t p = 0; p < P; ++p) acc += sums[2 * p];
+        *loss = acc;
+    }
+}
+
+template <typename T>
+cudaError_t refine_step_t(void* V, void* ang, const void* gV, void* mom, uint64_t vox, uint64_t P,
+                          const double* sums, double lr_v, double lr_a, int step, double* loss, cudaStream_t st) {
+    const T b1 = T(0.9), b2 = T(0.999), eps = T(1e-8);
+    const T c1 = T(1) - pow(b1, (T)step), c2 = T(1) - pow(b2, (T)step);
+    T* mv = static_cast<T*>(mom);
+    const uint64_t n = 2 * vox;
+    k_adam_volume<T><<<ew_grid(n, ADJ_THREADS), ADJ_THREADS, 0, st>>>(static_cast<T*>(V), static_cast<const T*>(gV), mv,
+                                                                       mv + n, n, (T)lr_v, b1, b2, eps, c1, c2);
+    k_adam_angles<T><<<1, 128, 0, st>>>(static_cast<T*>(ang), sums, mv + 2 * n, mv + 2 * n + P, P, (T)lr_a, b1, b2,
+                                        eps, c1, c2, loss);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t launch_refine_step(bool dbl, void* V, void* ang, const void* gV, void* moments, uint64_t vox, uint64_t P,
+                               const double* sums, double lr_volume, double lr_angle, int step, double* loss,
+                               cudaStream_t st) {
+    return dbl ? refine_step_t<double>(V, ang, gV, moments, vox, P, sums, lr_volume, lr_angle, step, loss, st)
+               : refine_step_t<float>(V, ang, gV, moments, vox, P, sums, lr_volume, lr_angle, step, loss, st);
+}
 
 cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, uint64_t m, uint64_t n, uint64_t p,
                          uint64_t l, cudaStream_t st) {

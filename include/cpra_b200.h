@@ -219,6 +219,27 @@ int cpra_b200_slice_loss_grad(cpra_b200_ctx* ctx, const void* V, const void* ang
                               uint64_t n, uint64_t p, uint64_t l, void* grad_V, double* loss_host,
                               double* grad_angles_host);
 
+/* Extension (project-defined): `steps` gradient-descent steps on the volume V
+ * ([l][n][m] complex, device, in/out) and the angles (device, element type,
+ * in/out) against the amplitude loss of cpra_b200_slice_loss_grad, with Adam
+ * (Kingma & Ba 2015; beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) and the
+ * learning rates lr_volume, lr_angle.  Gradients come from the hand-written
+ * adjoints each step (iterates are recomputed, not stored); the moments start
+ * at zero each call.  loss_host (may be null) receives the loss before each
+ * step; with it the call is synchronous. */
+int cpra_b200_refine(cpra_b200_ctx* ctx, void* V, void* angles, const void* A, uint64_t m, uint64_t n, uint64_t p,
+                     uint64_t l, int steps, double lr_volume, double lr_angle, double* loss_host);
+
+/* Extension: the best of the random starts, the step the reference's
+ * benchmark describes and omits (src/benchmark_mkl.cpp:127-138).  x is
+ * [P][batch][m][n] (the driver's layout), A is [P][m][n].  The score of start
+ * b is the mean over the P angles of its R-factor (cpra_b200_rfactor's
+ * definition, float64); best_host receives the lowest-score start (the first
+ * on ties), scores_host[batch] (may be null) the scores, and best_out (device
+ * [P][m][n] complex, may be null) that start's planes.  Synchronous. */
+int cpra_b200_best_start(cpra_b200_ctx* ctx, const void* x, const void* A, uint64_t P, uint64_t batch,
+                         double* scores_host, uint64_t* best_host, void* best_out);
+
 /* With CPRA_B200_OPT_KERNEL_TIMING on: total device time (ms) and number of
  * the fused difference-map launches since the last call, measured with CUDA
  * events on the context's stream; `pattern_iters` gets the patterns times

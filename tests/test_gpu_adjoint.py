@@ -133,3 +133,65 @@ def test_autograd_function_and_refinement(tb):
         opt.step()
         losses.append(loss.item())
     assert losses[-1] < 0.5 * losses[0], losses
+
+
+def test_refine_matches_torch_adam(tb):
+    """cpra_b200_refine (device-side Adam over the adjoints) follows the same
+    trajectory as torch.optim.Adam driven by the same gradients, and lowers the
+    loss of perturbed orientations."""
+    torch, cb = tb
+    M, P, L, steps = 16, 8, 16, 25
+    impl = cb.B200Impl(M, M, L, 1)
+    rng = np.random.default_rng(5)
+    Vt = (rng.standard_normal(L * M * M) + 1j * rng.standard_normal(L * M * M)).astype(np.complex64)
+    ang_t = np.deg2rad(np.linspace(10, 170, P)).astype(np.float32)
+    out = torch.zeros(P * M * M, dtype=torch.complex64, device="cuda")
+    impl.slice(torch.from_numpy(Vt).cuda(), torch.from_numpy(ang_t).cuda(), M, M, P, L, out)
+    impl.Sync()
+    A = out.abs().contiguous()
+    ang0 = (ang_t + np.deg2rad(rng.normal(0, 0.5, P))).astype(np.float32)
+
+    # torch Adam over the same C-ABI gradients
+    Vr = torch.view_as_real(torch.from_numpy(Vt).cuda()).clone().requires_grad_(True)
+    ang = torch.from_numpy(ang0).cuda().clone().requires_grad_(True)
+    opt = torch.optim.Adam([{"params": [ang], "lr": 1e-3}, {"params": [Vr], "lr": 1e-3}])
+    want = []
+    for _ in range(steps):
+        opt.zero_grad()
+        V = torch.view_as_complex(Vr.detach().contiguous())
+        gV = torch.zeros_like(V)
+        loss, ga = impl.slice_loss_grad(V, ang.detach().contiguous(), A, M, M, P, L, gV)
+        Vr.grad = torch.view_as_real(gV).clone()
+        ang.grad = torch.from_numpy(ga).to(ang)
+        opt.step()
+        want.append(loss)
+
+    V = torch.from_numpy(Vt).cuda().clone()
+    a = torch.from_numpy(ang0).cuda().clone()
+    got = impl.refine(V, a, A, M, M, P, L, steps, lr_volume=1e-3, lr_angle=1e-3)
+    assert got.shape == (steps,)
+    np.testing.assert_allclose(got, want, rtol=1e-4)
+    assert got[-1] < 0.5 * got[0], got
+    Vw = torch.view_as_complex(Vr.detach().contiguous()).cpu().numpy()
+    assert np.linalg.norm(V.cpu().numpy() - Vw) / np.linalg.norm(Vw) < 1e-4
+    np.testing.assert_allclose(a.cpu().numpy(), ang.detach().cpu().numpy(), rtol=0, atol=1e-6)
+
+
+def test_best_start(tb):
+    """The start whose planes produced the modulus data wins (R = 0); the
+    scores are the mean per-angle R-factors; best_out gathers its planes."""
+    torch, cb = tb
+    L, P, B, best = 64, 3, 5, 2
+    rng = np.random.default_rng(11)
+    x = (rng.standard_normal((P, B, L, L)) + 1j * rng.standard_normal((P, B, L, L))).astype(np.complex64)
+    A = np.stack([np.abs(np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(x[p, best])))) for p in range(P)])
+    A = A.astype(np.float32)
+    impl = cb.B200Impl(L, L, 1, B)
+    xd = torch.from_numpy(x.ravel()).cuda()
+    out = torch.zeros(P * L * L, dtype=torch.complex64, device="cuda")
+    b, scores = impl.best_start(xd, torch.from_numpy(A.ravel()).cuda(), P, B, best_out=out)
+    impl.Sync()
+    assert b == best
+    want = [np.mean([O.rfactor(x[p, k].ravel(), A[p].ravel(), L, L, 1) for p in range(P)]) for k in range(B)]
+    np.testing.assert_allclose(scores, want, rtol=1e-5, atol=1e-6)
+    np.testing.assert_array_equal(out.cpu().numpy().reshape(P, L, L), x[:, best])
