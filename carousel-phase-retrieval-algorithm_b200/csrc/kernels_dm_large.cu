@@ -85,9 +85,13 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_first(const DmlDev p) 
     B::F::fill_twiddles(tw, p.tw, t, B::THREADS);
     const uint64_t g = (uint64_t)blockIdx.x * B::LINES + line, b = g / L;
     const int r = (int)(g % L);
+    // distinct buffers (x is the angle's own plane, its neighbours' are
+    // others), so the loads of later elements need not wait for x's stores
     Cx<float>* __restrict__ X = p.x + g * L;
     const Cx<float>* __restrict__ T1 = p.t1 + g * L;
     const Cx<float>* __restrict__ T2 = p.t2 + g * L;
+    const Cx<float>* __restrict__ XP = p.xprev ? p.xprev + g * L : nullptr;
+    const Cx<float>* __restrict__ XN = p.xnext ? p.xnext + g * L : nullptr;
     const uint32_t* __restrict__ mr = p.mask + b * p.mask_stride + (uint64_t)r * B::MW;
     __syncthreads();  // twiddle table
 #pragma unroll 1
@@ -101,14 +105,13 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_first(const DmlDev p) 
             if (pl == 0) {
                 if (p.init_from_x) {
                     // the angle's start: carousel mix of x (src/CPRA_MKL.cpp:64-76), then t1 = x
-                    const uint64_t idx = g * L + n;
                     if (p.mix == MIX_FIRST) {
-                        xv = merge_apply(p.xnext[idx], xv, 0.5f, 0.5f);
+                        xv = merge_apply(XN[n], xv, 0.5f, 0.5f);
                     } else if (p.mix == MIX_LAST) {
-                        xv = merge_apply(p.xprev[idx], xv, 0.5f, 0.5f);
+                        xv = merge_apply(XP[n], xv, 0.5f, 0.5f);
                     } else if (p.mix == MIX_MIDDLE) {
-                        xv = merge_apply(p.xprev[idx], xv, 0.5f, 0.0f);
-                        xv = merge_apply(p.xnext[idx], xv, 0.5f, 1.0f);
+                        xv = merge_apply(XP[n], xv, 0.5f, 0.0f);
+                        xv = merge_apply(XN[n], xv, 0.5f, 1.0f);
                     }
                     if (p.mix != MIX_NONE) X[n] = xv;
                     z = xv;
