@@ -49,8 +49,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
-    ap.add_argument("--case", choices=["carousel", "uneven"], default="carousel",
-                    help="uneven: only the uneven-size HIO measurement (one JSON line, for profiling runs)")
+    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d"], default="carousel",
+                    help="uneven / carousel3d: only that side measurement (one JSON line, for profiling runs)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
     return ap.parse_args()
@@ -328,6 +328,12 @@ def main():
     import cpra_b200
     from cpra_b200 import synth
 
+    if a.case == "carousel3d":
+        out = carousel3d_adjoint(torch, cpra_b200, torch.device("cuda", local), n=a.size, P=a.angles,
+                                 B=a.starts, epi=a.episodes, iters=a.iters)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
     if a.case == "uneven":
         sizes = tuple(zip((64, 128, 256, 512), (int(v) for v in a.uneven_counts.split(","))))
         out = uneven_batch(torch, cpra_b200, torch.device("cuda", local), iters=a.uneven_iters,
@@ -462,6 +468,10 @@ def main():
             result["uneven_batch"] = uneven_batch(torch, cpra_b200, dev)
         except Exception as ex:
             result["uneven_batch"] = {"error": str(ex)[:200]}
+        try:
+            result["carousel3d_adjoint"] = carousel3d_adjoint(torch, cpra_b200, dev)
+        except Exception as ex:
+            result["carousel3d_adjoint"] = {"error": str(ex)[:200]}
 
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         rate, sample, cores = cpu_reference_rate(d["A"], d["S"], M, IT, a.cpu_seconds, os.cpu_count() or 1)
@@ -511,6 +521,110 @@ def episode_3d(torch, cpra_b200, d, dev, iters3d=10):
         torch.cuda.synchronize()
     return {"merge_ms": e[0].elapsed_time(e[1]), "iters3d": iters3d, "loop3d_ms": e[1].elapsed_time(e[2]),
             "total_ms": e[0].elapsed_time(e[2]), "volume": [n, n, n], "slices": P}
+
+
+def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=10, refine_steps=50):
+    """The 256^3 carousel with adjoint refinement: a 256^3 volume of 64
+    ellipsoids, 180 angles at 1 degree jittered by N(0, 0.3 degree), 256^2
+    patterns at 1e8 photons (synthesised on the GPU, cpra_b200.synth.
+    carousel_gpu).  Timed by CUDA events on the contexts' streams:
+      * the 2D stage: cpra_run, 10 episodes x 10 DM iterations per angle over B
+        random starts, with the convergence error and the final projection
+        (the line-pass DM kernels at 256^2), pattern-iterations/s and the
+        roofline of the fused launches at 56 B per pattern-pixel; beside it the
+        DM iteration as torch.fft (cuFFT) plus torch element-wise kernels on
+        one angle's batch (per_op_compare);
+      * best start by mean R-factor, Forward2D of its planes and the trilinear
+        merge into a 256^3 Fourier volume;
+      * `refine_steps` Adam steps on the volume and the 180 angles (from the
+        nominal angles) through the hand-written adjoints."""
+    from cpra_b200 import synth
+    t0 = time.perf_counter()
+    d = synth.carousel_gpu(torch, n=n, P=P, device=dev)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    A, S = d["A"].reshape(-1), d["S"].reshape(-1)
+    impl = cpra_b200.B200Impl(n, n, 1, B)
+    impl.set_option(cpra_b200.OPT_SEED, 99)
+    x0 = torch.empty(P * B * n * n, dtype=torch.complex64, device=dev)
+    impl.Initialize(torch.view_as_real(x0), 2 * x0.numel())
+    impl.Sync()
+    x = torch.empty_like(x0)
+    err = np.zeros(P * B, np.float32)
+    st = torch.cuda.ExternalStream(impl.stream(), device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def run2d(e, it, timing=False):
+        x.copy_(x0)
+        torch.cuda.synchronize()
+        if timing:
+            impl.set_option(cpra_b200.OPT_KERNEL_TIMING, 1)
+            impl.kernel_timing()
+        ev[0].record(st)
+        impl.cpra_run(x, A, S, P, B, e, it, 0, 0.9, final_step=True, err=err)
+        ev[1].record(st)
+        impl.Sync()
+        kt = impl.kernel_timing() if timing else None
+        if timing:
+            impl.set_option(cpra_b200.OPT_KERNEL_TIMING, 0)
+        return ev[0].elapsed_time(ev[1]), kt
+
+    run2d(1, 2)
+    ms2d, kt = run2d(epi, iters, timing=True)
+    units = P * B * epi * iters
+    peak, peak_kind = measured_peak()
+    roof = None
+    if kt and kt[1] > 0:
+        achieved = DM_BYTES_PER_PIXEL * n * n * kt[2] / (kt[0] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "kernels": "k_dml_first/k_dml_cols/k_dml_rows<256> (fused DM line passes)",
+                "fused_ms": kt[0], "share_of_stage": kt[0] / ms2d, "peak_kind": peak_kind}
+    try:
+        per_op = per_op_compare(torch, cpra_b200, d["A"].cpu().numpy(), d["S"].cpu().numpy(), B, n, iters)
+    except Exception as ex:  # the comparison must not sink the measurement
+        per_op = {"error": str(ex)[:200]}
+
+    planes = torch.empty(P * n * n, dtype=torch.complex64, device=dev)
+    best, scores = impl.best_start(x, A, P, B, best_out=planes)
+    impl2 = cpra_b200.B200Impl(n, n, 1, P)
+    impl3 = cpra_b200.B200Impl(n, n, n, 1)
+    V = torch.zeros(n ** 3, dtype=torch.complex64, device=dev)
+    st3 = torch.cuda.ExternalStream(impl3.stream(), device=dev)
+    impl.Sync()
+    torch.cuda.synchronize()
+    # the merge's slices are [P][N][M] with the rotated coordinate fastest
+    # (CUDA_Impl_Kernel.cuh:80-90); the patterns are [P][rotated][tilt axis]
+    A_sl = A.view(P, n, n).transpose(1, 2).contiguous().view(-1)
+    ev[0].record(st3)
+    impl2.Forward2D(planes)
+    impl2.Sync()
+    slices = planes.view(P, n, n).transpose(1, 2).contiguous().view(-1)
+    impl3.Complex2DTo3DInterpolation(slices, V, d["angles_nominal"], n, n, P, n)
+    ev[1].record(st3)
+    impl3.Sync()
+    merge_ms = ev[0].elapsed_time(ev[1])
+    ang = d["angles_nominal"].clone()
+    ev[0].record(st3)
+    losses = impl3.refine(V, ang, A_sl, n, n, P, n, refine_steps, lr_volume=1e-3, lr_angle=1e-3)
+    ev[1].record(st3)
+    impl3.Sync()
+    refine_ms = ev[0].elapsed_time(ev[1])
+    for o in (impl, impl2, impl3):
+        o.close()
+    return {
+        "workload": f"carousel 3D with adjoint refinement: {n}^3 volume (64 ellipsoids), {P} angles at 1 deg "
+                    f"jittered N(0, 0.3 deg), {n}^2 patterns at 1e8 photons; 2D stage {epi} episodes x {iters} DM "
+                    f"iterations x {B} starts; best start; merge; {refine_steps} Adam steps",
+        "stage2d": {"value": units / (ms2d / 1e3), "unit": METRIC, "ms": ms2d, "roofline": roof,
+                    "per_op_path": per_op,
+                    "convergence_error_median": float(np.median(err))},
+        "best_start": {"index": best, "mean_rfactor": float(scores[best]),
+                       "median_rfactor_over_starts": float(np.median(scores))},
+        "merge_ms": merge_ms,
+        "refine": {"steps": refine_steps, "ms": refine_ms, "ms_per_step": refine_ms / refine_steps,
+                   "loss_first": float(losses[0]), "loss_last": float(losses[-1])},
+        "data_generation_s": gen_s,
+    }
 
 
 UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns): 512 patterns, 18,612,224 pixels

@@ -124,3 +124,55 @@ def random_phase_start(A, seed=0):
     ph = np.exp(2j * np.pi * rng.uniform(size=A.shape))
     x = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(A * ph, axes=(-2, -1))), axes=(-2, -1))
     return x.astype(np.complex64)
+
+
+def carousel_gpu(torch, n=256, P=180, step_deg=1.0, jitter_deg=0.3, ellipsoids=64, axes=(4, 16), radius=None,
+                 photons=1e8, seed=3, device="cuda"):
+    """The carousel synthesis of ``carousel`` at sizes where numpy is too slow
+    (256^3 and up), on the GPU with torch: a real volume of random ellipsoids
+    inside a sphere, parallel projections at P angles (step_deg apart, each
+    jittered by N(0, jitter_deg)) about the same axis, Poisson-noised far-field
+    moduli and disc supports.  Data preparation only; trilinear resampling by
+    torch's grid_sample.  Returns dict(A, S [P][n][n] float32, angles_true,
+    angles_nominal [P] float32 radians, volume [n][n][n] float32), all on
+    `device`."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    radius = radius if radius is not None else 0.3125 * n
+    ax = torch.arange(n, device=device, dtype=torch.float32) - n / 2
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    vol = torch.zeros((n, n, n), device=device)
+    for _ in range(ellipsoids):
+        a = axes[0] + (axes[1] - axes[0]) * torch.rand(3, device=device, generator=g)
+        r = (radius - float(a.max())) * float(torch.rand(1, device=device, generator=g))
+        d = torch.randn(3, device=device, generator=g)
+        c = d / d.norm() * r
+        q, _ = torch.linalg.qr(torch.randn(3, 3, device=device, generator=g))
+        pts = torch.stack([z - c[0], y - c[1], x - c[2]], -1) @ q
+        inside = ((pts / a) ** 2).sum(-1) <= 1.0
+        vol += inside * (0.2 + 0.8 * float(torch.rand(1, device=device, generator=g)))
+        del pts, inside
+    vol[(z * z + y * y + x * x) > radius * radius] = 0
+    del z, y, x
+    nominal = torch.deg2rad(torch.arange(P, device=device, dtype=torch.float64) * step_deg)
+    true = nominal + torch.deg2rad(jitter_deg * torch.randn(P, device=device, generator=g, dtype=torch.float64))
+    # projection at angle a about the y axis: detector row u, integration w,
+    # x = cos(a) u + sin(a) w, z = -sin(a) u + cos(a) w (grid coordinates in [-1, 1])
+    lin = (torch.arange(n, device=device, dtype=torch.float32) + 0.5) / n * 2 - 1
+    w_, u_, y_ = torch.meshgrid(lin, lin, lin, indexing="ij")
+    src = vol[None, None]
+    proj = torch.empty((P, n, n), device=device)
+    for p in range(P):
+        ca, sa = float(torch.cos(true[p])), float(torch.sin(true[p]))
+        grid = torch.stack([ca * u_ + sa * w_, y_, -sa * u_ + ca * w_], -1)[None]
+        proj[p] = torch.nn.functional.grid_sample(src, grid, mode="bilinear", padding_mode="zeros",
+                                                  align_corners=False)[0, 0].sum(0)
+    del w_, u_, y_
+    F = torch.fft.fftshift(torch.fft.fft2(torch.fft.ifftshift(proj.double(), dim=(-2, -1))), dim=(-2, -1))
+    I = F.abs() ** 2
+    I = I * (photons / I.sum(dim=(-2, -1), keepdim=True))
+    A = torch.sqrt(torch.poisson(I, generator=g)).float()
+    yy, xx = torch.meshgrid(ax, ax, indexing="ij")
+    disc = ((yy * yy + xx * xx) <= (radius + 2) ** 2).float()
+    S = disc.expand(P, n, n).contiguous()
+    return {"A": A.contiguous(), "S": S, "angles_true": true.float(), "angles_nominal": nominal.float(),
+            "volume": vol}
