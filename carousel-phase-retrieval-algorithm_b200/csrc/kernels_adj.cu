@@ -122,47 +122,80 @@ __global__ void k_slice_residual(const Cx<T>* __restrict__ V, const T* __restric
     }
 }
 
-// gradient with respect to V: each voxel gathers w * G over the slices
+// gradient with respect to V: each voxel gathers w * G over the slices.  The
+// slices' sines, cosines and the reciprocals that bound each slice's rows are
+// staged per block in shared memory, ADJ_ANGLES at a time, so the voxel loop
+// evaluates no transcendental and no division.  The row window is computed in
+// float and widened by 0.01 of a row: it only bounds the loop (rows are
+// integers; its float rounding is below 1e-3 of a row at these coordinates),
+// and the double weights decide which rows contribute, exactly as before.
+constexpr int ADJ_ANGLES = 512;
+struct AngleRow {
+    double sa, ca;   // sin, cos
+    float isa, ica;  // 1/sin (0 when |sin| <= 1e-12), 1/cos (likewise)
+};
+
 template <typename T>
-__global__ void k_slice_adjoint(const Cx<T>* __restrict__ G, const T* __restrict__ ang, Cx<T>* __restrict__ gV,
-                                int64_t M, int64_t N, int64_t P, int64_t L) {
+__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __restrict__ G, const T* __restrict__ ang,
+                                                               Cx<T>* __restrict__ gV, int64_t M, int64_t N,
+                                                               int64_t P, int64_t L) {
+    __shared__ AngleRow tab[ADJ_ANGLES];
     const uint64_t total = (uint64_t)L * N * M;
-    for (uint64_t i = tid_g(); i < total; i += str_g()) {
-        const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
+    // every thread of the block runs the same number of outer iterations
+    const uint64_t iters = (total + str_g() - 1) / str_g();
+    for (uint64_t it = 0, i = tid_g(); it < iters; ++it, i += str_g()) {
+        const bool live = i < total;
+        const int64_t y = live ? (int64_t)(i % M) : 0, x = live ? (int64_t)((i / M) % N) : 0;
+        const int64_t z = live ? (int64_t)(i / ((uint64_t)M * N)) : 0;
+        const float czf = (float)(L / 2 - z), cyf = (float)(M / 2 - y);
         double re = 0.0, im = 0.0;
-        for (int64_t p = 0; p < P; ++p) {
-            const double a = (double)ang[p];
-            const double sa = sin(a), ca = cos(a);
-            // rows whose point (zf, yf) = (L/2 - yr sa, M/2 - yr ca) lies within 1 of (z, y) in both axes
-            double lo = -1e300, hi = 1e300;
-            const double cz = (double)(L / 2) - (double)z, cy = (double)(M / 2) - (double)y;
-            if (fabs(sa) > 1e-12) {
-                const double r0 = (cz - 1.0) / sa, r1 = (cz + 1.0) / sa;
-                lo = fmax(lo, fmin(r0, r1));
-                hi = fmin(hi, fmax(r0, r1));
-            } else if (fabs(cz) >= 1.0) {
-                continue;
+        for (int64_t p0 = 0; p0 < P; p0 += ADJ_ANGLES) {
+            const int64_t np = (P - p0 < ADJ_ANGLES) ? P - p0 : ADJ_ANGLES;
+            __syncthreads();
+            for (int64_t k = threadIdx.x; k < np; k += ADJ_THREADS) {
+                const double a = (double)ang[p0 + k];
+                const double sa = sin(a), ca = cos(a);
+                tab[k] = AngleRow{sa, ca, fabs(sa) > 1e-12 ? (float)(1.0 / sa) : 0.0f,
+                                  fabs(ca) > 1e-12 ? (float)(1.0 / ca) : 0.0f};
             }
-            if (fabs(ca) > 1e-12) {
-                const double r0 = (cy - 1.0) / ca, r1 = (cy + 1.0) / ca;
-                lo = fmax(lo, fmin(r0, r1));
-                hi = fmin(hi, fmax(r0, r1));
-            } else if (fabs(cy) >= 1.0) {
-                continue;
-            }
-            for (int64_t yr = (int64_t)ceil(lo); (double)yr <= hi; ++yr) {
-                const int64_t yIn = M / 2 - yr;
-                if (yIn < 0 || yIn >= M) continue;
-                const double wz = 1.0 - fabs((double)(L / 2) - (double)yr * sa - (double)z);
-                const double wy = 1.0 - fabs((double)(M / 2) - (double)yr * ca - (double)y);
-                if (!(wz > 0.0) || !(wy > 0.0)) continue;
-                const Cx<T> g = G[(p * N + x) * M + yIn];
-                const double w = wz * wy;
-                re += w * (double)g.x;
-                im += w * (double)g.y;
+            __syncthreads();
+            if (!live) continue;
+            for (int64_t k = 0; k < np; ++k) {
+                const AngleRow w = tab[k];
+                // rows whose point (zf, yf) = (L/2 - yr sa, M/2 - yr ca) lies within 1 of (z, y) in both axes
+                float lo = -3.0e38f, hi = 3.0e38f;
+                if (w.isa != 0.0f) {
+                    const float r0 = (czf - 1.0f) * w.isa, r1 = (czf + 1.0f) * w.isa;
+                    lo = fmaxf(lo, fminf(r0, r1));
+                    hi = fminf(hi, fmaxf(r0, r1));
+                } else if (fabsf(czf) >= 1.0f) {
+                    continue;
+                }
+                if (w.ica != 0.0f) {
+                    const float r0 = (cyf - 1.0f) * w.ica, r1 = (cyf + 1.0f) * w.ica;
+                    lo = fmaxf(lo, fminf(r0, r1));
+                    hi = fminf(hi, fmaxf(r0, r1));
+                } else if (fabsf(cyf) >= 1.0f) {
+                    continue;
+                }
+                if (lo > hi + 0.02f) continue;
+                lo = fmaxf(lo, (float)(-M));  // rows outside the slice never contribute
+                hi = fminf(hi, (float)M);
+                const int64_t p = p0 + k;
+                for (int64_t yr = (int64_t)ceilf(lo - 0.01f); (float)yr <= hi + 0.01f; ++yr) {
+                    const int64_t yIn = M / 2 - yr;
+                    if (yIn < 0 || yIn >= M) continue;
+                    const double wz = 1.0 - fabs((double)(L / 2) - (double)yr * w.sa - (double)z);
+                    const double wy = 1.0 - fabs((double)(M / 2) - (double)yr * w.ca - (double)y);
+                    if (!(wz > 0.0) || !(wy > 0.0)) continue;
+                    const Cx<T> g = G[(p * N + x) * M + yIn];
+                    const double wt = wz * wy;
+                    re += wt * (double)g.x;
+                    im += wt * (double)g.y;
+                }
             }
         }
-        gV[i] = Cx<T>{(T)re, (T)im};
+        if (live) gV[i] = Cx<T>{(T)re, (T)im};
     }
 }
 
