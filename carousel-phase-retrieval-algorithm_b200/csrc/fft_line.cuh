@@ -70,9 +70,24 @@ __device__ __forceinline__ int xslot(int m, int q) { return m * TPL + ((q + m) &
 template <typename T, int L, int TPL>
 struct LineFFT {
     static constexpr int R = L / TPL;
-    static constexpr int J = R / TPL;
+    // HALF: R = TPL / 2 (512 points over 32 threads, 16 values each); the
+    // TPL-point second stage of each m is split over a lane pair by one
+    // radix-2 step (natural_to_split_flat).  Otherwise TPL <= R.
+    static constexpr bool HALF = (R < TPL);
+    static constexpr int J = HALF ? 1 : R / TPL;
     static_assert(TPL >= 1 && TPL <= 32 && (TPL & (TPL - 1)) == 0, "TPL must be a power of two <= 32");
-    static_assert(R <= 32 && R >= TPL, "need TPL <= R <= 32");
+    static_assert(R <= 32 && (R >= TPL || (2 * R == TPL && TPL == 32)), "need TPL <= R <= 32, or R = TPL / 2 = 16");
+
+    // Flat output layout of natural_to_split_flat: output i < R of rank q is
+    // element pos(q, i) of the transformed line.  For TPL <= R this is the
+    // split layout below, o[j][s] = flat[j * TPL + s]; for HALF, rank q holds
+    // X[(q >> 1) + R (q & 1) + TPL i].
+    __host__ __device__ __forceinline__ static constexpr int pos(int q, int i) {
+        if constexpr (HALF)
+            return (q >> 1) + R * (q & 1) + TPL * i;
+        else
+            return q + TPL * (i / TPL) + R * (i % TPL);
+    }
 
     // Twiddle table layout: twq[p * TWS + m] = exp(-2 pi i p m / L) for p < TPL,
     // m < R.  The row pitch R + 1 puts the TPL ranks' entries for one m on
@@ -95,6 +110,7 @@ struct LineFFT {
     template <bool INV>
     __device__ __forceinline__ static void natural_to_split(Cx<T> (&v)[R], Cx<T> (&o)[J][TPL], Cx<T>* scratch,
                                                             int ss, const Cx<T>* twq, int q) {
+        static_assert(!HALF || sizeof(T) == 0, "HALF lines use natural_to_split_flat");
         dft_regs<T, R, INV>(v);
         if constexpr (TPL == 1) {
 #pragma unroll
@@ -122,10 +138,48 @@ struct LineFFT {
         }
     }
 
+    // natural -> flat (pos above).  For TPL <= R this is natural_to_split with
+    // the outputs flattened.  For HALF: an R-point DFT over k of
+    // x[q + TPL k], the twiddle W_L^(q m), the exchange, then for m = q >> 1
+    // the TPL-point DFT over the ranks, X[m + R s] = sum_p W_TPL^(p s) Y_p[m],
+    // as its even (q even) or odd (q odd) outputs: an R-point DFT of
+    // Y_p + Y_(p+R), or of (Y_p - Y_(p+R)) W_TPL^p.
+    template <bool INV>
+    __device__ __forceinline__ static void natural_to_split_flat(Cx<T> (&v)[R], Cx<T> (&o)[R], Cx<T>* scratch,
+                                                                 int ss, const Cx<T>* twq, int q) {
+        if constexpr (!HALF) {
+            natural_to_split<INV>(v, reinterpret_cast<Cx<T>(&)[J][TPL]>(o), scratch, ss, twq, q);
+        } else {
+            dft_regs<T, R, INV>(v);
+            __syncwarp();
+#pragma unroll
+            for (int m = 0; m < R; ++m) {
+                Cx<T> y = v[brev<R>(m)];
+                if (m != 0) y = INV ? cmulc(y, twq[q * TWS + m]) : cmul(y, twq[q * TWS + m]);
+                scratch[xslot<TPL>(m, q) * ss] = y;
+            }
+            __syncwarp();
+            const int m = q >> 1;
+            const bool odd = (q & 1) != 0;
+            Cx<T> b[R];
+#pragma unroll
+            for (int p = 0; p < R; ++p) {
+                const Cx<T> a0 = scratch[xslot<TPL>(m, p) * ss];
+                const Cx<T> a1 = scratch[xslot<TPL>(m, p + R) * ss];
+                b[p] = odd ? rot32<T, INV>(csub(a0, a1), p) : cadd(a0, a1);  // W_32^p (TPL = 32)
+            }
+            dft_regs<T, R, INV>(b);
+#pragma unroll
+            for (int i = 0; i < R; ++i) o[i] = b[brev<R>(i)];
+            __syncwarp();
+        }
+    }
+
     // split -> natural (the reverse of natural_to_split's data movement)
     template <bool INV>
     __device__ __forceinline__ static void split_to_natural(Cx<T> (&o)[J][TPL], Cx<T> (&v)[R], Cx<T>* scratch,
                                                             int ss, const Cx<T>* twq, int q) {
+        static_assert(!HALF || sizeof(T) == 0, "HALF lines have no split_to_natural");
         if constexpr (TPL == 1) {
 #pragma unroll
             for (int m = 0; m < R; ++m) v[m] = o[m][0];

@@ -15,8 +15,9 @@
 // only by the last one.  D = (-1)^(row + col) folds the fftshifts; the two
 // around DataConstraint cancel (it commutes with the sign pattern).
 //
-// Every 1D transform is LineFFT::natural_to_split with the per-operator axis
-// passes' split (16 threads per line, kernels_fft.cu), fed in natural order,
+// Every 1D transform is LineFFT::natural_to_split_flat with the per-operator
+// axis passes' split (line_pass.cuh LineGeom: 16 threads per line at 256, 32
+// at 512), fed in natural order,
 // and the element-wise steps are ops_ew.cuh's, so a launch writes the same
 // bits as the 12 per-operator calls per iteration.  SpaceConstraint is the
 // threshold form (MKL_Impl.inl:70-84) through a bit mask of the support.
@@ -28,17 +29,13 @@ namespace cpra_b200 {
 namespace {
 
 template <int L>
-struct DmLP {
+struct DmLP : LineGeom<L> {
     using G = LineGeom<L>;
     using F = typename G::F;
-    static constexpr int TPL = G::TPL, R = G::R, J = G::J;
-    static constexpr int LINES = (L >= 512) ? 8 : 16;
-    static constexpr int THREADS = LINES * TPL;
-    static constexpr int CS = LINES + 2;  // column tile pitch (complex), as in kernels_large.cu
-    static constexpr int AS = LINES + 4;  // A tile pitch (floats)
-    static constexpr int MW = L / 32;     // mask words per row
-    static constexpr size_t tile = (size_t)LINES * L;
-    static_assert(L % LINES == 0, "a CTA's lines must belong to one pattern");
+    static constexpr int TPL = G::TPL, R = G::R, NT = G::THREADS;
+    static constexpr int RL = G::ROW_LINES, CL = G::COL_LINES, CS = G::CS, AS = G::AS;
+    static constexpr int MW = L / 32;  // mask words per row
+    static constexpr size_t tile = G::row_tile;
     // rows: Y1, Y2 and x tiles, twiddles, mask tile
     static constexpr size_t row_smem() { return sizeof(Cx<float>) * (3 * tile + F::TW_ENTRIES) + tile / 8; }
     static constexpr size_t col_smem() {
@@ -76,14 +73,16 @@ __global__ void k_dml_pack(const float* __restrict__ S, uint64_t s_stride, uint6
 }
 
 template <int L>
-__global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_first(const DmlDev p) {
+__global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_first(const DmlDev p) {
     using B = DmLP<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* scratch = reinterpret_cast<Cx<float>*>(smem_raw);
     Cx<float>* tw = scratch + B::tile;
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
-    B::F::fill_twiddles(tw, p.tw, t, B::THREADS);
-    const uint64_t g = (uint64_t)blockIdx.x * B::LINES + line, b = g / L;
+    const int t = threadIdx.x;
+    int line, q;
+    B::row_lane(t, line, q);
+    B::F::fill_twiddles(tw, p.tw, t, B::NT);
+    const uint64_t g = (uint64_t)blockIdx.x * B::RL + line, b = g / L;
     const int r = (int)(g % L);
     // distinct buffers (x is the angle's own plane, its neighbours' are
     // others), so the loads of later elements need not wait for x's stores
@@ -96,7 +95,7 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_first(const DmlDev p) 
     __syncthreads();  // twiddle table
 #pragma unroll 1
     for (int pl = 0; pl < 2; ++pl) {
-        Cx<float> v[B::R], o[B::J][B::TPL];
+        Cx<float> v[B::R], o[B::R];
 #pragma unroll
         for (int k = 0; k < B::R; ++k) {
             const int n = q + B::TPL * k;
@@ -124,85 +123,58 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_first(const DmlDev p) 
             }
             v[k] = flip(z, r + n);
         }
-        B::F::template natural_to_split<false>(v, o, scratch + line * L, 1, tw, q);
+        B::F::template natural_to_split_flat<false>(v, o, scratch + line * L, 1, tw, q);
         Cx<float>* __restrict__ yr = p.Y + ((2 * b + pl) * (uint64_t)L + r) * L;
 #pragma unroll
-        for (int j = 0; j < B::J; ++j)
-#pragma unroll
-            for (int s = 0; s < B::TPL; ++s) yr[B::G::split_pos(q, j, s)] = o[j][s];
+        for (int i = 0; i < B::R; ++i) yr[B::pos(q, i)] = o[i];
     }
 }
 
-// a tile of LINES columns of one plane (2 per pattern): forward column DFT,
+// a tile of column lines of one plane (2 per pattern): forward column DFT,
 // DataConstraint with the pattern's A, inverse column DFT, in place
 template <int L>
-__global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_cols(const DmlDev p) {
+__global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_cols(const DmlDev p) {
     using B = DmLP<L>;
-    constexpr int CS = B::CS, AS = B::AS, LN = B::LINES, NT = B::THREADS;
+    constexpr int CS = B::CS, AS = B::AS, LN = B::CL, NT = B::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
     Cx<float>* tw = buf + L * CS;
     float* As = reinterpret_cast<float*>(tw + B::F::TW_ENTRIES);
-    // two columns per warp, interleaved: each half-warp (which a 64-bit shared
-    // access serves as one unit) reads 8 ranks of both columns, 16 distinct
-    // 8-byte bank pairs at the tile pitch CS
-    const int t = threadIdx.x, line = 2 * (t >> 5) + (t & 1), q = (t & 31) >> 1;
+    const int t = threadIdx.x;
+    int line, q;
+    B::col_lane(t, line, q);
     constexpr int TILES = L / LN;
     const uint64_t pl = blockIdx.x / TILES, b = pl / 2;
     const int c0 = (int)(blockIdx.x % TILES) * LN;
     Cx<float>* __restrict__ P = p.Y + pl * (uint64_t)L * L + c0;
-    const float* __restrict__ Ab = p.A + b * p.a_stride + c0;
-    constexpr int YCH = LN / 2;
-    for (int i = t; i < L * YCH; i += NT) {
-        const int n = i / YCH, k = i % YCH;
-        cp_async16(buf + n * CS + 2 * k, P + (uint64_t)n * L + 2 * k);
-    }
-    if (p.vec_a) {
-        constexpr int ACH = LN / 4;
-        for (int i = t; i < L * ACH; i += NT) {
-            const int n = i / ACH, k = i % ACH;
-            cp_async16(As + n * AS + 4 * k, Ab + (uint64_t)n * L + 4 * k);
-        }
-    } else {
-        for (int i = t; i < L * LN; i += NT) {
-            const int n = i / LN, k = i % LN;
-            cp_async4(As + n * AS + k, Ab + (uint64_t)n * L + k);
-        }
-    }
+    stage_col_tile<L, LN, CS, AS>(buf, P, As, p.A + b * p.a_stride + c0, L, p.vec_a != 0, t, NT);
     cp_async_commit();
     B::F::fill_twiddles(tw, p.tw, t, NT);
     cp_async_wait<0>();
     __syncthreads();
     Cx<float>* col = buf + line;  // slot u of this column at col[u * CS]
-    Cx<float> v[B::R], o[B::J][B::TPL];
+    Cx<float> v[B::R], o[B::R];
 #pragma unroll
     for (int k = 0; k < B::R; ++k) v[k] = col[(q + B::TPL * k) * CS];
-    B::F::template natural_to_split<false>(v, o, col, CS, tw, q);
+    B::F::template natural_to_split_flat<false>(v, o, col, CS, tw, q);
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int f = B::G::split_pos(q, j, s);
-            col[f * CS] = data_apply(o[j][s], As[f * AS + line], p.data_mode);
-        }
+    for (int i = 0; i < B::R; ++i) {
+        const int f = B::pos(q, i);
+        col[f * CS] = data_apply(o[i], As[f * AS + line], p.data_mode);
+    }
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < B::R; ++k) v[k] = col[(q + B::TPL * k) * CS];
-    B::F::template natural_to_split<true>(v, o, col, CS, tw, q);
+    B::F::template natural_to_split_flat<true>(v, o, col, CS, tw, q);
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) col[B::G::split_pos(q, j, s) * CS] = o[j][s];
+    for (int i = 0; i < B::R; ++i) col[B::pos(q, i) * CS] = o[i];
     __syncthreads();
-    for (int i = t; i < L * YCH; i += NT) {
-        const int n = i / YCH, k = i % YCH;
-        *reinterpret_cast<float4*>(P + (uint64_t)n * L + 2 * k) = *reinterpret_cast<const float4*>(buf + n * CS + 2 * k);
-    }
+    store_col_tile<L, LN, CS>(P, buf, L, t, NT);
 }
 
 // the rest of an iteration and, unless `last`, the next one's forward rows
 template <int L>
-__global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_rows(const DmlDev p, int last) {
+__global__ void __launch_bounds__(DmLP<L>::NT, 2) k_dml_rows(const DmlDev p, int last) {
     using B = DmLP<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* Y1t = reinterpret_cast<Cx<float>*>(smem_raw);
@@ -210,19 +182,21 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_rows(const DmlDev p, i
     Cx<float>* Xt = Y2t + B::tile;
     Cx<float>* tw = Xt + B::tile;
     uint32_t* Mt = reinterpret_cast<uint32_t*>(tw + B::F::TW_ENTRIES);
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
-    const uint64_t g0 = (uint64_t)blockIdx.x * B::LINES, b = g0 / L;
+    const int t = threadIdx.x;
+    int line, q;
+    B::row_lane(t, line, q);
+    const uint64_t g0 = (uint64_t)blockIdx.x * B::RL, b = g0 / L;
     const int r0 = (int)(g0 % L);
     Cx<float>* Y1 = p.Y + (2 * b * (uint64_t)L + r0) * L;
     Cx<float>* Y2 = Y1 + (uint64_t)L * L;
-    stage(Y1t, Y1, (uint32_t)(B::tile * 8), true, t, B::THREADS);
+    stage(Y1t, Y1, (uint32_t)(B::tile * 8), true, t, B::NT);
     cp_async_commit();
-    stage(Xt, p.x + g0 * L, (uint32_t)(B::tile * 8), p.vec_x, t, B::THREADS);
-    stage(Mt, p.mask + b * p.mask_stride + (uint64_t)r0 * B::MW, (uint32_t)(B::tile / 8), true, t, B::THREADS);
+    stage(Xt, p.x + g0 * L, (uint32_t)(B::tile * 8), p.vec_x, t, B::NT);
+    stage(Mt, p.mask + b * p.mask_stride + (uint64_t)r0 * B::MW, (uint32_t)(B::tile / 8), true, t, B::NT);
     cp_async_commit();
-    stage(Y2t, Y2, (uint32_t)(B::tile * 8), true, t, B::THREADS);
+    stage(Y2t, Y2, (uint32_t)(B::tile * 8), true, t, B::NT);
     cp_async_commit();
-    B::F::fill_twiddles(tw, p.tw, t, B::THREADS);
+    B::F::fill_twiddles(tw, p.tw, t, B::NT);
     const int r = r0 + line;
     const uint64_t row = g0 + line;
     Cx<float>* y1 = Y1t + line * L;
@@ -230,62 +204,56 @@ __global__ void __launch_bounds__(DmLP<L>::THREADS) k_dml_rows(const DmlDev p, i
     Cx<float>* xs = Xt + line * L;
     const uint32_t* ms = Mt + line * B::MW;
     auto bit = [&](int f) { return (ms[f >> 5] >> (f & 31)) & 1u; };
-    Cx<float> v[B::R], o[B::J][B::TPL];
+    Cx<float> v[B::R], o[B::R];
 
     // t1 <- S(a1*x + b1*P_M(t1)); x1 = a3*t1 + b3*x (kept in the x tile)
     cp_async_wait<2>();
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < B::R; ++k) v[k] = y1[q + B::TPL * k];
-    B::F::template natural_to_split<true>(v, o, y1, 1, tw, q);
+    B::F::template natural_to_split_flat<true>(v, o, y1, 1, tw, q);
     cp_async_wait<1>();
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int f = B::G::split_pos(q, j, s);
-            const Cx<float> pm = flip(cscale(o[j][s], p.scale), r + f);
-            const Cx<float> xv = xs[f];
-            const Cx<float> t1n = keep_re(merge_apply(xv, pm, p.a1, p.b1), bit(f));
-            xs[f] = merge_apply(t1n, xv, p.a3, p.b3);
-            y1[f] = t1n;
-            if (last) p.t1[row * L + f] = t1n;
-        }
+    for (int i = 0; i < B::R; ++i) {
+        const int f = B::pos(q, i);
+        const Cx<float> pm = flip(cscale(o[i], p.scale), r + f);
+        const Cx<float> xv = xs[f];
+        const Cx<float> t1n = keep_re(merge_apply(xv, pm, p.a1, p.b1), bit(f));
+        xs[f] = merge_apply(t1n, xv, p.a3, p.b3);
+        y1[f] = t1n;
+        if (last) p.t1[row * L + f] = t1n;
+    }
     // t2 <- P_M(t2'); x <- a4*t2 + b4*x1; the next t2' = a2*x + b2*S(t2)
     cp_async_wait<0>();
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < B::R; ++k) v[k] = y2[q + B::TPL * k];
-    B::F::template natural_to_split<true>(v, o, y2, 1, tw, q);
+    B::F::template natural_to_split_flat<true>(v, o, y2, 1, tw, q);
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int f = B::G::split_pos(q, j, s);
-            const Cx<float> t2n = flip(cscale(o[j][s], p.scale), r + f);
-            const Cx<float> xn = merge_apply(t2n, xs[f], p.a4, p.b4);
-            p.x[row * L + f] = xn;
-            if (last)
-                p.t2[row * L + f] = t2n;
-            else
-                y2[f] = merge_apply(xn, keep_re(t2n, bit(f)), p.a2, p.b2);
-        }
+    for (int i = 0; i < B::R; ++i) {
+        const int f = B::pos(q, i);
+        const Cx<float> t2n = flip(cscale(o[i], p.scale), r + f);
+        const Cx<float> xn = merge_apply(t2n, xs[f], p.a4, p.b4);
+        p.x[row * L + f] = xn;
+        if (last)
+            p.t2[row * L + f] = t2n;
+        else
+            y2[f] = merge_apply(xn, keep_re(t2n, bit(f)), p.a2, p.b2);
+    }
     if (last) return;
     // the next iteration's forward row transforms (rows are read back in
-    // natural order from the tiles the update above wrote in split order)
+    // natural order from the tiles the update above wrote in flat order)
     __syncwarp();
 #pragma unroll 1
     for (int pl = 0; pl < 2; ++pl) {
         Cx<float>* yt = pl ? y2 : y1;
 #pragma unroll
         for (int k = 0; k < B::R; ++k) v[k] = flip(yt[q + B::TPL * k], r + q + B::TPL * k);
-        B::F::template natural_to_split<false>(v, o, yt, 1, tw, q);
+        B::F::template natural_to_split_flat<false>(v, o, yt, 1, tw, q);
         Cx<float>* __restrict__ yg = pl ? Y2 + (uint64_t)line * L : Y1 + (uint64_t)line * L;
 #pragma unroll
-        for (int j = 0; j < B::J; ++j)
-#pragma unroll
-            for (int s = 0; s < B::TPL; ++s) yg[B::G::split_pos(q, j, s)] = o[j][s];
+        for (int i = 0; i < B::R; ++i) yg[B::pos(q, i)] = o[i];
     }
 }
 
@@ -329,12 +297,12 @@ cudaError_t dml_launch(const DmArgs& a, const void* tw, void* Y, uint32_t* mask,
     d.vec_a = (reinterpret_cast<uintptr_t>(a.A) & 15u) == 0 && a.a_stride % 4 == 0;
     const uint64_t planes = a.s_stride ? a.batch : 1;
     k_dml_pack<<<ew_grid(planes * plane, 256), 256, 0, st>>>((const float*)a.S, a.s_stride, plane, planes, mask);
-    const unsigned row_ctas = (unsigned)(a.batch * L / B::LINES);
-    const unsigned col_ctas = (unsigned)(2 * a.batch * (L / B::LINES));
-    k_dml_first<L><<<row_ctas, B::THREADS, B::row_smem(), st>>>(d);
+    const unsigned row_ctas = (unsigned)(a.batch * L / B::RL);
+    const unsigned col_ctas = (unsigned)(2 * a.batch * (L / B::CL));
+    k_dml_first<L><<<row_ctas, B::NT, B::row_smem(), st>>>(d);
     for (int it = 0; it < a.iters; ++it) {
-        k_dml_cols<L><<<col_ctas, B::THREADS, B::col_smem(), st>>>(d);
-        k_dml_rows<L><<<row_ctas, B::THREADS, B::row_smem(), st>>>(d, it + 1 == a.iters ? 1 : 0);
+        k_dml_cols<L><<<col_ctas, B::NT, B::col_smem(), st>>>(d);
+        k_dml_rows<L><<<row_ctas, B::NT, B::row_smem(), st>>>(d, it + 1 == a.iters ? 1 : 0);
     }
     count_launches(2 + 2 * (uint64_t)a.iters);
     return cudaGetLastError();

@@ -142,21 +142,19 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         v[k] = buf[line * LSX + n];
         if (shift) v[k] = csign(v[k], n);
     }
-    Cx<T> o[J][TPL];
+    Cx<T> o[R];
     if (inverse)
-        F::template natural_to_split<true>(v, o, buf + line * LSX, 1, tw, q);
+        F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
     else
-        F::template natural_to_split<false>(v, o, buf + line * LSX, 1, tw, q);
+        F::template natural_to_split_flat<false>(v, o, buf + line * LSX, 1, tw, q);
 #pragma unroll
-    for (int j = 0; j < J; ++j)
-#pragma unroll
-        for (int s = 0; s < TPL; ++s) {
-            const int f = q + TPL * j + R * s;
-            Cx<T> w = o[j][s];
-            if (do_scale) w = cscale(w, scale);
-            if (shift) w = csign(w, f + out_neg);
-            buf[line * LSX + f] = w;
-        }
+    for (int i = 0; i < R; ++i) {
+        const int f = F::pos(q, i);
+        Cx<T> w = o[i];
+        if (do_scale) w = cscale(w, scale);
+        if (shift) w = csign(w, f + out_neg);
+        buf[line * LSX + f] = w;
+    }
     __syncthreads();
     for (int e = t; e < LINES * L; e += AXIS_THREADS) {
         int l, n;
@@ -264,10 +262,10 @@ cudaError_t axis_pass(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi,
         case 32: return axis_fft_t<T, 32, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 64: return axis_fft_t<T, 64, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 128: return axis_fft_t<T, 128, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        // 256 and 512: 16 threads per line, the split of the fused line passes
-        // (line_pass.cuh LineGeom), so those round exactly like these calls
+        // 256 and 512: 16 and 32 threads per line, the split of the fused line
+        // passes (line_pass.cuh LineGeom), so those round exactly like these calls
         case 256: return axis_fft_t<T, 256, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 512: return axis_fft_t<T, 512, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 512: return axis_fft_t<T, 512, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         case 1024: return axis_fft_t<T, 1024, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
         default: return cudaErrorInvalidValue;
     }

@@ -17,13 +17,16 @@
 // in L2 measured slower on B200 than whole-batch passes, whose larger grids
 // keep every SM busy), each chunk through all iterations.
 //
-// Lines: 16 threads per line (TPL), R = L / 16 values per thread, 16 lines
-// per 256-thread CTA; the line FFT is fft_line.cuh's.  The row passes read
-// and write global memory directly in the split/natural register layouts (16
-// consecutive elements per thread group and step: full 128-byte segments);
-// the column pass stages a tile of 16 columns of Y and A in shared memory.
-// Per iteration the passes move 56 bytes per pixel (rows: Y, x read and
-// written, S read; columns: Y read and written, A read).
+// Lines follow line_pass.cuh's LineGeom (16 values per thread; 16 threads per
+// line at 256, 32 at 512).  Transforms take their line in natural order
+// (LineFFT::natural_to_split_flat) and leave it in the flat layout.  Where a
+// second transform follows, at 256 it runs straight from the split layout in
+// registers (split_to_natural); at 512 (no such inverse for the half-split
+// form) the values go back through the line's shared slots.  Row passes stage Y and x tiles with cp.async and write global
+// memory directly (a thread group's outputs for one i are consecutive
+// elements); the column pass stages a tile of columns of Y and A.  Per
+// iteration the passes move 52 bytes and a bit per pixel (rows: Y, x read and
+// written, the support mask; columns: Y read and written, A read).
 #include "cpra_internal.h"
 #include "line_pass.cuh"
 #include "ops_ew.cuh"
@@ -32,140 +35,111 @@ namespace cpra_b200 {
 namespace {
 
 template <int L>
-struct Big {
-    static constexpr int TPL = 16;
-    static constexpr int R = L / TPL;
-    static constexpr int J = R / TPL;
-    // lines per CTA: 16 (256 threads) at 256, 8 (128 threads) at 512, so that
-    // a row tile's Y and x stage in about 70 KB and three CTAs share an SM
-    static constexpr int LINES = (L >= 512) ? 8 : 16;
-    static constexpr int THREADS = LINES * TPL;
-    // column tile pitches (16-byte rows for the asynchronous copies): with two
-    // columns interleaved per warp (k_big_cols), CS = LINES + 2 complex puts
-    // each half-warp's 8-byte accesses (8 ranks x 2 columns) on 16 distinct
-    // bank pairs; the A tile's AS = LINES + 4 floats costs at most two
-    // wavefronts per read
-    static constexpr int CS = LINES + 2;
-    static constexpr int AS = LINES + 4;
-    using F = LineFFT<float, L, TPL>;
-    static_assert(L % LINES == 0, "a CTA's lines must belong to one pattern");
-    static constexpr size_t tile = (size_t)LINES * L;
+struct Big : LineGeom<L> {
+    using G = LineGeom<L>;
+    using F = typename G::F;
+    static constexpr int TPL = G::TPL, R = G::R, NT = G::THREADS;
+    static constexpr int RL = G::ROW_LINES, CL = G::COL_LINES, CS = G::CS, AS = G::AS;
+    static constexpr size_t tile = G::row_tile;
     static constexpr int MW = L / 32;  // support mask words per row
+    // CTAs per SM the register budget is sized for (80 registers; shared
+    // memory allows 3 as well)
+    static constexpr int MINB = 3;
     // rows: Y tile (also the exchange scratch), x tile, twiddles, mask tile, max
     static constexpr size_t row_smem() { return sizeof(Cx<float>) * (2 * tile + F::TW_ENTRIES) + tile / 8 + 16; }
     static constexpr size_t col_smem() {
         return sizeof(Cx<float>) * ((size_t)L * CS + F::TW_ENTRIES) + sizeof(float) * ((size_t)L * AS + L);
     }
-    __device__ __forceinline__ static int split_pos(int q, int j, int s) { return q + TPL * j + R * s; }
 };
 
-// forward row transform of the sequence in split positions o into Y's row
-// (natural frequency order): split_to_natural<false> is the forward DFT of
-// its input read as a sequence indexed by the split positions
+// Y's row from the line's natural-order values v (already D-flipped): the
+// forward transform (scratch: the line's shared slots), stored in the flat layout
 template <int L>
-__device__ __forceinline__ void big_row_forward_split(Cx<float> (&o)[Big<L>::J][Big<L>::TPL], Cx<float>* scratch,
-                                                      const Cx<float>* tw, int q, Cx<float>* __restrict__ yr) {
+__device__ __forceinline__ void big_row_forward(Cx<float> (&v)[Big<L>::R], Cx<float>* scratch, const Cx<float>* tw,
+                                                int q, Cx<float>* __restrict__ yr) {
     using B = Big<L>;
-    Cx<float> v[B::R];
-    B::F::template split_to_natural<false>(o, v, scratch, 1, tw, q);
+    Cx<float> o[B::R];
+    B::F::template natural_to_split_flat<false>(v, o, scratch, 1, tw, q);
 #pragma unroll
-    for (int i = 0; i < B::R; ++i) yr[q + B::TPL * brev<B::R>(i)] = v[i];
+    for (int i = 0; i < B::R; ++i) yr[B::pos(q, i)] = o[i];
 }
 
 // Y <- row DFT of D (.) x; with V: also the support mask <- { V > threshold *
 // vmax } (the support of a shrinkwrap update).  vec_x: x rows 16-byte aligned
 template <int L>
-__global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_rows_fwd(const Cx<float>* __restrict__ x,
-                                                                     Cx<float>* __restrict__ Y,
-                                                                     const Cx<float>* __restrict__ twg,
-                                                                     const float* __restrict__ V,
-                                                                     const unsigned int* __restrict__ vmax,
-                                                                     uint16_t* __restrict__ mask16, float threshold,
-                                                                     int vec_x) {
+__global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_rows_fwd(const Cx<float>* __restrict__ x,
+                                                                Cx<float>* __restrict__ Y,
+                                                                const Cx<float>* __restrict__ twg,
+                                                                const float* __restrict__ V,
+                                                                const unsigned int* __restrict__ vmax,
+                                                                uint32_t* __restrict__ mask, float threshold,
+                                                                int vec_x) {
     using B = Big<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* Yt = reinterpret_cast<Cx<float>*>(smem_raw);
     Cx<float>* Xt = Yt + B::tile;
     Cx<float>* tw = Xt + B::tile;
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
-    const uint64_t g0 = (uint64_t)blockIdx.x * B::LINES;  // first row of the chunk's [batch*L][L] plane stack
-    stage(Xt, x + g0 * L, (uint32_t)(B::tile * 8), vec_x, t, B::THREADS);
+    int line, q;
+    B::row_lane(threadIdx.x, line, q);
+    const int t = threadIdx.x;
+    const uint64_t g0 = (uint64_t)blockIdx.x * B::RL;  // first row of the chunk's [batch*L][L] plane stack
+    stage(Xt, x + g0 * L, (uint32_t)(B::tile * 8), vec_x, t, B::NT);
     cp_async_commit();
-    B::F::fill_twiddles(tw, twg, t, B::THREADS);
+    B::F::fill_twiddles(tw, twg, t, B::NT);
     const uint64_t g = g0 + line, b = g / L;
     const int r = (int)(g % L);
     if (V) {
-        // a warp holds two rows (16 lanes each); per (j, s) the lanes of a row
-        // hold 16 consecutive pixels from f0 = 16 j + R s, one half mask word
+        // lanes of a row hold TPL consecutive pixels TPL k + q: a 32-thread
+        // line fills one mask word per k, a 16-thread line half of one (the
+        // warp's other half is the next row)
         const float thr = threshold * unordered(vmax[b]);
         const float* __restrict__ Vr = V + g * L;
 #pragma unroll
-        for (int j = 0; j < B::J; ++j)
-#pragma unroll
-            for (int s = 0; s < B::TPL; ++s) {
-                const int f0 = B::TPL * j + B::R * s;
-                const unsigned bal = __ballot_sync(0xffffffffu, Vr[f0 + q] > thr);
-                if (q == 0) mask16[(g * L + f0) >> 4] = (uint16_t)(bal >> (t & 16));
+        for (int k = 0; k < B::R; ++k) {
+            const int n0 = B::TPL * k;
+            const unsigned bal = __ballot_sync(0xffffffffu, Vr[n0 + q] > thr);
+            if constexpr (B::TPL == 32) {
+                if (q == 0) mask[(g * L + n0) >> 5] = bal;
+            } else {
+                if (q == 0) reinterpret_cast<uint16_t*>(mask)[(g * L + n0) >> 4] = (uint16_t)(bal >> (t & 16));
             }
+        }
     }
     cp_async_wait<0>();
     __syncthreads();
-    Cx<float> o[B::J][B::TPL];
+    Cx<float> v[B::R];
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int n = B::split_pos(q, j, s);
-            o[j][s] = flip(Xt[line * L + n], r + n);
-        }
-    big_row_forward_split<L>(o, Yt + line * L, tw, q, Y + g * L);
+    for (int k = 0; k < B::R; ++k) {
+        const int n = q + B::TPL * k;
+        v[k] = flip(Xt[line * L + n], r + n);
+    }
+    big_row_forward<L>(v, Yt + line * L, tw, q, Y + g * L);
 }
 
-// a tile of LINES columns of one pattern: DFT, op, IDFT, in place.
+// a tile of column lines of one pattern: DFT, op, IDFT, in place.
 // op 0: modulus projection with A (pattern b's plane at A + b * a_stride;
 // vec_a: its rows 16-byte aligned); op 1: multiply by gt[f] * gt[c] (and zero
 // vmax[0..nzero) for the blur pass)
 template <int L>
-__global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_cols(Cx<float>* __restrict__ Y, const float* __restrict__ A,
-                                                              uint64_t a_stride, const float* __restrict__ gtab,
-                                                              const Cx<float>* __restrict__ twg, int op, int data_mode,
-                                                              unsigned int* __restrict__ vzero, int nzero, int vec_a) {
+__global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_cols(Cx<float>* __restrict__ Y, const float* __restrict__ A,
+                                                            uint64_t a_stride, const float* __restrict__ gtab,
+                                                            const Cx<float>* __restrict__ twg, int op, int data_mode,
+                                                            unsigned int* __restrict__ vzero, int nzero, int vec_a) {
     using B = Big<L>;
-    constexpr int CS = B::CS, AS = B::AS, LN = B::LINES, NT = B::THREADS;
+    constexpr int CS = B::CS, AS = B::AS, LN = B::CL, NT = B::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
     Cx<float>* tw = buf + L * CS;
     float* As = reinterpret_cast<float*>(tw + B::F::TW_ENTRIES);
     float* gt = As + L * AS;
-    // two columns per warp, interleaved: each half-warp (which a 64-bit shared
-    // access serves as one unit) reads 8 ranks of both columns, 16 distinct
-    // 8-byte bank pairs at the tile pitch CS
-    const int t = threadIdx.x, line = 2 * (t >> 5) + (t & 1), q = (t & 31) >> 1;
+    const int t = threadIdx.x;
+    int line, q;
+    B::col_lane(t, line, q);
     constexpr int TILES = L / LN;
     const uint64_t b = blockIdx.x / TILES;
     const int c0 = (int)(blockIdx.x % TILES) * LN;
     Cx<float>* __restrict__ P = Y + b * (uint64_t)L * L + c0;
-    const float* __restrict__ Ab = A + b * a_stride + c0;
-    // tile rows: LN complex (LN / 2 16-byte chunks) of Y, LN floats of A
-    constexpr int YCH = LN / 2;
-    for (int i = t; i < L * YCH; i += NT) {
-        const int n = i / YCH, k = i % YCH;
-        cp_async16(buf + n * CS + 2 * k, P + (uint64_t)n * L + 2 * k);
-    }
-    if (op == 0) {
-        if (vec_a) {
-            constexpr int ACH = LN / 4;
-            for (int i = t; i < L * ACH; i += NT) {
-                const int n = i / ACH, k = i % ACH;
-                cp_async16(As + n * AS + 4 * k, Ab + (uint64_t)n * L + 4 * k);
-            }
-        } else {
-            for (int i = t; i < L * LN; i += NT) {
-                const int n = i / LN, k = i % LN;
-                cp_async4(As + n * AS + k, Ab + (uint64_t)n * L + k);
-            }
-        }
-    }
+    stage_col_tile<L, LN, CS, AS>(buf, P, As, op == 0 ? A + b * a_stride + c0 : nullptr, L, vec_a != 0, t, NT);
     cp_async_commit();
     B::F::fill_twiddles(tw, twg, t, NT);
     if (op == 1)
@@ -175,25 +149,33 @@ __global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_cols(Cx<float>* __re
     cp_async_wait<0>();
     __syncthreads();
     const int c = c0 + line;
-    Cx<float> v[B::R], o[B::J][B::TPL];
+    Cx<float>* col = buf + line;  // slot u of this column at col[u * CS]
+    Cx<float> v[B::R], o[B::R];
 #pragma unroll
-    for (int k = 0; k < B::R; ++k) v[k] = buf[(q + B::TPL * k) * CS + line];
-    B::F::template natural_to_split<false>(v, o, buf + line, CS, tw, q);
+    for (int k = 0; k < B::R; ++k) v[k] = col[(q + B::TPL * k) * CS];
+    B::F::template natural_to_split_flat<false>(v, o, col, CS, tw, q);
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int f = B::split_pos(q, j, s);
-            o[j][s] = (op == 0) ? data_apply(o[j][s], As[f * AS + line], data_mode) : cscale(o[j][s], gt[f] * gt[c]);
-        }
-    B::F::template split_to_natural<true>(o, v, buf + line, CS, tw, q);
-#pragma unroll
-    for (int i = 0; i < B::R; ++i) buf[(q + B::TPL * brev<B::R>(i)) * CS + line] = v[i];
-    __syncthreads();
-    for (int i = t; i < L * YCH; i += NT) {
-        const int n = i / YCH, k = i % YCH;
-        *reinterpret_cast<float4*>(P + (uint64_t)n * L + 2 * k) = *reinterpret_cast<const float4*>(buf + n * CS + 2 * k);
+    for (int i = 0; i < B::R; ++i) {
+        const int f = B::pos(q, i);
+        o[i] = (op == 0) ? data_apply(o[i], As[f * AS + line], data_mode) : cscale(o[i], gt[f] * gt[c]);
     }
+    if constexpr (!B::F::HALF) {
+        // split layout in registers: the inverse runs straight from it
+        B::F::template split_to_natural<true>(reinterpret_cast<Cx<float>(&)[B::F::J][B::TPL]>(o), v, col, CS, tw, q);
+#pragma unroll
+        for (int i = 0; i < B::R; ++i) col[(q + B::TPL * brev<B::R>(i)) * CS] = v[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < B::R; ++i) col[B::pos(q, i) * CS] = o[i];
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < B::R; ++k) v[k] = col[(q + B::TPL * k) * CS];
+        B::F::template natural_to_split_flat<true>(v, o, col, CS, tw, q);
+#pragma unroll
+        for (int i = 0; i < B::R; ++i) col[B::pos(q, i) * CS] = o[i];
+    }
+    __syncthreads();
+    store_col_tile<L, LN, CS>(P, buf, L, t, NT);
 }
 
 enum RowsMode : int { ROWS_HIO = 0, ROWS_HIO_NEXT = 1, ROWS_HIO_MAG = 2, ROWS_BLUR = 3, ROWS_ESTIMATE = 4 };
@@ -209,12 +191,11 @@ enum RowsMode : int { ROWS_HIO = 0, ROWS_HIO_NEXT = 1, ROWS_HIO_MAG = 2, ROWS_BL
 // Y's rows arrive by asynchronous copy first, x's and the support mask's
 // while the inverse transform runs.  vec_x: x rows 16-byte aligned.
 template <int L>
-__global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_rows(Cx<float>* __restrict__ Y, Cx<float>* __restrict__ x,
-                                                                 const uint32_t* __restrict__ mask,
-                                                                 float* __restrict__ vout,
-                                                                 unsigned int* __restrict__ vmax,
-                                                                 const Cx<float>* __restrict__ twg, float scale,
-                                                                 float beta, int positivity, int mode, int vec_x) {
+__global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_rows(Cx<float>* __restrict__ Y, Cx<float>* __restrict__ x,
+                                                            const uint32_t* __restrict__ mask,
+                                                            float* __restrict__ vout, unsigned int* __restrict__ vmax,
+                                                            const Cx<float>* __restrict__ twg, float scale, float beta,
+                                                            int positivity, int mode, int vec_x) {
     using B = Big<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* Yt = reinterpret_cast<Cx<float>*>(smem_raw);
@@ -222,25 +203,28 @@ __global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_rows(Cx<float>* __re
     Cx<float>* tw = Xt + B::tile;
     uint32_t* Mt = reinterpret_cast<uint32_t*>(tw + B::F::TW_ENTRIES);
     unsigned int* smax = Mt + B::tile / 32;
-    const int t = threadIdx.x, line = t / B::TPL, q = t % B::TPL;
-    const uint64_t g0 = (uint64_t)blockIdx.x * B::LINES;
+    const int t = threadIdx.x;
+    int line, q;
+    B::row_lane(t, line, q);
+    const uint64_t g0 = (uint64_t)blockIdx.x * B::RL;
     const uint64_t b = g0 / L;
     const bool hio = mode <= ROWS_HIO_MAG;
-    stage(Yt, Y + g0 * L, (uint32_t)(B::tile * 8), true, t, B::THREADS);
+    stage(Yt, Y + g0 * L, (uint32_t)(B::tile * 8), true, t, B::NT);
     cp_async_commit();
-    if (hio) stage(Xt, x + g0 * L, (uint32_t)(B::tile * 8), vec_x, t, B::THREADS);
-    if (hio || mode == ROWS_ESTIMATE) stage(Mt, mask + g0 * B::MW, (uint32_t)(B::tile / 8), true, t, B::THREADS);
+    if (hio) stage(Xt, x + g0 * L, (uint32_t)(B::tile * 8), vec_x, t, B::NT);
+    if (hio || mode == ROWS_ESTIMATE) stage(Mt, mask + g0 * B::MW, (uint32_t)(B::tile / 8), true, t, B::NT);
     cp_async_commit();
-    B::F::fill_twiddles(tw, twg, t, B::THREADS);
+    B::F::fill_twiddles(tw, twg, t, B::NT);
     if (t == 0) *smax = 0u;
     const uint64_t g = g0 + line;
     const int r = (int)(g % L);
+    Cx<float>* yl = Yt + line * L;
     cp_async_wait<1>();  // the Y tile
     __syncthreads();
-    Cx<float> v[B::R], o[B::J][B::TPL];
+    Cx<float> v[B::R], o[B::R];
 #pragma unroll
-    for (int k = 0; k < B::R; ++k) v[k] = Yt[line * L + q + B::TPL * k];
-    B::F::template natural_to_split<true>(v, o, Yt + line * L, 1, tw, q);
+    for (int k = 0; k < B::R; ++k) v[k] = yl[q + B::TPL * k];
+    B::F::template natural_to_split_flat<true>(v, o, yl, 1, tw, q);
     cp_async_wait<0>();  // x and mask tiles
     __syncthreads();
     Cx<float>* __restrict__ xr = x + g * L;
@@ -249,25 +233,44 @@ __global__ void __launch_bounds__(Big<L>::THREADS, 3) k_big_rows(Cx<float>* __re
     auto inside = [&](int f) { return (ms[f >> 5] >> (f & 31)) & 1u; };
     float lmax = -INFINITY;
 #pragma unroll
-    for (int j = 0; j < B::J; ++j)
-#pragma unroll
-        for (int s = 0; s < B::TPL; ++s) {
-            const int f = B::split_pos(q, j, s);
-            const Cx<float> y = flip(cscale(o[j][s], scale), r + f);
-            if (hio) {
-                const bool keep = inside(f) && (!positivity || y.x >= 0.0f);
-                const Cx<float> xn = keep ? y : merge_apply(y, xs[f], -beta, 1.0f);
-                xr[f] = xn;
-                o[j][s] = flip(mode == ROWS_HIO_MAG ? Cx<float>{sqrtf(fmaf(xn.x, xn.x, xn.y * xn.y)), 0.0f} : xn,
-                               r + f);
-            } else if (mode == ROWS_BLUR) {
-                vout[g * L + f] = y.x;
-                lmax = fmaxf(lmax, y.x);
-            } else {
-                xr[f] = inside(f) ? y : Cx<float>{0.0f, 0.0f};
-            }
+    for (int i = 0; i < B::R; ++i) {
+        const int f = B::pos(q, i);
+        const Cx<float> y = flip(cscale(o[i], scale), r + f);
+        if (hio) {
+            const bool keep = inside(f) && (!positivity || y.x >= 0.0f);
+            const Cx<float> xn = keep ? y : merge_apply(y, xs[f], -beta, 1.0f);
+            xr[f] = xn;
+            // the next forward transform's input (kept in registers in the
+            // split layout, else in the line's now free slots)
+            const Cx<float> z =
+                flip(mode == ROWS_HIO_MAG ? Cx<float>{sqrtf(fmaf(xn.x, xn.x, xn.y * xn.y)), 0.0f} : xn, r + f);
+            if constexpr (!B::F::HALF)
+                o[i] = z;
+            else
+                yl[f] = z;
+        } else if (mode == ROWS_BLUR) {
+            vout[g * L + f] = y.x;
+            lmax = fmaxf(lmax, y.x);
+        } else {
+            xr[f] = inside(f) ? y : Cx<float>{0.0f, 0.0f};
         }
-    if (mode == ROWS_HIO_NEXT || mode == ROWS_HIO_MAG) big_row_forward_split<L>(o, Yt + line * L, tw, q, Y + g * L);
+    }
+    if (mode == ROWS_HIO_NEXT || mode == ROWS_HIO_MAG) {
+        if constexpr (!B::F::HALF) {
+            // split_to_natural<false> is the forward DFT of its input read as
+            // a sequence indexed by the split positions: Y's row in natural order
+            B::F::template split_to_natural<false>(reinterpret_cast<Cx<float>(&)[B::F::J][B::TPL]>(o), v, yl, 1, tw,
+                                                   q);
+            Cx<float>* __restrict__ yr = Y + g * L;
+#pragma unroll
+            for (int i = 0; i < B::R; ++i) yr[q + B::TPL * brev<B::R>(i)] = v[i];
+        } else {
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < B::R; ++k) v[k] = yl[q + B::TPL * k];
+            big_row_forward<L>(v, yl, tw, q, Y + g * L);
+        }
+    }
     if (mode == ROWS_BLUR) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
@@ -329,19 +332,18 @@ template <int L>
 cudaError_t big_chunk(const HioArgs& a, uint64_t b0, uint64_t nb, const Cx<float>* tw, Cx<float>* Y, float* V,
                       unsigned int* vmax, uint32_t* mask, cudaStream_t st) {
     using B = Big<L>;
-    constexpr int NT = B::THREADS;
+    constexpr int NT = B::NT;
     const uint64_t plane = (uint64_t)L * L;
     Cx<float>* x = (Cx<float>*)a.x + b0 * plane;
     const float* A = (const float*)a.A + b0 * a.a_stride;
     float* S = (float*)a.S + b0 * a.s_stride;
     const int vx = aligned16(a.x), va = aligned16(a.A) && a.a_stride % 4 == 0;
-    const unsigned row_ctas = (unsigned)(nb * L / B::LINES);
-    const unsigned col_ctas = (unsigned)(nb * (L / B::LINES));
+    const unsigned row_ctas = (unsigned)(nb * L / B::RL);
+    const unsigned col_ctas = (unsigned)(nb * (L / B::CL));
     const unsigned ew = ew_grid(nb * plane, 256);
     const size_t rs = B::row_smem(), cs = B::col_smem();
     const float scale = 1.0f / (float)plane, beta = (float)a.beta, thr = (float)a.threshold;
     const bool est = a.estimate != nullptr;
-    uint16_t* mask16 = reinterpret_cast<uint16_t*>(mask);
     auto cols = [&](int op, const float* gtab, unsigned int* vz) {
         k_big_cols<L><<<col_ctas, NT, cs, st>>>(Y, A, a.a_stride, gtab, tw, op, a.data_mode, vz, (int)nb, va);
     };
@@ -349,7 +351,7 @@ cudaError_t big_chunk(const HioArgs& a, uint64_t b0, uint64_t nb, const Cx<float
         k_big_rows<L><<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, mode, vdst);
     };
     k_big_pack<<<ew, 256, 0, st>>>(S, a.s_stride, plane, nb, mask);
-    k_big_rows_fwd<L><<<row_ctas, NT, rs, st>>>(x, Y, tw, nullptr, nullptr, mask16, thr, vx);
+    k_big_rows_fwd<L><<<row_ctas, NT, rs, st>>>(x, Y, tw, nullptr, nullptr, mask, thr, vx);
     uint64_t launches = 2;
     int update = 0;
     for (int it = 0; it < a.iters; ++it) {
@@ -369,7 +371,7 @@ cudaError_t big_chunk(const HioArgs& a, uint64_t b0, uint64_t nb, const Cx<float
         if (last && !est)
             k_big_threshold<<<ew, 256, 0, st>>>(V, vmax, mask, plane, nb, thr);
         else
-            k_big_rows_fwd<L><<<row_ctas, NT, rs, st>>>(x, Y, tw, V, vmax, mask16, thr, vx);
+            k_big_rows_fwd<L><<<row_ctas, NT, rs, st>>>(x, Y, tw, V, vmax, mask, thr, vx);
         ++launches;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;

@@ -6,16 +6,52 @@
 
 namespace cpra_b200 {
 
-// Threads per line of the line transforms at 256 and 512 (R = L / 16 values
-// per thread).  The per-operator axis passes (kernels_fft.cu) use the same
-// split, so line passes built from the same LineFFT steps round identically.
+// Geometry of the line passes at 256 and 512.  A line is TPL threads of one
+// warp with R = 16 values each: 16 threads at 256, 32 at 512 (LineFFT's HALF
+// form), so a thread holds 16 complex values at both sizes.  The per-operator
+// axis passes (kernels_fft.cu) use the same split, so line passes built from
+// the same LineFFT steps round identically.  Outputs of a transform are in the
+// flat layout LineFFT::pos.
+//   rows:    ROW_LINES lines per 256-thread CTA, each line's L slots of a tile
+//            in shared memory (row-major, pitch L).
+//   columns: COL_LINES columns per 256-thread CTA in a [L][CS] tile.  At 256
+//            two columns share a warp, interleaved lane by lane (line =
+//            2 (t >> 5) + (t & 1)), and CS = 18 (16-byte rows): a half-warp's
+//            8-byte accesses touch 8 ranks of both columns on 16 distinct bank
+//            pairs.  At 512 a warp is one column and CS = 9 (odd, 8-byte rows
+//            and copies): a half-warp's 16 consecutive ranks or slots land on
+//            16 distinct bank pairs.  The A tile's pitch AS is 20 (16-byte
+//            rows) at 256 and 9 at 512 (4-byte copies; odd, so a warp's 32
+//            rows of one column hit 32 distinct banks).
 template <int L>
 struct LineGeom {
-    static constexpr int TPL = 16;
+    static constexpr int TPL = (L >= 512) ? 32 : 16;
     static constexpr int R = L / TPL;
-    static constexpr int J = R / TPL;
     using F = LineFFT<float, L, TPL>;
-    __device__ __forceinline__ static int split_pos(int q, int j, int s) { return q + TPL * j + R * s; }
+    static constexpr int THREADS = 256;
+    static constexpr int ROW_LINES = THREADS / TPL;
+    static constexpr int COL_LINES = THREADS / TPL;
+    static constexpr bool PAIRED = (TPL == 16);  // two columns per warp
+    static constexpr int CS = PAIRED ? COL_LINES + 2 : COL_LINES + 1;
+    static constexpr int AS = PAIRED ? COL_LINES + 4 : COL_LINES + 1;
+    static constexpr size_t row_tile = (size_t)ROW_LINES * L;  // elements
+    static_assert(R == 16, "16 values per thread");
+    static_assert(L % ROW_LINES == 0 && L % COL_LINES == 0, "a CTA's lines must belong to one pattern");
+    __device__ __forceinline__ static int pos(int q, int i) { return F::pos(q, i); }
+    // (line, rank) of thread t in a row pass and in a column pass
+    __device__ __forceinline__ static void row_lane(int t, int& line, int& q) {
+        line = t / TPL;
+        q = t % TPL;
+    }
+    __device__ __forceinline__ static void col_lane(int t, int& line, int& q) {
+        if constexpr (PAIRED) {
+            line = 2 * (t >> 5) + (t & 1);
+            q = (t & 31) >> 1;
+        } else {
+            line = t >> 5;
+            q = t & 31;
+        }
+    }
 };
 
 __device__ __forceinline__ Cx<float> flip(Cx<float> z, int n) { return (n & 1) ? Cx<float>{-z.x, -z.y} : z; }
@@ -38,6 +74,10 @@ __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -52,6 +92,58 @@ __device__ __forceinline__ void stage(void* dst, const void* src, uint32_t bytes
         for (uint32_t i = 16u * t; i < bytes; i += 16u * nt) cp_async16(d + i, s + i);
     else
         for (uint32_t i = 4u * t; i < bytes; i += 4u * nt) cp_async4(d + i, s + i);
+}
+
+// A column tile: rows n < L of LN consecutive complex at src + n * ld into
+// dst + n * CS (16-byte copies when CS is even, 8-byte copies otherwise), and
+// optionally LN floats per row of A at a + n * ld into as + n * AS (16-byte
+// copies when `avec` and AS % 4 == 0, else 4-byte copies).
+template <int L, int LN, int CS, int AS>
+__device__ __forceinline__ void stage_col_tile(Cx<float>* dst, const Cx<float>* src, float* as, const float* a,
+                                               uint64_t ld, bool avec, int t, int nt) {
+    if constexpr (CS % 2 == 0) {
+        constexpr int CH = LN / 2;
+        for (int i = t; i < L * CH; i += nt) {
+            const int n = i / CH, k = i % CH;
+            cp_async16(dst + n * CS + 2 * k, src + (uint64_t)n * ld + 2 * k);
+        }
+    } else {
+        for (int i = t; i < L * LN; i += nt) {
+            const int n = i / LN, k = i % LN;
+            cp_async8(dst + n * CS + k, src + (uint64_t)n * ld + k);
+        }
+    }
+    if (!a) return;
+    if (AS % 4 == 0 && avec) {
+        constexpr int CH = LN / 4;
+        for (int i = t; i < L * CH; i += nt) {
+            const int n = i / CH, k = i % CH;
+            cp_async16(as + n * AS + 4 * k, a + (uint64_t)n * ld + 4 * k);
+        }
+    } else {
+        for (int i = t; i < L * LN; i += nt) {
+            const int n = i / LN, k = i % LN;
+            cp_async4(as + n * AS + k, a + (uint64_t)n * ld + k);
+        }
+    }
+}
+
+// the tile back: rows of LN complex from src + n * CS to dst + n * ld
+template <int L, int LN, int CS>
+__device__ __forceinline__ void store_col_tile(Cx<float>* dst, const Cx<float>* src, uint64_t ld, int t, int nt) {
+    if constexpr (CS % 2 == 0) {
+        constexpr int CH = LN / 2;
+        for (int i = t; i < L * CH; i += nt) {
+            const int n = i / CH, k = i % CH;
+            *reinterpret_cast<float4*>(dst + (uint64_t)n * ld + 2 * k) =
+                *reinterpret_cast<const float4*>(src + n * CS + 2 * k);
+        }
+    } else {
+        for (int i = t; i < L * LN; i += nt) {
+            const int n = i / LN, k = i % LN;
+            dst[(uint64_t)n * ld + k] = src[n * CS + k];
+        }
+    }
 }
 
 }  // namespace cpra_b200
