@@ -209,11 +209,41 @@ __device__ __forceinline__ void adam_apply(T& p, T g, T& m, T& v, T lr, T b1, T 
     p -= (lr / c1) * m / (sqrt(v) / sqrt(c2) + eps);
 }
 
-// the volume as 2 * count reals (re, im interleaved), moments alike
+// the volume as 2 * count reals (re, im interleaved), moments alike; 16-byte
+// vectors (4 floats or 2 doubles) per thread and step, the tail one by one
 template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int N = 4;
+};
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int N = 2;
+};
+
+template <typename T, bool VEC>
 __global__ void k_adam_volume(T* __restrict__ V, const T* __restrict__ g, T* __restrict__ m, T* __restrict__ v,
                               uint64_t n, T lr, T b1, T b2, T eps, T c1, T c2) {
-    for (uint64_t i = tid_g(); i < n; i += str_g()) adam_apply(V[i], g[i], m[i], v[i], lr, b1, b2, eps, c1, c2);
+    using W = typename Vec16<T>::type;
+    constexpr int K = Vec16<T>::N;
+    const uint64_t nv = VEC ? n / K : 0;
+    for (uint64_t i = tid_g(); i < nv; i += str_g()) {
+        W pv = reinterpret_cast<W*>(V)[i], gv = reinterpret_cast<const W*>(g)[i];
+        W mv = reinterpret_cast<W*>(m)[i], vv = reinterpret_cast<W*>(v)[i];
+        T* pp = reinterpret_cast<T*>(&pv);
+        const T* gp = reinterpret_cast<const T*>(&gv);
+        T* mp = reinterpret_cast<T*>(&mv);
+        T* vp = reinterpret_cast<T*>(&vv);
+#pragma unroll
+        for (int k = 0; k < K; ++k) adam_apply(pp[k], gp[k], mp[k], vp[k], lr, b1, b2, eps, c1, c2);
+        reinterpret_cast<W*>(V)[i] = pv;
+        reinterpret_cast<W*>(m)[i] = mv;
+        reinterpret_cast<W*>(v)[i] = vv;
+    }
+    for (uint64_t i = nv * K + tid_g(); i < n; i += str_g()) adam_apply(V[i], g[i], m[i], v[i], lr, b1, b2, eps, c1, c2);
 }
 
 // angles from the per-slice sums (sums[2p + 1] = dL/d ang[p]); loss[step] =
@@ -238,8 +268,13 @@ cudaError_t refine_step_t(void* V, void* ang, const void* gV, void* mom, uint64_
     const T c1 = T(1) - pow(b1, (T)step), c2 = T(1) - pow(b2, (T)step);
     T* mv = static_cast<T*>(mom);
     const uint64_t n = 2 * vox;
-    k_adam_volume<T><<<ew_grid(n, ADJ_THREADS), ADJ_THREADS, 0, st>>>(static_cast<T*>(V), static_cast<const T*>(gV), mv,
-                                                                       mv + n, n, (T)lr_v, b1, b2, eps, c1, c2);
+    auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    if (a16(V) && a16(gV) && a16(mv) && a16(mv + n))
+        k_adam_volume<T, true><<<ew_grid(n / Vec16<T>::N + 1, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
+            static_cast<T*>(V), static_cast<const T*>(gV), mv, mv + n, n, (T)lr_v, b1, b2, eps, c1, c2);
+    else
+        k_adam_volume<T, false><<<ew_grid(n, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
+            static_cast<T*>(V), static_cast<const T*>(gV), mv, mv + n, n, (T)lr_v, b1, b2, eps, c1, c2);
     k_adam_angles<T><<<1, 128, 0, st>>>(static_cast<T*>(ang), sums, mv + 2 * n, mv + 2 * n + P, P, (T)lr_a, b1, b2,
                                         eps, c1, c2, loss);
     count_launches(2);

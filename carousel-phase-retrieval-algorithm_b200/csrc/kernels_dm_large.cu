@@ -36,8 +36,8 @@ struct DmLP : LineGeom<L> {
     static constexpr int RL = G::ROW_LINES, CL = G::COL_LINES, CS = G::CS, AS = G::AS;
     static constexpr int MW = L / 32;  // mask words per row
     static constexpr size_t tile = G::row_tile;
-    // rows: Y1, Y2 and x tiles, twiddles, mask tile
-    static constexpr size_t row_smem() { return sizeof(Cx<float>) * (3 * tile + F::TW_ENTRIES) + tile / 8; }
+    // rows: Y tile (Y1's rows, then each line's Y2 row), x tile, twiddles, mask tile
+    static constexpr size_t row_smem() { return sizeof(Cx<float>) * (2 * tile + F::TW_ENTRIES) + tile / 8; }
     static constexpr size_t col_smem() {
         return sizeof(Cx<float>) * ((size_t)L * CS + F::TW_ENTRIES) + sizeof(float) * (size_t)L * AS;
     }
@@ -172,14 +172,16 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_cols(const DmlDev p) {
     store_col_tile<L, LN, CS>(P, buf, L, t, NT);
 }
 
-// the rest of an iteration and, unless `last`, the next one's forward rows
+// the rest of an iteration and, unless `last`, the next one's forward rows.
+// t1's half (inverse, update, next forward into Y1) completes first; then each
+// line's threads copy that line's row of Y2 into the slots it has freed, so a
+// CTA stages two tiles (Y, x), not three.
 template <int L>
-__global__ void __launch_bounds__(DmLP<L>::NT, 2) k_dml_rows(const DmlDev p, int last) {
+__global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_rows(const DmlDev p, int last) {
     using B = DmLP<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Cx<float>* Y1t = reinterpret_cast<Cx<float>*>(smem_raw);
-    Cx<float>* Y2t = Y1t + B::tile;
-    Cx<float>* Xt = Y2t + B::tile;
+    Cx<float>* Yt = reinterpret_cast<Cx<float>*>(smem_raw);
+    Cx<float>* Xt = Yt + B::tile;
     Cx<float>* tw = Xt + B::tile;
     uint32_t* Mt = reinterpret_cast<uint32_t*>(tw + B::F::TW_ENTRIES);
     const int t = threadIdx.x;
@@ -189,30 +191,36 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 2) k_dml_rows(const DmlDev p, int
     const int r0 = (int)(g0 % L);
     Cx<float>* Y1 = p.Y + (2 * b * (uint64_t)L + r0) * L;
     Cx<float>* Y2 = Y1 + (uint64_t)L * L;
-    stage(Y1t, Y1, (uint32_t)(B::tile * 8), true, t, B::NT);
+    stage(Yt, Y1, (uint32_t)(B::tile * 8), true, t, B::NT);
     cp_async_commit();
     stage(Xt, p.x + g0 * L, (uint32_t)(B::tile * 8), p.vec_x, t, B::NT);
     stage(Mt, p.mask + b * p.mask_stride + (uint64_t)r0 * B::MW, (uint32_t)(B::tile / 8), true, t, B::NT);
     cp_async_commit();
-    stage(Y2t, Y2, (uint32_t)(B::tile * 8), true, t, B::NT);
-    cp_async_commit();
     B::F::fill_twiddles(tw, p.tw, t, B::NT);
     const int r = r0 + line;
     const uint64_t row = g0 + line;
-    Cx<float>* y1 = Y1t + line * L;
-    Cx<float>* y2 = Y2t + line * L;
+    Cx<float>* yl = Yt + line * L;
     Cx<float>* xs = Xt + line * L;
     const uint32_t* ms = Mt + line * B::MW;
     auto bit = [&](int f) { return (ms[f >> 5] >> (f & 31)) & 1u; };
     Cx<float> v[B::R], o[B::R];
+    // the line's natural-order slots (D-flipped) through the forward row
+    // transform into the global row yg
+    auto forward_row = [&](Cx<float>* __restrict__ yg) {
+#pragma unroll
+        for (int k = 0; k < B::R; ++k) v[k] = flip(yl[q + B::TPL * k], r + q + B::TPL * k);
+        B::F::template natural_to_split_flat<false>(v, o, yl, 1, tw, q);
+#pragma unroll
+        for (int i = 0; i < B::R; ++i) yg[B::pos(q, i)] = o[i];
+    };
 
     // t1 <- S(a1*x + b1*P_M(t1)); x1 = a3*t1 + b3*x (kept in the x tile)
-    cp_async_wait<2>();
+    cp_async_wait<1>();
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < B::R; ++k) v[k] = y1[q + B::TPL * k];
-    B::F::template natural_to_split_flat<true>(v, o, y1, 1, tw, q);
-    cp_async_wait<1>();
+    for (int k = 0; k < B::R; ++k) v[k] = yl[q + B::TPL * k];
+    B::F::template natural_to_split_flat<true>(v, o, yl, 1, tw, q);
+    cp_async_wait<0>();
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < B::R; ++i) {
@@ -221,15 +229,20 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 2) k_dml_rows(const DmlDev p, int
         const Cx<float> xv = xs[f];
         const Cx<float> t1n = keep_re(merge_apply(xv, pm, p.a1, p.b1), bit(f));
         xs[f] = merge_apply(t1n, xv, p.a3, p.b3);
-        y1[f] = t1n;
+        yl[f] = t1n;
         if (last) p.t1[row * L + f] = t1n;
     }
-    // t2 <- P_M(t2'); x <- a4*t2 + b4*x1; the next t2' = a2*x + b2*S(t2)
+    __syncwarp();
+    if (!last) forward_row(Y1 + (uint64_t)line * L);
+    // the line's row of Y2 into its slots (this line's threads only)
+    stage(yl, Y2 + (uint64_t)line * L, (uint32_t)(L * 8), true, q, B::TPL);
+    cp_async_commit();
     cp_async_wait<0>();
-    __syncthreads();
+    __syncwarp();
+    // t2 <- P_M(t2'); x <- a4*t2 + b4*x1; the next t2' = a2*x + b2*S(t2)
 #pragma unroll
-    for (int k = 0; k < B::R; ++k) v[k] = y2[q + B::TPL * k];
-    B::F::template natural_to_split_flat<true>(v, o, y2, 1, tw, q);
+    for (int k = 0; k < B::R; ++k) v[k] = yl[q + B::TPL * k];
+    B::F::template natural_to_split_flat<true>(v, o, yl, 1, tw, q);
 #pragma unroll
     for (int i = 0; i < B::R; ++i) {
         const int f = B::pos(q, i);
@@ -239,22 +252,11 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 2) k_dml_rows(const DmlDev p, int
         if (last)
             p.t2[row * L + f] = t2n;
         else
-            y2[f] = merge_apply(xn, keep_re(t2n, bit(f)), p.a2, p.b2);
+            yl[f] = merge_apply(xn, keep_re(t2n, bit(f)), p.a2, p.b2);
     }
     if (last) return;
-    // the next iteration's forward row transforms (rows are read back in
-    // natural order from the tiles the update above wrote in flat order)
     __syncwarp();
-#pragma unroll 1
-    for (int pl = 0; pl < 2; ++pl) {
-        Cx<float>* yt = pl ? y2 : y1;
-#pragma unroll
-        for (int k = 0; k < B::R; ++k) v[k] = flip(yt[q + B::TPL * k], r + q + B::TPL * k);
-        B::F::template natural_to_split_flat<false>(v, o, yt, 1, tw, q);
-        Cx<float>* __restrict__ yg = pl ? Y2 + (uint64_t)line * L : Y1 + (uint64_t)line * L;
-#pragma unroll
-        for (int i = 0; i < B::R; ++i) yg[B::pos(q, i)] = o[i];
-    }
+    forward_row(Y2 + (uint64_t)line * L);
 }
 
 template <int L>
