@@ -14,6 +14,7 @@
 // results; the fused kernel performs the same arithmetic.
 #include "cpra_b200.h"
 #include "cpra_internal.h"
+#include "angle_table.cuh"
 
 #include <algorithm>
 #include <atomic>
@@ -181,6 +182,9 @@ struct cpra_b200_ctx {
     uint64_t refine_bytes = 0;
     void* best_sums = nullptr;
     uint64_t best_bytes = 0;
+    // slices sorted by direction for the gathers over slices (angle_table.cuh)
+    void* atab = nullptr;
+    uint64_t atab_bytes = 0;
     bool graphs = false;
     bool capturing = false;
     uint64_t epoch = 0;  // bumped whenever a context buffer is freed or reallocated
@@ -251,6 +255,20 @@ int ensure_reduction(cpra_b200_ctx* c, uint64_t members) {
     CPRA_CHECK_CUDA(cudaMalloc(&c->sums, sizeof(double) * 2 * members), "cudaMalloc(sums)");
     CPRA_CHECK_CUDA(cudaMallocHost(&c->host_sums, sizeof(double) * 2 * members), "cudaMallocHost(sums)");
     c->red_cap = members;
+    return CPRA_B200_OK;
+}
+
+int ensure_buffer(cpra_b200_ctx* c, void** buf, uint64_t* have, uint64_t bytes, const char* what) {
+    if (*have >= bytes) return CPRA_B200_OK;
+    ++c->epoch;
+    if (*buf) {
+        cudaDeviceSynchronize();
+        cudaFree(*buf);
+        *buf = nullptr;
+        *have = 0;
+    }
+    CPRA_CHECK_CUDA(cudaMalloc(buf, bytes), what);
+    *have = bytes;
     return CPRA_B200_OK;
 }
 
@@ -587,6 +605,7 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     for (GraphEntry& g : c->graph_cache) cudaGraphExecDestroy(g.exec);
     if (c->refine_buf) cudaFree(c->refine_buf);
     if (c->best_sums) cudaFree(c->best_sums);
+    if (c->atab) cudaFree(c->atab);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -810,7 +829,13 @@ int cpra_b200_complex2d_to_3d(cpra_b200_ctx* c, const void* src, void* dst, cons
     if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "Complex2DTo3DInterpolation: zero size");
     int r = flush(c);
     if (r) return take_deferred(c);
-    CPRA_CHECK_CUDA(launch_complex2d_to_3d(c->dbl, src, dst, angles, m, n, p, l, c->stream),
+    void* atab = nullptr;
+    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
+        int rr = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
+        if (rr) return rr;
+        atab = c->atab;
+    }
+    CPRA_CHECK_CUDA(launch_complex2d_to_3d(c->dbl, src, dst, angles, m, n, p, l, atab, c->stream),
                     "Complex2DTo3DInterpolation");
     return CPRA_B200_OK;
 }
@@ -1098,19 +1123,6 @@ int hio_check_params(const HioParams& h, const char* who) {
     return CPRA_B200_OK;
 }
 
-int ensure_buffer(cpra_b200_ctx* c, void** buf, uint64_t* have, uint64_t bytes, const char* what) {
-    if (*have >= bytes) return CPRA_B200_OK;
-    ++c->epoch;
-    if (*buf) {
-        cudaDeviceSynchronize();
-        cudaFree(*buf);
-        *buf = nullptr;
-        *have = 0;
-    }
-    CPRA_CHECK_CUDA(cudaMalloc(buf, bytes), what);
-    *have = bytes;
-    return CPRA_B200_OK;
-}
 
 }  // namespace
 
@@ -1233,7 +1245,13 @@ int cpra_b200_slice_loss_grad(cpra_b200_ctx* c, const void* V, const void* angle
     if (r) return r;
     r = ensure_reduction(c, p);
     if (r) return r;
-    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, grad_V, m, n, p, l, c->partials, c->sums,
+    void* atab = nullptr;
+    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
+        r = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
+        if (r) return r;
+        atab = c->atab;
+    }
+    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, grad_V, m, n, p, l, c->partials, c->sums, atab,
                                            c->stream),
                     "slice_loss_grad");
     CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * p, cudaMemcpyDeviceToHost, c->stream),
@@ -1267,13 +1285,19 @@ int cpra_b200_refine(cpra_b200_ctx* c, void* V, void* angles, const void* A, uin
     if (r) return r;
     r = ensure_reduction(c, p);
     if (r) return r;
+    void* atab = nullptr;
+    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
+        r = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
+        if (r) return r;
+        atab = c->atab;
+    }
     char* buf = static_cast<char*>(c->refine_buf);
     void* gV = buf;
     void* mom = buf + mofs;
     double* loss_dev = reinterpret_cast<double*>(buf + lofs);
     CPRA_CHECK_CUDA(cudaMemsetAsync(mom, 0, mbytes, c->stream), "refine");
     for (int k = 1; k <= steps; ++k) {
-        CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, gV, m, n, p, l, c->partials, c->sums,
+        CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, gV, m, n, p, l, c->partials, c->sums, atab,
                                                c->stream),
                         "refine");
         CPRA_CHECK_CUDA(launch_refine_step(c->dbl, V, angles, gV, mom, vox, p, c->sums, lr_volume, lr_angle, k,

@@ -69,8 +69,11 @@ cudaError_t launch_rfactor_sums(bool dbl, const void* F, const void* A, uint64_t
                                 uint64_t batch, double* partials, double* sums, cudaStream_t st);
 cudaError_t launch_real2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m, uint64_t n,
                                 uint64_t p, uint64_t l, cudaStream_t st);
+// atab (may be null): scratch of angle_table_bytes(p) (angle_table.cuh); with
+// it, and p <= ANGLE_TABLE_MAX, each voxel visits only the slices that can
+// reach it
 cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m,
-                                   uint64_t n, uint64_t p, uint64_t l, cudaStream_t st);
+                                   uint64_t n, uint64_t p, uint64_t l, void* atab, cudaStream_t st);
 
 // ---- fused difference-map iterations (kernels_dm.cu) ---------------------
 // Coefficients of the four MergeAddData calls of one iteration
@@ -122,7 +125,7 @@ cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, ui
 // sums[2p+1] = dL/d ang[p] (partials: >= P * CONVERGE_BLOCKS * 2 doubles)
 cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
                                    uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
-                                   cudaStream_t st);
+                                   void* atab, cudaStream_t st);
 // one Adam step (step >= 1) on the volume (vox complex) and the P angles from
 // gV and the per-slice sums; moments: 4*vox + 2*P elements of the element
 // type, zero before step 1; loss <- sum_p sums[2p]

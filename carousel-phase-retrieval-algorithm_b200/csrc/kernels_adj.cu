@@ -22,6 +22,7 @@
 // Coordinates and weights are computed in double; data stay in T.
 #include "cpra_internal.h"
 #include "ops_ew.cuh"
+#include "angle_table.cuh"
 
 namespace cpra_b200 {
 namespace {
@@ -199,6 +200,51 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __re
     }
 }
 
+// the same gather visiting only the slices that can reach the voxel
+// (angle_table.cuh), in direction order; rows and weights as above, in double
+template <typename T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __restrict__ G, const AngleTable tab,
+                                                                 Cx<T>* __restrict__ gV, int64_t M, int64_t N,
+                                                                 int64_t L) {
+    const uint64_t total = (uint64_t)L * N * M;
+    for (uint64_t i = tid_g(); i < total; i += str_g()) {
+        const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
+        const double cz = (double)(L / 2) - (double)z, cy = (double)(M / 2) - (double)y;
+        double re = 0.0, im = 0.0;
+        for_slices_near(tab, cz, cy, [&](int64_t p, double sa, double ca) {
+            double lo = -1e300, hi = 1e300;
+            if (fabs(sa) > 1e-12) {
+                const double r0 = (cz - 1.0) / sa, r1 = (cz + 1.0) / sa;
+                lo = fmax(lo, fmin(r0, r1));
+                hi = fmin(hi, fmax(r0, r1));
+            } else if (fabs(cz) >= 1.0) {
+                return;
+            }
+            if (fabs(ca) > 1e-12) {
+                const double r0 = (cy - 1.0) / ca, r1 = (cy + 1.0) / ca;
+                lo = fmax(lo, fmin(r0, r1));
+                hi = fmin(hi, fmax(r0, r1));
+            } else if (fabs(cy) >= 1.0) {
+                return;
+            }
+            lo = fmax(lo, (double)(-M));
+            hi = fmin(hi, (double)M);
+            for (int64_t yr = (int64_t)ceil(lo - 1e-9); (double)yr <= hi + 1e-9; ++yr) {
+                const int64_t yIn = M / 2 - yr;
+                if (yIn < 0 || yIn >= M) continue;
+                const double wz = 1.0 - fabs((double)(L / 2) - (double)yr * sa - (double)z);
+                const double wy = 1.0 - fabs((double)(M / 2) - (double)yr * ca - (double)y);
+                if (!(wz > 0.0) || !(wy > 0.0)) continue;
+                const Cx<T> g = G[(p * N + x) * M + yIn];
+                const double wt = wz * wy;
+                re += wt * (double)g.x;
+                im += wt * (double)g.y;
+            }
+        });
+        gV[i] = Cx<T>{(T)re, (T)im};
+    }
+}
+
 // Adam (Kingma & Ba, 2015), in the form with bias-corrected step and
 // denominator: m <- b1 m + (1-b1) g, v <- b2 v + (1-b2) g^2,
 // p <- p - (lr / c1) * m / (sqrt(v) / sqrt(c2) + eps), c_k = 1 - b_k^t.
@@ -306,7 +352,7 @@ cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, ui
 
 cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
                                    uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
-                                   cudaStream_t st) {
+                                   void* atab, cudaStream_t st) {
     if (p == 0) return cudaSuccess;
     if (p > 65535) return cudaErrorInvalidValue;
     dim3 grid(CONVERGE_BLOCKS, (unsigned)p);
@@ -322,6 +368,18 @@ cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, con
     if (e != cudaSuccess) return e;
     const uint64_t vox = l * n * m;
     const unsigned g = ew_grid(vox, ADJ_THREADS);
+    if (atab && p <= (uint64_t)ANGLE_TABLE_MAX) {
+        e = dbl ? launch_sort_angles<double>((const double*)ang, (int64_t)p, atab, st)
+                : launch_sort_angles<float>((const float*)ang, (int64_t)p, atab, st);
+        if (e != cudaSuccess) return e;
+        const AngleTable t = angle_table_view(atab, (int64_t)p);
+        if (dbl)
+            k_slice_adjoint_w<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)G, t, (Cx<double>*)gV, m, n, l);
+        else
+            k_slice_adjoint_w<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)G, t, (Cx<float>*)gV, m, n, l);
+        count_launches(3);
+        return cudaGetLastError();
+    }
     if (dbl)
         k_slice_adjoint<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)G, (const double*)ang, (Cx<double>*)gV,
                                                            m, n, p, l);

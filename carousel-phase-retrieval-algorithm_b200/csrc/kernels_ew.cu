@@ -5,6 +5,7 @@
 // (include/detail/MKL_Impl.inl:83,98,121): each thread keeps one plane value
 // in a register and applies it to every repetition, so a plane is read once.
 #include "cpra_internal.h"
+#include "angle_table.cuh"
 #include "ops_ew.cuh"
 
 #include <cmath>
@@ -340,6 +341,46 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d(const Cx<T>* __r
     }
 }
 
+// the same merge visiting only the slices that can reach the voxel
+// (angle_table.cuh), in direction order
+template <typename T>
+__global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d_w(const Cx<T>* __restrict__ src,
+                                                                  Cx<T>* __restrict__ dst, const AngleTable tab,
+                                                                  int64_t M, int64_t N, int64_t L) {
+    const uint64_t total = (uint64_t)M * N * L;
+    for (uint64_t idx = gtid(); idx < total; idx += gstride()) {
+        const int64_t y = (int64_t)(idx % M);
+        const int64_t x = (int64_t)((idx / M) % N);
+        const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
+        const double j = (double)(L / 2 - z), l = (double)(M / 2 - y);
+        double accx = 0.0, accy = 0.0, wsum = 0.0;
+        for_slices_near(tab, j, l, [&](int64_t p, double sa, double ca) {
+            const double d = j * ca - l * sa;
+            const double wd = 1.0 - fabs(d);
+            if (!(wd > 0.0)) return;
+            const double yIn = (double)(M / 2) - (j * sa + l * ca);
+            const double y0f = floor(yIn);
+            const int64_t y0 = (int64_t)y0f;
+            const double fy = yIn - y0f;
+            double sx = 0.0, sy = 0.0, sw = 0.0;
+            for (int dy = 0; dy < 2; ++dy) {
+                const int64_t yy = y0 + dy;
+                const double wy = dy ? fy : 1.0 - fy;
+                if (yy < 0 || yy >= M || wy == 0.0) continue;
+                const Cx<T> v = src[p * M * N + x * M + yy];
+                sx += wy * (double)v.x;
+                sy += wy * (double)v.y;
+                sw += wy;
+            }
+            if (sw == 0.0) return;
+            accx += wd * sx;
+            accy += wd * sy;
+            wsum += wd * sw;
+        });
+        dst[idx] = (wsum > 0.0) ? Cx<T>{(T)(accx / wsum), (T)(accy / wsum)} : Cx<T>{T(0), T(0)};
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_space_constraint(bool dbl, void* x, const void* s, uint64_t num, uint64_t plane, int mode,
@@ -496,10 +537,24 @@ cudaError_t launch_real2d_to_3d(bool dbl, const void* src, void* dst, const void
 }
 
 cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const void* angles, uint64_t m,
-                                   uint64_t n, uint64_t p, uint64_t l, cudaStream_t st) {
+                                   uint64_t n, uint64_t p, uint64_t l, void* atab, cudaStream_t st) {
     const uint64_t total = m * n * l;
     if (total == 0) return cudaSuccess;
     const unsigned g = ew_grid(total, EW_THREADS);
+    if (atab && p <= (uint64_t)ANGLE_TABLE_MAX) {
+        cudaError_t e = dbl ? launch_sort_angles<double>((const double*)angles, (int64_t)p, atab, st)
+                            : launch_sort_angles<float>((const float*)angles, (int64_t)p, atab, st);
+        if (e != cudaSuccess) return e;
+        const AngleTable t = angle_table_view(atab, (int64_t)p);
+        if (dbl)
+            k_complex2d_to_3d_w<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst, t,
+                                                                  (int64_t)m, (int64_t)n, (int64_t)l);
+        else
+            k_complex2d_to_3d_w<float><<<g, EW_THREADS, 0, st>>>((const Cx<float>*)src, (Cx<float>*)dst, t,
+                                                                 (int64_t)m, (int64_t)n, (int64_t)l);
+        count_launches(2);
+        return cudaGetLastError();
+    }
     if (dbl)
         k_complex2d_to_3d<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst,
                                                             (const double*)angles, (int64_t)m, (int64_t)n,

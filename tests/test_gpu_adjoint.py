@@ -195,3 +195,32 @@ def test_best_start(tb):
     want = [np.mean([O.rfactor(x[p, k].ravel(), A[p].ravel(), L, L, 1) for p in range(P)]) for k in range(B)]
     np.testing.assert_allclose(scores, want, rtol=1e-5, atol=1e-6)
     np.testing.assert_array_equal(out.cpu().numpy().reshape(P, L, L), x[:, best])
+
+
+@pytest.mark.parametrize("P", [37, 4100])
+def test_gathers_any_angles_vs_oracle(tb, P):
+    """The gathers over slices (merge adjoint and trilinear merge) visit only the
+    slices whose direction can reach a voxel (sorted table, up to 4096 slices)
+    or all of them (above): both match the float64 oracle for angles over
+    several turns, negative, beyond pi, repeated, and on 0 and pi exactly."""
+    torch, cb = tb
+    M, L = 8, 8
+    rng = np.random.default_rng(P)
+    V = (rng.standard_normal(L * M * M) + 1j * rng.standard_normal(L * M * M)).astype(np.complex128)
+    ang = rng.uniform(-7.0, 9.0, P)
+    ang[:4] = [0.0, np.pi, -np.pi, 2 * np.pi]
+    ang[4:8] = ang[8:12]
+    A = rng.uniform(0.2, 2.0, P * M * M)
+    impl = cb.B200Impl(M, M, L, 1, dtype="float64")
+    gV = torch.zeros(V.size, dtype=torch.complex128, device="cuda")
+    loss, ga = impl.slice_loss_grad(torch.from_numpy(V).cuda(), torch.from_numpy(ang).cuda(),
+                                    torch.from_numpy(A).cuda(), M, M, P, L, gV)
+    lo, gVo, gao = O.slice_loss_grad(V, ang, A, M, M, P, L)
+    assert abs(loss - lo) / lo < 1e-12
+    assert O.rel_l2(gV.cpu().numpy(), gVo.ravel()) < 1e-12
+    src = (rng.standard_normal(P * M * M) + 1j * rng.standard_normal(P * M * M)).astype(np.complex128)
+    dst = torch.zeros(L * M * M, dtype=torch.complex128, device="cuda")
+    assert impl.Complex2DTo3DInterpolation(torch.from_numpy(src).cuda(), dst, torch.from_numpy(ang).cuda(),
+                                           M, M, P, L) and impl.Sync()
+    want = O.complex2d_to_3d(np.float64, src, ang, M, M, P, L)
+    assert O.rel_l2(dst.cpu().numpy(), want) < 1e-12
