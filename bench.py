@@ -53,6 +53,12 @@ def parse():
                     help="uneven / carousel3d: only that side measurement (one JSON line, for profiling runs)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
+    # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
+    ap.add_argument("--angle-step", type=float, default=1.0, help="degrees between projections")
+    ap.add_argument("--photons", type=float, default=1e8)
+    ap.add_argument("--ellipsoids", type=int, default=64)
+    ap.add_argument("--axes", default="4,16", help="ellipsoid semi-axis range, voxels")
+    ap.add_argument("--refine-steps", type=int, default=50)
     return ap.parse_args()
 
 
@@ -330,7 +336,9 @@ def main():
 
     if a.case == "carousel3d":
         out = carousel3d_adjoint(torch, cpra_b200, torch.device("cuda", local), n=a.size, P=a.angles,
-                                 B=a.starts, epi=a.episodes, iters=a.iters)
+                                 B=a.starts, epi=a.episodes, iters=a.iters, refine_steps=a.refine_steps,
+                                 step_deg=a.angle_step, photons=a.photons, ellipsoids=a.ellipsoids,
+                                 axes=tuple(float(v) for v in a.axes.split(",")))
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -523,7 +531,8 @@ def episode_3d(torch, cpra_b200, d, dev, iters3d=10):
             "total_ms": e[0].elapsed_time(e[2]), "volume": [n, n, n], "slices": P}
 
 
-def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=10, refine_steps=50):
+def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=10, refine_steps=50, step_deg=1.0,
+                       photons=1e8, ellipsoids=64, axes=(4, 16)):
     """The 256^3 carousel with adjoint refinement: a 256^3 volume of 64
     ellipsoids, 180 angles at 1 degree jittered by N(0, 0.3 degree), 256^2
     patterns at 1e8 photons (synthesised on the GPU, cpra_b200.synth.
@@ -541,7 +550,8 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
         nominal angles) through the hand-written adjoints."""
     from cpra_b200 import synth
     t0 = time.perf_counter()
-    d = synth.carousel_gpu(torch, n=n, P=P, device=dev)
+    d = synth.carousel_gpu(torch, n=n, P=P, step_deg=step_deg, photons=photons, ellipsoids=ellipsoids, axes=axes,
+                           device=dev)
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     A, S = d["A"].reshape(-1), d["S"].reshape(-1)
@@ -584,7 +594,7 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     if kt and kt[1] > 0:
         achieved = DM_BYTES_PER_PIXEL * n * n * kt[2] / (kt[0] / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "kernels": "k_dml_first/k_dml_cols/k_dml_rows<256> (fused DM line passes)",
+                "kernels": f"k_dml_first/k_dml_cols/k_dml_rows<{n}> (fused DM line passes)",
                 "fused_ms": kt[0], "share_of_stage": kt[0] / ms_direct, "peak_kind": peak_kind}
     try:
         per_op = per_op_compare(torch, cpra_b200, d["A"].cpu().numpy(), d["S"].cpu().numpy(), B, n, iters)
@@ -619,9 +629,10 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     for o in (impl, impl2, impl3):
         o.close()
     return {
-        "workload": f"carousel 3D with adjoint refinement: {n}^3 volume (64 ellipsoids), {P} angles at 1 deg "
-                    f"jittered N(0, 0.3 deg), {n}^2 patterns at 1e8 photons; 2D stage {epi} episodes x {iters} DM "
-                    f"iterations x {B} starts; best start; merge; {refine_steps} Adam steps",
+        "workload": f"carousel 3D with adjoint refinement: {n}^3 volume ({ellipsoids} ellipsoids, semi-axes "
+                    f"{axes[0]:g}-{axes[1]:g}), {P} angles at {step_deg:g} deg jittered N(0, 0.3 deg), {n}^2 "
+                    f"patterns at {photons:.0e} photons; 2D stage {epi} episodes x {iters} DM iterations x {B} "
+                    f"starts; best start; merge; {refine_steps} Adam steps",
         "stage2d": {"value": units / (ms2d / 1e3), "unit": METRIC, "ms": ms2d, "graph": True,
                     "value_direct": units / (ms_direct / 1e3), "roofline": roof,
                     "per_op_path": per_op,
