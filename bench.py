@@ -69,6 +69,15 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(value, dist, device):
+    """The slowest rank's time: all ranks take part (same collective, same
+    order), each contributing its own CUDA-event time."""
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload_config(a, ws):
     return {
         "workload": f"carousel 2D stage: {a.size}x{a.size} complex64, {a.angles} angles, "
@@ -401,9 +410,7 @@ def main():
         if kernel_timing:
             impl.set_option(cpra_b200.OPT_KERNEL_TIMING, 0)
         if ws > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = max_over_ranks(ms, dist, dev)
             dist.barrier()
         return ms, launches, kt
 
