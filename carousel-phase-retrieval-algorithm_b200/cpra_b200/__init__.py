@@ -87,6 +87,7 @@ _SIGS = {
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                  C.c_void_p],
+    "cpra_b200_constraint3d": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int],
     "cpra_b200_refine": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 +
                         [C.c_int, C.c_double, C.c_double, C.c_void_p],
     "cpra_b200_best_start": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p,
@@ -328,6 +329,12 @@ class B200Impl:
                                                int(l), _addr(grad_V), loss.ctypes.data_as(C.c_void_p),
                                                ga.ctypes.data_as(C.c_void_p)), "slice_loss_grad")
         return float(loss[0]), ga
+
+    def constraint3d(self, x, C, S, iters=1) -> bool:
+        """iters x (Forward3D, complex DataConstraint with C, Backward3D,
+        SpaceConstraint with S) on the context's volumes, fused."""
+        return _check(lib().cpra_b200_constraint3d(self._h, _addr(x), _addr(C), _addr(S), int(iters)),
+                      "constraint3d")
 
     def refine(self, V, angles, A, m, n, p, l, steps, lr_volume=1e-3, lr_angle=1e-3):
         """Adam steps on the volume and the angles against the amplitude loss

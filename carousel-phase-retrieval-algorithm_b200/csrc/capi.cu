@@ -736,6 +736,40 @@ static int run_fft3d(cpra_b200_ctx* c, void* x, bool inverse) {
     return CPRA_B200_OK;
 }
 
+int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void* S, int iters) {
+    CTX_OR_RETURN(c);
+    if (!x || !C || !S) return fail(CPRA_B200_EARG, "constraint3d: null pointer");
+    if (iters < 0) return fail(CPRA_B200_EARG, "constraint3d: iters must be >= 0");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
+        return fail(CPRA_B200_EUNSUP, "constraint3d: each size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t vol = c->m * c->n * c->l, num = vol * c->batch;
+    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
+    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
+    if (constraint3d_fused_supported(c->m, c->n, c->l)) {
+        CPRA_CHECK_CUDA(launch_constraint3d(c->dbl, x, C, S, c->m, c->n, c->l, c->batch, iters, c->space_mode, scale,
+                                            twiddles(c, c->m), twiddles(c, c->n), twiddles(c, c->l), c->work,
+                                            c->stream),
+                        "constraint3d");
+        return CPRA_B200_OK;
+    }
+    // other sizes: the four operators in turn
+    r = ensure_work(c, num * c->csize());
+    if (r) return r;
+    for (int it = 0; it < iters; ++it) {
+        CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, false, scale, twiddles(c, c->m),
+                                     twiddles(c, c->n), twiddles(c, c->l), c->work, c->stream),
+                        "constraint3d");
+        CPRA_CHECK_CUDA(launch_data_constraint_complex(c->dbl, x, C, num, vol, c->stream), "constraint3d");
+        CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, true, scale, twiddles(c, c->m),
+                                     twiddles(c, c->n), twiddles(c, c->l), c->work, c->stream),
+                        "constraint3d");
+        CPRA_CHECK_CUDA(launch_space_constraint(c->dbl, x, S, num, vol, c->space_mode, c->stream), "constraint3d");
+    }
+    return CPRA_B200_OK;
+}
+
 int cpra_b200_forward3d(cpra_b200_ctx* c, void* x) {
     CTX_OR_RETURN(c);
     return run_fft3d(c, x, false);

@@ -30,6 +30,15 @@ cudaError_t launch_fft2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t bat
 cudaError_t launch_fft3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch, bool inverse,
                          double scale, const void* tw_m, const void* tw_n, const void* tw_l, void* work,
                          cudaStream_t st);
+// The benchmark's 3D step (src/benchmark_mkl.cpp:164-170), `iters` times:
+// Forward3D; DataConstraint (complex C, plane M*N*L); Backward3D (scale);
+// SpaceConstraint (S, plane M*N*L, space_mode) as five axis passes per
+// iteration, same bits as the four per-operator calls.  Power-of-two sizes
+// 2..1024 on every axis.
+bool constraint3d_fused_supported(uint64_t M, uint64_t N, uint64_t L);
+cudaError_t launch_constraint3d(bool dbl, void* x, const void* C, const void* S, uint64_t M, uint64_t N, uint64_t L,
+                                uint64_t batch, int iters, int space_mode, double scale, const void* tw_m,
+                                const void* tw_n, const void* tw_l, void* work, cudaStream_t st);
 // True when the 2D shape runs as one CTA per plane (one HBM round trip).
 bool fft2d_single_cta(bool dbl, uint64_t M, uint64_t N);
 // True when a 1D length is supported at all by the transforms.

@@ -12,6 +12,7 @@
 //   * other even lengths: a direct O(L^2) DFT pass per axis.
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
+#include "ops_ew.cuh"
 
 namespace cpra_b200 {
 
@@ -89,17 +90,30 @@ cudaError_t plane_fft(void* x, uint64_t batch, bool inverse, T scale, int s_neg,
 // ---------------------------------------------------------------------------
 constexpr int AXIS_THREADS = 256;
 
+// Optional per-line work of an axis pass (the fused 3D constraint step):
+//   AXIS_DC_ROUNDTRIP: forward transform, complex DataConstraint with C at
+//     each element, inverse transform, with the per-call passes' sign flips in
+//     the same order (output flip, constraint, input flip of the inverse);
+//   AXIS_SPACE: SpaceConstraint with S on the pass's output.
+// aux is indexed as the operators index their constraint, i % aux_plane.
+enum AxisOpKind : int { AXIS_PLAIN = 0, AXIS_DC_ROUNDTRIP = 1, AXIS_SPACE = 2 };
+struct AxisOp {
+    int kind = AXIS_PLAIN;
+    const void* aux = nullptr;
+    uint64_t aux_plane = 1;
+    int space_mode = 0;
+};
+
 template <typename T, int L, int TPL>
 __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ data, uint64_t Bo, uint64_t Bi,
                                                            uint64_t tiles_i, const Cx<T>* __restrict__ twg,
                                                            int inverse, int shift, int out_neg, T scale,
-                                                           int do_scale) {
+                                                           int do_scale, AxisOp op) {
     constexpr int LINES = AXIS_THREADS / TPL;
     constexpr int PADL = TPL < 16 ? TPL : 0;
     constexpr int LSX = L + PADL;
     constexpr int R = L / TPL;
-    constexpr int J = R / TPL;
-    using F = LineFFT<T, L, TPL>;
+        using F = LineFFT<T, L, TPL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
     Cx<T>* tw = buf + LINES * LSX;
@@ -147,12 +161,35 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
     else
         F::template natural_to_split_flat<false>(v, o, buf + line * LSX, 1, tw, q);
+    // global index of element n of this thread's line, and whether the line exists
+    const bool line_ok = contig ? (o0 + line) < Bo : (i0 + line) < Bi;
+    auto gindex = [&](int n) -> uint64_t {
+        return contig ? (o0 + line) * (uint64_t)L + n : (o0 * L + n) * Bi + i0 + line;
+    };
+    if (op.kind == AXIS_DC_ROUNDTRIP) {
+        const Cx<T>* __restrict__ C = static_cast<const Cx<T>*>(op.aux);
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int f = F::pos(q, i);
+            Cx<T> w = o[i];
+            if (shift) w = csign(w, f + out_neg);
+            if (line_ok) w = data_apply_complex(w, C[gindex(f) % op.aux_plane]);
+            if (shift) w = csign(w, f);  // the inverse pass's input flip
+            buf[line * LSX + f] = w;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < R; ++k) v[k] = buf[line * LSX + q + TPL * k];
+        F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
+    }
 #pragma unroll
     for (int i = 0; i < R; ++i) {
         const int f = F::pos(q, i);
         Cx<T> w = o[i];
         if (do_scale) w = cscale(w, scale);
         if (shift) w = csign(w, f + out_neg);
+        if (op.kind == AXIS_SPACE && line_ok)
+            w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
         buf[line * LSX + f] = w;
     }
     __syncthreads();
@@ -177,7 +214,7 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
 
 template <typename T, int L, int TPL>
 cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shift, int out_neg, T scale,
-                       bool do_scale, const void* tw, cudaStream_t st) {
+                       bool do_scale, const void* tw, cudaStream_t st, AxisOp op = AxisOp{}) {
     constexpr int LINES = AXIS_THREADS / TPL;
     constexpr int PADL = TPL < 16 ? TPL : 0;
     const size_t smem = sizeof(Cx<T>) * ((size_t)LINES * (L + PADL) + LineFFT<T, L, TPL>::TW_ENTRIES);
@@ -194,7 +231,7 @@ cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shi
     if (tiles == 0) return cudaSuccess;
     if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
     kf<<<(unsigned)tiles, AXIS_THREADS, smem, st>>>((Cx<T>*)x, Bo, Bi, tiles_i, (const Cx<T>*)tw, inverse ? 1 : 0,
-                                                    shift ? 1 : 0, out_neg, scale, do_scale ? 1 : 0);
+                                                    shift ? 1 : 0, out_neg, scale, do_scale ? 1 : 0, op);
     count_launches();
     return cudaGetLastError();
 }
@@ -247,7 +284,7 @@ bool is_pow2(uint64_t n) { return n > 0 && (n & (n - 1)) == 0; }
 
 template <typename T>
 cudaError_t axis_pass(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi, bool inverse, T scale,
-                      bool do_scale, const void* tw, cudaStream_t st) {
+                      bool do_scale, const void* tw, cudaStream_t st, AxisOp op = AxisOp{}) {
     const int out_neg = (int)((L / 2) & 1);  // s_a = (-1)^(L/2)
     if (L == 1) {
         if (!do_scale) return cudaSuccess;
@@ -255,18 +292,18 @@ cudaError_t axis_pass(void* x, void* work, uint64_t Bo, uint64_t L, uint64_t Bi,
     }
     if (!is_pow2(L) || L > 1024) return axis_dft_t<T>(x, work, Bo, L, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
     switch (L) {
-        case 2: return axis_fft_t<T, 2, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 4: return axis_fft_t<T, 4, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 8: return axis_fft_t<T, 8, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 16: return axis_fft_t<T, 16, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 32: return axis_fft_t<T, 32, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 64: return axis_fft_t<T, 64, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 128: return axis_fft_t<T, 128, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 2: return axis_fft_t<T, 2, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 4: return axis_fft_t<T, 4, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 8: return axis_fft_t<T, 8, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 16: return axis_fft_t<T, 16, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 32: return axis_fft_t<T, 32, 1>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 64: return axis_fft_t<T, 64, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 128: return axis_fft_t<T, 128, 4>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
         // 256 and 512: 16 and 32 threads per line, the split of the fused line
         // passes (line_pass.cuh LineGeom), so those round exactly like these calls
-        case 256: return axis_fft_t<T, 256, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 512: return axis_fft_t<T, 512, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
-        case 1024: return axis_fft_t<T, 1024, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st);
+        case 256: return axis_fft_t<T, 256, 16>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 512: return axis_fft_t<T, 512, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
+        case 1024: return axis_fft_t<T, 1024, 32>(x, Bo, Bi, inverse, true, out_neg, scale, do_scale, tw, st, op);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -308,7 +345,51 @@ cudaError_t fft3d_t(void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch,
     return axis_pass<T>(x, work, batch * L * M, N, 1, true, scale, true, tw_n, st);
 }
 
+// iters x [Forward3D; DataConstraint(C); Backward3D; SpaceConstraint(S)] as
+// five axis passes per iteration (x, y forward; z forward + constraint +
+// inverse; y inverse; x inverse + SpaceConstraint), the per-call passes'
+// arithmetic in the same order
+template <typename T>
+cudaError_t constraint3d_t(void* x, const void* C, const void* S, uint64_t M, uint64_t N, uint64_t L, uint64_t batch,
+                           int iters, int space_mode, T scale, const void* tw_m, const void* tw_n, const void* tw_l,
+                           void* work, cudaStream_t st) {
+    const uint64_t plane = M * N * L;
+    AxisOp dc;
+    dc.kind = AXIS_DC_ROUNDTRIP;
+    dc.aux = C;
+    dc.aux_plane = plane;
+    AxisOp sc;
+    sc.kind = AXIS_SPACE;
+    sc.aux = S;
+    sc.aux_plane = plane;
+    sc.space_mode = space_mode;
+    cudaError_t e;
+    for (int it = 0; it < iters; ++it) {
+        if ((e = axis_pass<T>(x, work, batch * L * M, N, 1, false, scale, false, tw_n, st)) != cudaSuccess) return e;
+        if ((e = axis_pass<T>(x, work, batch * L, M, N, false, scale, false, tw_m, st)) != cudaSuccess) return e;
+        if ((e = axis_pass<T>(x, work, batch, L, M * N, false, scale, false, tw_l, st, dc)) != cudaSuccess) return e;
+        if ((e = axis_pass<T>(x, work, batch * L, M, N, true, scale, false, tw_m, st)) != cudaSuccess) return e;
+        if ((e = axis_pass<T>(x, work, batch * L * M, N, 1, true, scale, true, tw_n, st, sc)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
+
+bool constraint3d_fused_supported(uint64_t M, uint64_t N, uint64_t L) {
+    auto p2 = [](uint64_t v) { return v >= 2 && (v & (v - 1)) == 0 && v <= 1024; };
+    return p2(M) && p2(N) && p2(L);
+}
+
+cudaError_t launch_constraint3d(bool dbl, void* x, const void* C, const void* S, uint64_t M, uint64_t N, uint64_t L,
+                                uint64_t batch, int iters, int space_mode, double scale, const void* tw_m,
+                                const void* tw_n, const void* tw_l, void* work, cudaStream_t st) {
+    if (!constraint3d_fused_supported(M, N, L)) return cudaErrorInvalidValue;
+    if (batch == 0 || iters <= 0) return cudaSuccess;
+    return dbl ? constraint3d_t<double>(x, C, S, M, N, L, batch, iters, space_mode, scale, tw_m, tw_n, tw_l, work, st)
+               : constraint3d_t<float>(x, C, S, M, N, L, batch, iters, space_mode, (float)scale, tw_m, tw_n, tw_l,
+                                       work, st);
+}
 
 bool fft2d_single_cta(bool dbl, uint64_t M, uint64_t N) {
     if (M != N) return false;

@@ -202,6 +202,16 @@ int cpra_b200_hio_batched(cpra_b200_ctx* ctx, const cpra_b200_hio_bucket* bucket
                           double beta, int sw_every, double sigma_start, double sigma_end, double threshold,
                           int positivity);
 
+/* Extension: `iters` repetitions of the reference benchmark's 3D step
+ * (src/benchmark_mkl.cpp:164-170) on the context's [batch][l][m][n] volumes:
+ * Forward3D(x); DataConstraint(x, C, m*n*l*batch, batch) (complex C, one
+ * volume shared by the batch); Backward3D(x); SpaceConstraint(x, S, same).
+ * For power-of-two sizes (2..1024 per axis) an iteration is five axis passes
+ * (the z pass runs forward transform, constraint and inverse transform per
+ * line; the last x pass applies SpaceConstraint) with the same results, bit
+ * for bit, as the four operator calls; other sizes run the four operators. */
+int cpra_b200_constraint3d(cpra_b200_ctx* ctx, void* x, const void* C, const void* S, int iters);
+
 /* Extension (project-defined): central slices of a Fourier volume.  V is
  * [l][n][m] complex (y fastest), slices are [p][n][m]; slice pixel (xIn, yIn)
  * at angle a (radians, element type) samples V bilinearly at z = l/2 - yr sin a,

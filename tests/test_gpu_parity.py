@@ -834,3 +834,48 @@ def test_hio_batched_graph_replay_bitwise(tb):
         for b, w in zip(bk, want):
             np.testing.assert_array_equal(host(b["x"]), host(w["x"]))
             np.testing.assert_array_equal(host(b["S"]), host(w["S"]))
+
+
+# ---- the benchmark's 3D step, fused ---------------------------------------------------------
+@pytest.mark.parametrize("T,M,N,L,B,mode", [(np.float32, 32, 32, 32, 2, 0), (np.float32, 64, 64, 64, 1, 1),
+                                            (np.float64, 16, 16, 16, 1, 0), (np.float32, 8, 16, 32, 2, 0),
+                                            (np.float32, 24, 24, 24, 1, 0)])
+def test_constraint3d_equals_operator_calls(tb, T, M, N, L, B, mode):
+    """constraint3d (five axis passes per iteration) writes the same bits as
+    Forward3D, DataConstraint (complex), Backward3D, SpaceConstraint called one
+    at a time (src/benchmark_mkl.cpp:164-170), and follows the oracle."""
+    torch, cb = tb
+    rng = np.random.default_rng(M * N + L)
+    cdt = np.complex64 if T == np.float32 else np.complex128
+    vol = M * N * L
+    x0 = (rng.standard_normal(B * vol) + 1j * rng.standard_normal(B * vol)).astype(cdt)
+    C = (rng.standard_normal(vol) + 1j * rng.standard_normal(vol)).astype(cdt)
+    C[rng.uniform(size=vol) < 0.3] = 0
+    S = (rng.uniform(size=vol) > 0.4).astype(T)
+    dtype = "float32" if T == np.float32 else "float64"
+    outs = []
+    for fused in (False, True):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
+        assert impl.set_option(cb.OPT_SPACE_MODE, mode)
+        x = dev(torch, x0)
+        Cd, Sd = dev(torch, C), dev(torch, S)
+        for _ in range(2):
+            if fused:
+                assert impl.constraint3d(x, Cd, Sd, 1)
+            else:
+                assert impl.Forward3D(x)
+                assert impl.DataConstraint(x, Cd, B * vol, B)
+                assert impl.Backward3D(x)
+                assert impl.SpaceConstraint(x, Sd, B * vol, B)
+        assert impl.Sync()
+        outs.append(host(x))
+    np.testing.assert_array_equal(outs[0], outs[1])
+    if mode == 0:
+        o = O.OracleImpl(T, M, N, L, B)
+        xo = x0.copy()
+        for _ in range(2):
+            o.Forward3D(xo)
+            o.DataConstraint(xo, C, B * vol, B)
+            o.Backward3D(xo)
+            o.SpaceConstraint(xo, S, B * vol, B)
+        assert O.rel_l2(outs[1], xo) < (1e-5 if T == np.float32 else 1e-12)
