@@ -75,7 +75,7 @@ int cuda_fail(cudaError_t e, const char* where) {
         if (_e != cudaSuccess) return cuda_fail(_e, where); \
     } while (0)
 
-enum class OpKind { Fwd2D, Bwd2D, DataReal, Merge, Space };
+enum class OpKind { Fwd2D, Bwd2D, DataReal, Merge, Space, Fwd3D, Bwd3D };
 
 struct Op {
     OpKind kind;
@@ -90,8 +90,10 @@ struct DmPattern {
     const void *A, *S;
     uint64_t num, batch;
     DmCoef c;
+    int dim = 2;  // 2: Forward2D/Backward2D iteration; 3: the same with Forward3D/Backward3D
     bool operator==(const DmPattern& o) const {
-        return x == o.x && t1 == o.t1 && t2 == o.t2 && A == o.A && S == o.S && num == o.num && batch == o.batch &&
+        return dim == o.dim && x == o.x && t1 == o.t1 && t2 == o.t2 && A == o.A && S == o.S && num == o.num &&
+               batch == o.batch &&
                c.a1 == o.c.a1 && c.b1 == o.c.b1 && c.a2 == o.c.a2 && c.b2 == o.c.b2 && c.a3 == o.c.a3 &&
                c.b3 == o.c.b3 && c.a4 == o.c.a4 && c.b4 == o.c.b4;
     }
@@ -295,10 +297,28 @@ int run_fft2d(cpra_b200_ctx* c, void* x, bool inverse) {
     return CPRA_B200_OK;
 }
 
+// the 3D transform itself (arguments checked, recorder already flushed)
+int exec_fft3d(cpra_b200_ctx* c, void* x, bool inverse) {
+    auto p2 = [](uint64_t v) { return (v & (v - 1)) == 0 && v <= 1024; };
+    if (!(p2(c->m) && p2(c->n) && p2(c->l))) {
+        int r = ensure_work(c, c->batch * c->m * c->n * c->l * c->csize());
+        if (r) return r;
+    }
+    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
+    const uint64_t vol = c->m * c->n * c->l;
+    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
+    CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, inverse, scale, twiddles(c, c->m),
+                                 twiddles(c, c->n), twiddles(c, c->l), c->work, c->stream),
+                    inverse ? "Backward3D" : "Forward3D");
+    return CPRA_B200_OK;
+}
+
 int exec_op(cpra_b200_ctx* c, const Op& op) {
     switch (op.kind) {
         case OpKind::Fwd2D: return run_fft2d(c, op.dst, false);
         case OpKind::Bwd2D: return run_fft2d(c, op.dst, true);
+        case OpKind::Fwd3D: return exec_fft3d(c, op.dst, false);
+        case OpKind::Bwd3D: return exec_fft3d(c, op.dst, true);
         case OpKind::DataReal:
             CPRA_CHECK_CUDA(launch_data_constraint_real(c->dbl, op.dst, op.src, op.num, op.num / op.batch, c->data_mode,
                                                         c->stream),
@@ -355,6 +375,7 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
     a.space_mode = c->space_mode;
     a.data_mode = c->data_mode;
     a.c = p.c;
+    a.L = (p.dim == 3) ? c->l : 1;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     const bool timed = c->timing && !c->capturing;  // graph replays are not timed per launch
     if (timed) {
@@ -368,7 +389,17 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
         }
         CPRA_CHECK_CUDA(cudaEventRecord(ev[0], c->stream), "cudaEventRecord");
     }
-    int r = run_dm(c, a, "fused difference-map iteration");
+    int r;
+    if (p.dim == 3) {
+        const uint64_t vol = c->m * c->n * c->l;
+        const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
+        CPRA_CHECK_CUDA(launch_dm3d_iterations(c->dbl, a, scale, twiddles(c, c->m), twiddles(c, c->n),
+                                               twiddles(c, c->l), c->work, c->stream),
+                        "fused 3D difference-map iteration");
+        r = CPRA_B200_OK;
+    } else {
+        r = run_dm(c, a, "fused difference-map iteration");
+    }
     if (r) return r;
     if (timed) {
         CPRA_CHECK_CUDA(cudaEventRecord(ev[1], c->stream), "cudaEventRecord");
@@ -429,24 +460,31 @@ int take_deferred(cpra_b200_ctx* c) {
 }
 
 bool fusable_shape(const cpra_b200_ctx* c) { return c->fusion && dm_fusable(c); }
+// the 3D iteration fuses for power-of-two volumes (axis passes)
+bool fusable_shape3d(const cpra_b200_ctx* c) {
+    return c->fusion && c->l > 1 && constraint3d_fused_supported(c->m, c->n, c->l);
+}
 
 // Does `op` extend the pending prefix (of length k) of the pattern?
 bool extends(const cpra_b200_ctx* c, const Op& op) {
     const std::vector<Op>& P = c->pending;
     const size_t k = P.size();
-    const uint64_t num = c->plane() * c->batch;
+    const bool d3 = P[0].kind == OpKind::Fwd3D;
+    const uint64_t plane = c->plane() * (d3 ? c->l : 1);  // the constraints' plane (num / batch)
+    const uint64_t num = plane * c->batch;
     const uint64_t cbytes = num * c->csize();
-    const uint64_t rbytes = c->plane() * c->esize();
+    const uint64_t rbytes = plane * c->esize();
+    const OpKind FWD = d3 ? OpKind::Fwd3D : OpKind::Fwd2D, BWD = d3 ? OpKind::Bwd3D : OpKind::Bwd2D;
     auto T1 = [&]() { return P[0].dst; };
     auto is_ew = [&](OpKind kind) {
         return op.kind == kind && op.num == num && op.batch == c->batch && op.num % op.batch == 0 &&
-               op.num / op.batch == c->plane();
+               op.num / op.batch == plane;
     };
     switch (k) {
         case 1:  // DataConstraint(t1, A)
             return is_ew(OpKind::DataReal) && op.dst == T1() && !overlap(op.src, rbytes, T1(), cbytes);
         case 2:  // Backward2D(t1)
-            return op.kind == OpKind::Bwd2D && op.dst == T1();
+            return op.kind == BWD && op.dst == T1();
         case 3:  // MergeAddData(x, t1, a1, b1)
             return op.kind == OpKind::Merge && op.num == num && op.dst == T1() && !overlap(op.src, cbytes, T1(), cbytes) &&
                    !overlap(op.src, cbytes, P[1].src, rbytes);
@@ -462,11 +500,11 @@ bool extends(const cpra_b200_ctx* c, const Op& op) {
         case 6:  // MergeAddData(x, t2, a2, b2)
             return op.kind == OpKind::Merge && op.num == num && op.src == P[3].src && op.dst == P[5].dst;
         case 7:  // Forward2D(t2)
-            return op.kind == OpKind::Fwd2D && op.dst == P[5].dst;
+            return op.kind == FWD && op.dst == P[5].dst;
         case 8:  // DataConstraint(t2, A)
             return is_ew(OpKind::DataReal) && op.dst == P[5].dst && op.src == P[1].src;
         case 9:  // Backward2D(t2)
-            return op.kind == OpKind::Bwd2D && op.dst == P[5].dst;
+            return op.kind == BWD && op.dst == P[5].dst;
         case 10:  // MergeAddData(t1, x, a3, b3)
             return op.kind == OpKind::Merge && op.num == num && op.src == T1() && op.dst == P[3].src;
         case 11:  // MergeAddData(t2, x, a4, b4)
@@ -485,19 +523,17 @@ DmPattern pattern_of(const std::vector<Op>& P) {
     d.num = P[1].num;
     d.batch = P[1].batch;
     d.c = {P[3].alpha, P[3].beta, P[6].alpha, P[6].beta, P[10].alpha, P[10].beta, P[11].alpha, P[11].beta};
+    d.dim = (P[0].kind == OpKind::Fwd3D) ? 3 : 2;
     return d;
 }
 
 // Entry for every operator that the recorder may hold.
 int submit(cpra_b200_ctx* c, const Op& op) {
-    if (!fusable_shape(c)) {
-        int r = flush(c);
-        if (r) return take_deferred(c);
-        return exec_op(c, op);
-    }
     if (c->pending.empty()) {
-        if (op.kind == OpKind::Fwd2D) {
-            if (c->held_iters > 0 && op.dst != c->held.t1) {
+        const bool start2 = op.kind == OpKind::Fwd2D && fusable_shape(c);
+        const bool start3 = op.kind == OpKind::Fwd3D && fusable_shape3d(c);
+        if (start2 || start3) {
+            if (c->held_iters > 0 && (op.dst != c->held.t1 || c->held.dim != (start3 ? 3 : 2))) {
                 int r = flush(c);
                 if (r) return take_deferred(c);
             }
@@ -720,20 +756,7 @@ static int run_fft3d(cpra_b200_ctx* c, void* x, bool inverse) {
     if (!x) return fail(CPRA_B200_EARG, inverse ? "Backward3D: null pointer" : "Forward3D: null pointer");
     if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
         return fail(CPRA_B200_EUNSUP, "3D transform: each size must be 1 or even and at most 4096");
-    int r = flush(c);
-    if (r) return take_deferred(c);
-    auto p2 = [](uint64_t v) { return (v & (v - 1)) == 0 && v <= 1024; };
-    if (!(p2(c->m) && p2(c->n) && p2(c->l))) {
-        r = ensure_work(c, c->batch * c->m * c->n * c->l * c->csize());
-        if (r) return r;
-    }
-    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
-    const uint64_t vol = c->m * c->n * c->l;
-    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
-    CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, inverse, scale, twiddles(c, c->m),
-                                 twiddles(c, c->n), twiddles(c, c->l), c->work, c->stream),
-                    inverse ? "Backward3D" : "Forward3D");
-    return CPRA_B200_OK;
+    return submit(c, Op{inverse ? OpKind::Bwd3D : OpKind::Fwd3D, x, nullptr, 0, 0, 0, 0});
 }
 
 int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void* S, int iters) {

@@ -114,9 +114,16 @@ struct DmArgs {
     int space_mode;
     int data_mode;
     DmCoef c;
+    uint64_t L = 1;  // 3D difference map: volumes [batch][L][M][N] (launch_dm3d_iterations)
 };
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
+// The difference-map iteration with the 3D transforms (src/CONV_MKL.cpp:37-88)
+// on [batch][L][M][N] volumes, A and S one volume each (a_stride, s_stride
+// unused), `iters` times as ten axis passes per iteration; same bits as the
+// 12 operator calls.  Power-of-two sizes 2..1024 (constraint3d_fused_supported).
+cudaError_t launch_dm3d_iterations(bool dbl, const DmArgs& a, double scale, const void* tw_m, const void* tw_n,
+                                   const void* tw_l, void* work, cudaStream_t st);
 
 // ---- the same iterations as line passes at 256 and 512 (kernels_dm_large.cu) ----
 // Float square planes with the threshold SpaceConstraint; S shared

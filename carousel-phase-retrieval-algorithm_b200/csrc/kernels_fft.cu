@@ -96,12 +96,28 @@ constexpr int AXIS_THREADS = 256;
 //     the same order (output flip, constraint, input flip of the inverse);
 //   AXIS_SPACE: SpaceConstraint with S on the pass's output.
 // aux is indexed as the operators index their constraint, i % aux_plane.
-enum AxisOpKind : int { AXIS_PLAIN = 0, AXIS_DC_ROUNDTRIP = 1, AXIS_SPACE = 2 };
+//   AXIS_DCR_ROUNDTRIP: the same with the real modulus DataConstraint (A, data_mode);
+//   AXIS_T2_PROLOGUE: the pass's input is t2' = a2*x + b2*SpaceConstraint(t2)
+//     (data holds t2; x = x_in, S = aux), the difference map's second half;
+//   AXIS_T1_EPILOGUE: the output w becomes SpaceConstraint(a1*x + b1*w) (x = x_in);
+//   AXIS_X_EPILOGUE: the output w is t2; x <- a4*w + b4*(a3*t1 + b3*x) (t1 = t1_in).
+enum AxisOpKind : int {
+    AXIS_PLAIN = 0,
+    AXIS_DC_ROUNDTRIP = 1,
+    AXIS_SPACE = 2,
+    AXIS_DCR_ROUNDTRIP = 3,
+    AXIS_T2_PROLOGUE = 4,
+    AXIS_T1_EPILOGUE = 5,
+    AXIS_X_EPILOGUE = 6
+};
 struct AxisOp {
     int kind = AXIS_PLAIN;
-    const void* aux = nullptr;
+    const void* aux = nullptr;  // C, A or S
     uint64_t aux_plane = 1;
-    int space_mode = 0;
+    int space_mode = 0, data_mode = 0;
+    void* x_in = nullptr;       // x of the difference map
+    const void* t1_in = nullptr;
+    double a = 0.0, b = 0.0, a2 = 0.0, b2 = 0.0;  // merge coefficients (rounded to T by the caller)
 };
 
 template <typename T, int L, int TPL>
@@ -149,11 +165,22 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
     __syncthreads();
 
     const int line = t / TPL, q = t % TPL;
+    // global index of element n of this thread's line, and whether the line exists
+    const bool line_ok = contig ? (o0 + line) < Bo : (i0 + line) < Bi;
+    auto gindex = [&](int n) -> uint64_t {
+        return contig ? (o0 + line) * (uint64_t)L + n : (o0 * L + n) * Bi + i0 + line;
+    };
     Cx<T> v[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int n = q + TPL * k;
         v[k] = buf[line * LSX + n];
+        if (op.kind == AXIS_T2_PROLOGUE && line_ok) {
+            const uint64_t gi = gindex(n);
+            const T sv = static_cast<const T*>(op.aux)[gi % op.aux_plane];
+            v[k] = merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], space_apply(v[k], sv, op.space_mode),
+                               (T)op.a, (T)op.b);
+        }
         if (shift) v[k] = csign(v[k], n);
     }
     Cx<T> o[R];
@@ -161,19 +188,17 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
     else
         F::template natural_to_split_flat<false>(v, o, buf + line * LSX, 1, tw, q);
-    // global index of element n of this thread's line, and whether the line exists
-    const bool line_ok = contig ? (o0 + line) < Bo : (i0 + line) < Bi;
-    auto gindex = [&](int n) -> uint64_t {
-        return contig ? (o0 + line) * (uint64_t)L + n : (o0 * L + n) * Bi + i0 + line;
-    };
-    if (op.kind == AXIS_DC_ROUNDTRIP) {
-        const Cx<T>* __restrict__ C = static_cast<const Cx<T>*>(op.aux);
+    if (op.kind == AXIS_DC_ROUNDTRIP || op.kind == AXIS_DCR_ROUNDTRIP) {
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             const int f = F::pos(q, i);
             Cx<T> w = o[i];
             if (shift) w = csign(w, f + out_neg);
-            if (line_ok) w = data_apply_complex(w, C[gindex(f) % op.aux_plane]);
+            if (line_ok) {
+                const uint64_t ai = gindex(f) % op.aux_plane;
+                w = (op.kind == AXIS_DC_ROUNDTRIP) ? data_apply_complex(w, static_cast<const Cx<T>*>(op.aux)[ai])
+                                                   : data_apply(w, static_cast<const T*>(op.aux)[ai], op.data_mode);
+            }
             if (shift) w = csign(w, f);  // the inverse pass's input flip
             buf[line * LSX + f] = w;
         }
@@ -188,8 +213,20 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         Cx<T> w = o[i];
         if (do_scale) w = cscale(w, scale);
         if (shift) w = csign(w, f + out_neg);
-        if (op.kind == AXIS_SPACE && line_ok)
-            w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
+        if (line_ok) {
+            if (op.kind == AXIS_SPACE) {
+                w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
+            } else if (op.kind == AXIS_T1_EPILOGUE) {
+                const uint64_t gi = gindex(f);
+                w = space_apply(merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], w, (T)op.a, (T)op.b),
+                                static_cast<const T*>(op.aux)[gi % op.aux_plane], op.space_mode);
+            } else if (op.kind == AXIS_X_EPILOGUE) {
+                const uint64_t gi = gindex(f);
+                Cx<T>* X = static_cast<Cx<T>*>(op.x_in);
+                const Cx<T> x1 = merge_apply(static_cast<const Cx<T>*>(op.t1_in)[gi], X[gi], (T)op.a, (T)op.b);
+                X[gi] = merge_apply(w, x1, (T)op.a2, (T)op.b2);
+            }
+        }
         buf[line * LSX + f] = w;
     }
     __syncthreads();
@@ -374,7 +411,70 @@ cudaError_t constraint3d_t(void* x, const void* C, const void* S, uint64_t M, ui
     return cudaSuccess;
 }
 
+// the difference-map iteration (src/CPRA_MKL.cpp:94-110, here with the 3D
+// transforms: src/CONV_MKL.cpp:37-88), `iters` times, as ten axis passes:
+// t1's projection (x, y forward; z forward + modulus + inverse; y inverse; x
+// inverse + merge with x + SpaceConstraint), then t2's (x forward from
+// a2*x + b2*S(t2); y; z; y; x inverse + the merges into x)
+template <typename T>
+cudaError_t dm3d_t(const DmArgs& a, T scale, const void* tw_m, const void* tw_n, const void* tw_l, void* work,
+                   cudaStream_t st) {
+    const uint64_t M = a.M, N = a.N, L = a.L, batch = a.batch, plane = M * N * L;
+    AxisOp dc;
+    dc.kind = AXIS_DCR_ROUNDTRIP;
+    dc.aux = a.A;
+    dc.aux_plane = plane;
+    dc.data_mode = a.data_mode;
+    AxisOp e1;
+    e1.kind = AXIS_T1_EPILOGUE;
+    e1.aux = a.S;
+    e1.aux_plane = plane;
+    e1.space_mode = a.space_mode;
+    e1.x_in = a.x;
+    e1.a = a.c.a1;
+    e1.b = a.c.b1;
+    AxisOp p2;
+    p2.kind = AXIS_T2_PROLOGUE;
+    p2.aux = a.S;
+    p2.aux_plane = plane;
+    p2.space_mode = a.space_mode;
+    p2.x_in = a.x;
+    p2.a = a.c.a2;
+    p2.b = a.c.b2;
+    AxisOp ex;
+    ex.kind = AXIS_X_EPILOGUE;
+    ex.x_in = a.x;
+    ex.t1_in = a.t1;
+    ex.a = a.c.a3;
+    ex.b = a.c.b3;
+    ex.a2 = a.c.a4;
+    ex.b2 = a.c.b4;
+    cudaError_t e;
+    auto project = [&](void* v, AxisOp first, AxisOp last) -> cudaError_t {
+        cudaError_t r;
+        if ((r = axis_pass<T>(v, work, batch * L * M, N, 1, false, scale, false, tw_n, st, first)) != cudaSuccess)
+            return r;
+        if ((r = axis_pass<T>(v, work, batch * L, M, N, false, scale, false, tw_m, st)) != cudaSuccess) return r;
+        if ((r = axis_pass<T>(v, work, batch, L, M * N, false, scale, false, tw_l, st, dc)) != cudaSuccess) return r;
+        if ((r = axis_pass<T>(v, work, batch * L, M, N, true, scale, false, tw_m, st)) != cudaSuccess) return r;
+        return axis_pass<T>(v, work, batch * L * M, N, 1, true, scale, true, tw_n, st, last);
+    };
+    for (int it = 0; it < a.iters; ++it) {
+        if ((e = project(a.t1, AxisOp{}, e1)) != cudaSuccess) return e;
+        if ((e = project(a.t2, p2, ex)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
+
+cudaError_t launch_dm3d_iterations(bool dbl, const DmArgs& a, double scale, const void* tw_m, const void* tw_n,
+                                   const void* tw_l, void* work, cudaStream_t st) {
+    if (!constraint3d_fused_supported(a.M, a.N, a.L)) return cudaErrorInvalidValue;
+    if (a.batch == 0 || a.iters <= 0) return cudaSuccess;
+    return dbl ? dm3d_t<double>(a, scale, tw_m, tw_n, tw_l, work, st)
+               : dm3d_t<float>(a, (float)scale, tw_m, tw_n, tw_l, work, st);
+}
 
 bool constraint3d_fused_supported(uint64_t M, uint64_t N, uint64_t L) {
     auto p2 = [](uint64_t v) { return v >= 2 && (v & (v - 1)) == 0 && v <= 1024; };

@@ -879,3 +879,62 @@ def test_constraint3d_equals_operator_calls(tb, T, M, N, L, B, mode):
             o.Backward3D(xo)
             o.SpaceConstraint(xo, S, B * vol, B)
         assert O.rel_l2(outs[1], xo) < (1e-5 if T == np.float32 else 1e-12)
+
+
+# ---- the conventional 3D difference map (src/CONV_MKL.cpp:37-88) through the recorder ------
+def dm3d_per_call(impl, x, t1, t2, A, S, num, B, beta):
+    """src/CONV_MKL.cpp:47-61, one interface call at a time."""
+    b = float(np.float32(beta)) if x.dtype == __import__("torch").complex64 else float(beta)
+    impl.Forward3D(t1)
+    impl.DataConstraint(t1, A, num, B)
+    impl.Backward3D(t1)
+    impl.MergeAddData(x, t1, -1.0 / b, 1.0 + 1.0 / b, num)
+    impl.SpaceConstraint(t1, S, num, B)
+    impl.SpaceConstraint(t2, S, num, B)
+    impl.MergeAddData(x, t2, 1.0 / b, 1.0 - 1.0 / b, num)
+    impl.Forward3D(t2)
+    impl.DataConstraint(t2, A, num, B)
+    impl.Backward3D(t2)
+    impl.MergeAddData(t1, x, b, 1.0, num)
+    impl.MergeAddData(t2, x, -1.0 * b, 1.0, num)
+
+
+@pytest.mark.parametrize("T,M,N,L,B,iters", [(np.float32, 16, 16, 16, 1, 3), (np.float32, 32, 16, 8, 2, 2),
+                                             (np.float64, 16, 16, 16, 1, 2), (np.float32, 12, 12, 12, 1, 2)])
+def test_dm3d_recorder_equals_per_call(tb, T, M, N, L, B, iters):
+    """The 12-call iteration with the 3D transforms, issued one call at a time,
+    runs as ten fused axis passes per iteration (power-of-two sizes) and
+    writes the same bits as with fusion off; other sizes run per call."""
+    torch, cb = tb
+    rng = np.random.default_rng(M * N * L + B)
+    vol = M * N * L
+    num = vol * B
+    cdt = np.complex64 if T == np.float32 else np.complex128
+    amps = (rng.uniform(0, 40, vol) * (rng.uniform(0, 1, vol) > 0.1)).astype(T)
+    sup = (rng.uniform(0, 1, vol) > 0.5).astype(T)
+    x0 = (rng.uniform(0, 1, num) + 1j * rng.uniform(0, 1, num)).astype(cdt)
+    dtype = "float32" if T == np.float32 else "float64"
+    outs = []
+    for fusion in (0, 1):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
+        impl.set_option(cb.OPT_FUSION, fusion)
+        x, t1, t2 = (dev(torch, x0) for _ in range(3))
+        A, S = dev(torch, amps), dev(torch, sup)
+        for _ in range(iters):
+            dm3d_per_call(impl, x, t1, t2, A, S, num, B, 0.9)
+        assert impl.Sync()
+        outs.append([host(v) for v in (x, t1, t2)])
+    for a, b in zip(outs[0], outs[1]):
+        np.testing.assert_array_equal(a, b)
+    o = O.OracleImpl(T, M, N, L, B)
+    xo, t1o, t2o = x0.copy(), x0.copy(), x0.copy()
+    bb = float(np.float32(0.9)) if T == np.float32 else 0.9
+    for _ in range(iters):
+        o.Forward3D(t1o); o.DataConstraint(t1o, amps, num, B); o.Backward3D(t1o)
+        o.MergeAddData(xo, t1o, -1.0 / bb, 1.0 + 1.0 / bb, num); o.SpaceConstraint(t1o, sup, num, B)
+        o.SpaceConstraint(t2o, sup, num, B); o.MergeAddData(xo, t2o, 1.0 / bb, 1.0 - 1.0 / bb, num)
+        o.Forward3D(t2o); o.DataConstraint(t2o, amps, num, B); o.Backward3D(t2o)
+        o.MergeAddData(t1o, xo, bb, 1.0, num); o.MergeAddData(t2o, xo, -1.0 * bb, 1.0, num)
+    tol = (FP32_DM_TOL if T == np.float32 else 1e-12) * iters
+    for got, want in zip(outs[1], (xo, t1o, t2o)):
+        assert O.rel_l2(got, want) < tol
