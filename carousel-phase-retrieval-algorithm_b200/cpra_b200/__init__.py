@@ -83,6 +83,8 @@ _SIGS = {
                                 C.c_void_p, C.c_uint64, C.c_uint64, C.c_double, C.c_int],
     "cpra_b200_cpra_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                            C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
+    "cpra_b200_cpra_run_host": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
+                                C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -286,6 +288,14 @@ class B200Impl:
                                                int(iters), int(pre_iter), float(beta), 1 if final_step else 0,
                                                _host_addr(err) if err is not None else 0), "cpra_run")
 
+    def cpra_run_host(self, x, A, S, P, batch, epi, iters, pre_iter, beta, final_step=True, err=None) -> bool:
+        """``cpra_run`` on host arrays (numpy or CPU tensors; pinned ones let the
+        per-angle copies overlap the computation); ``x`` is overwritten."""
+        return _check(lib().cpra_b200_cpra_run_host(self._h, _host_addr(x), _host_addr(A), _host_addr(S), int(P),
+                                                    int(batch), int(epi), int(iters), int(pre_iter), float(beta),
+                                                    1 if final_step else 0,
+                                                    _host_addr(err) if err is not None else 0), "cpra_run_host")
+
     def hio_shrinkwrap(self, x, A, S, batch, iters, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5,
                        threshold=0.1, positivity=False, a_stride=None, s_stride=None, estimate=None) -> bool:
         """Fused HIO iterations with shrinkwrap support updates (project-defined);
@@ -390,7 +400,7 @@ def _host_addr(a) -> int:
         return a.ctypes.data
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
-    raise TypeError("ConvergeError needs a host buffer")
+    raise TypeError("a host buffer (numpy array, CPU tensor or address) is required")
 
 
 def NewCpraImpl(impl_type, m, n, l, batch_size, dtype: str = "float32") -> B200Impl:

@@ -25,6 +25,7 @@
 #include <tuple>
 #include <mutex>
 #include <string>
+#include <functional>
 #include <vector>
 
 using namespace cpra_b200;
@@ -184,6 +185,15 @@ struct cpra_b200_ctx {
     uint64_t refine_bytes = 0;
     void* best_sums = nullptr;
     uint64_t best_bytes = 0;
+    // cpra_b200_cpra_run_host: device copies of x, A, S, the copy stream and events
+    void* hx = nullptr;
+    uint64_t hx_bytes = 0;
+    void* hA = nullptr;
+    uint64_t hA_bytes = 0;
+    void* hS = nullptr;
+    uint64_t hS_bytes = 0;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> run_events;
     // slices sorted by direction for the gathers over slices (angle_table.cuh)
     void* atab = nullptr;
     uint64_t atab_bytes = 0;
@@ -642,6 +652,12 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     if (c->refine_buf) cudaFree(c->refine_buf);
     if (c->best_sums) cudaFree(c->best_sums);
     if (c->atab) cudaFree(c->atab);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    if (c->hx) cudaFree(c->hx);
+    if (c->hA) cudaFree(c->hA);
+    if (c->hS) cudaFree(c->hS);
+    for (cudaEvent_t e : c->run_events) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->err_sums) cudaFree(c->err_sums);
     if (c->host_err) cudaFreeHost(c->host_err);
     for (auto& pr : c->timed) {
@@ -1447,9 +1463,16 @@ int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, ui
     return CPRA_B200_OK;
 }
 
-int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
-                       int iters, int pre_iter, double beta, int final_step, void* err_host) {
-    CTX_OR_RETURN(c);
+// The carousel driver on device buffers.  ready (optional, P events): angle
+// p's plane of x is complete once ready[p] has fired; the first episode (and
+// the pre-iterations) wait for each plane they read, just before its first
+// use.  done (optional, P events): recorded after angle p's final projection.
+// after_enqueue (optional) runs once all the work is enqueued, before the
+// wait for the error sums.
+static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
+                         int iters, int pre_iter, double beta, int final_step, void* err_host,
+                         const cudaEvent_t* ready, const cudaEvent_t* done,
+                         const std::function<int()>& after_enqueue = {}) {
     if (!x || !A || !S) return fail(CPRA_B200_EARG, "cpra_run: null pointer");
     if (P < 2) return fail(CPRA_B200_EARG, "cpra_run: P >= 2 (the carousel mix reads angles p-1 and p+1)");
     if (batch != c->batch) return fail(CPRA_B200_EARG, "cpra_run: batch must equal the context's batch_size");
@@ -1528,69 +1551,96 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
     };
     auto enqueue = [&]() -> int {
     int r = CPRA_B200_OK;
+    auto await = [&](uint64_t p) -> int {
+        if (ready) CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, ready[p < P ? p : P - 1], 0), "cpra_run");
+        return CPRA_B200_OK;
+    };
+    if (ready) {
+        // Step A reads angle 0; angle 0 of the first episode also reads angle 1
+        if ((r = await(0))) return r;
+    }
     // Step A (:35-55): pre-reconstruction of angle 0 with the first constraint planes
     if (pre_iter > 0) {
         CPRA_CHECK_CUDA(copy(t1, xp(0)), "cpra_run");
         CPRA_CHECK_CUDA(copy(t2, xp(0)), "cpra_run");
         if ((r = dm_any(c, pattern(0, 0), pre_iter))) return r;
     }
-    // Step B (:59-124)
-    for (int e = 0; e < epi; ++e) {
-        for (uint64_t p = 0; p < P; ++p) {
-            const DmPattern pat = pattern(p, p);
-            const bool err_here = want_err && e == epi - 1;
-            const bool fused = iters > 0 && dm_fusable(c);
-            if (fused && (!err_here || iters >= 2)) {
-                // carousel mix, t1 = t2 = x and the angle's iterations (all but
-                // the last one on an error-reporting angle) in one launch
-                const int mix = (p == 0) ? MIX_FIRST : (p == P - 1) ? MIX_LAST : MIX_MIDDLE;
-                if ((r = launch_fused(c, pat, err_here ? iters - 1 : iters, mix, p > 0 ? xp(p - 1) : nullptr,
-                                      p + 1 < P ? xp(p + 1) : nullptr, 1)))
-                    return r;
-                if (!err_here) continue;
+    // one angle of an episode (src/CPRA_MKL.cpp:63-123)
+    auto run_angle = [&](int e, uint64_t p) -> int {
+        int r = CPRA_B200_OK;
+        const DmPattern pat = pattern(p, p);
+        const bool err_here = want_err && e == epi - 1;
+        const bool fused = iters > 0 && dm_fusable(c);
+        if (fused && (!err_here || iters >= 2)) {
+            // carousel mix, t1 = t2 = x and the angle's iterations (all but
+            // the last one on an error-reporting angle) in one launch
+            const int mix = (p == 0) ? MIX_FIRST : (p == P - 1) ? MIX_LAST : MIX_MIDDLE;
+            if ((r = launch_fused(c, pat, err_here ? iters - 1 : iters, mix, p > 0 ? xp(p - 1) : nullptr,
+                                  p + 1 < P ? xp(p + 1) : nullptr, 1)))
+                return r;
+            if (!err_here) return CPRA_B200_OK;
+        } else {
+            if (p == P - 1) {
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
+            } else if (p == 0) {
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
             } else {
-                if (p == P - 1) {
-                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
-                } else if (p == 0) {
-                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 0.5, MNB, c->stream), "cpra_run");
-                } else {
-                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.0, MNB, c->stream), "cpra_run");
-                    CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 1.0, MNB, c->stream), "cpra_run");
-                }
-                CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
-                CPRA_CHECK_CUDA(copy(t2, xp(p)), "cpra_run");
-                if (!err_here) {
-                    if ((r = dm_any(c, pat, iters))) return r;
-                    continue;
-                }
-                if ((r = dm_any(c, pat, iters - 1))) return r;
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p - 1), xp(p), 0.5, 0.0, MNB, c->stream), "cpra_run");
+                CPRA_CHECK_CUDA(launch_merge_add(c->dbl, xp(p + 1), xp(p), 0.5, 1.0, MNB, c->stream), "cpra_run");
             }
-            CPRA_CHECK_CUDA(copy(old, xp(p)), "cpra_run");
-            if ((r = dm_any(c, pat, 1))) return r;
             CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
-            if ((r = run_fft2d(c, old, false))) return r;
-            if ((r = run_fft2d(c, t1, false))) return r;
-            // ConvergeError (CUDA_Impl.inl:145-172): old <- t1 - old, ||old_i|| / ||t1_i||
-            CPRA_CHECK_CUDA(launch_merge_add(c->dbl, t1, old, 1.0, -1.0, MNB, c->stream), "cpra_run");
-            CPRA_CHECK_CUDA(launch_norm_pairs(c->dbl, old, t1, MN, MN, batch, c->partials, c->err_sums + 2 * batch * p,
-                                              c->stream),
-                            "cpra_run");
+            CPRA_CHECK_CUDA(copy(t2, xp(p)), "cpra_run");
+            if (!err_here) {
+                if ((r = dm_any(c, pat, iters))) return r;
+                return CPRA_B200_OK;
+            }
+            if ((r = dm_any(c, pat, iters - 1))) return r;
         }
-    }
-    // final projection (:126-140)
-    if (final_step) {
+        CPRA_CHECK_CUDA(copy(old, xp(p)), "cpra_run");
+        if ((r = dm_any(c, pat, 1))) return r;
+        CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+        if ((r = run_fft2d(c, old, false))) return r;
+        if ((r = run_fft2d(c, t1, false))) return r;
+        // ConvergeError (CUDA_Impl.inl:145-172): old <- t1 - old, ||old_i|| / ||t1_i||
+        CPRA_CHECK_CUDA(launch_merge_add(c->dbl, t1, old, 1.0, -1.0, MNB, c->stream), "cpra_run");
+        CPRA_CHECK_CUDA(launch_norm_pairs(c->dbl, old, t1, MN, MN, batch, c->partials, c->err_sums + 2 * batch * p,
+                                          c->stream),
+                        "cpra_run");
+        return CPRA_B200_OK;
+    };
+    // final projection of one angle (:126-140)
+    auto final_projection = [&](uint64_t p) -> int {
+        int r = CPRA_B200_OK;
+        const DmPattern pat = pattern(p, p);
+        CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
+        const Op seq[5] = {{OpKind::Fwd2D, t1, nullptr, 0, 0, 0, 0},
+                           {OpKind::DataReal, t1, pat.A, MNB, batch, 0, 0},
+                           {OpKind::Bwd2D, t1, nullptr, 0, 0, 0, 0},
+                           {OpKind::Merge, t1, xp(p), MNB, 1, coef.a1, coef.b1},
+                           {OpKind::Space, t1, pat.S, MNB, batch, 0, 0}};
+        for (const Op& op : seq)
+            if ((r = exec_op(c, op))) return r;
+        CPRA_CHECK_CUDA(copy(xp(p), t1), "cpra_run");
+        if (done) CPRA_CHECK_CUDA(cudaEventRecord(done[p], c->stream), "cpra_run");
+        return CPRA_B200_OK;
+    };
+    // Step B (:59-124).  The final projection of angle p depends on x[p] alone
+    // and nothing of the last episode reads x[p] after angle p + 1 has run, so
+    // it is issued right there: the same operations on the same data as after
+    // the loop (:126-140), with each angle's result complete early.
+    for (int e = 0; e < epi; ++e) {
+        const bool last = final_step && e == epi - 1;
         for (uint64_t p = 0; p < P; ++p) {
-            const DmPattern pat = pattern(p, p);
-            CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
-            const Op seq[5] = {{OpKind::Fwd2D, t1, nullptr, 0, 0, 0, 0},
-                               {OpKind::DataReal, t1, pat.A, MNB, batch, 0, 0},
-                               {OpKind::Bwd2D, t1, nullptr, 0, 0, 0, 0},
-                               {OpKind::Merge, t1, xp(p), MNB, 1, coef.a1, coef.b1},
-                               {OpKind::Space, t1, pat.S, MNB, batch, 0, 0}};
-            for (const Op& op : seq)
-                if ((r = exec_op(c, op))) return r;
-            CPRA_CHECK_CUDA(copy(xp(p), t1), "cpra_run");
+            if (e == 0 && (r = await(p + 1))) return r;
+            if ((r = run_angle(e, p))) return r;
+            if (last && p > 0 && (r = final_projection(p - 1))) return r;
         }
+        if (last && (r = final_projection(P - 1))) return r;
+    }
+    if (final_step && epi == 0) {
+        if ((r = await(P - 1))) return r;
+        for (uint64_t p = 0; p < P; ++p)
+            if ((r = final_projection(p))) return r;
     }
     if (want_err)
         CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_err, c->err_sums, sizeof(double) * 2 * P * batch,
@@ -1598,11 +1648,13 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
                         "cpra_run");
     return CPRA_B200_OK;
     };
-    r = run_maybe_graph(c,
-                        graph_key("cpra_run", x, A, S, P, batch, epi, iters, pre_iter, b, final_step, want_err,
-                                  c->space_mode, c->data_mode, c->fusion),
-                        enqueue);
+    r = (ready || done) ? enqueue()
+                        : run_maybe_graph(c,
+                                          graph_key("cpra_run", x, A, S, P, batch, epi, iters, pre_iter, b,
+                                                    final_step, want_err, c->space_mode, c->data_mode, c->fusion),
+                                          enqueue);
     if (r) return r;
+    if (after_enqueue && (r = after_enqueue())) return r;
     if (want_err) {
         CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "cpra_run");
         for (uint64_t i = 0; i < P * batch; ++i) {
@@ -1613,6 +1665,75 @@ int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, 
                 static_cast<float*>(err_host)[i] = (float)v;
         }
     }
+    return CPRA_B200_OK;
+}
+
+
+int cpra_b200_cpra_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
+                       int iters, int pre_iter, double beta, int final_step, void* err_host) {
+    CTX_OR_RETURN(c);
+    return cpra_run_impl(c, x, A, S, P, batch, epi, iters, pre_iter, beta, final_step, err_host, nullptr, nullptr);
+}
+
+int cpra_b200_cpra_run_host(cpra_b200_ctx* c, void* x_host, const void* A_host, const void* S_host, uint64_t P,
+                            uint64_t batch, int epi, int iters, int pre_iter, double beta, int final_step,
+                            void* err_host) {
+    CTX_OR_RETURN(c);
+    if (!x_host || !A_host || !S_host) return fail(CPRA_B200_EARG, "cpra_run_host: null pointer");
+    if (P < 2 || batch != c->batch) return fail(CPRA_B200_EARG, "cpra_run_host: P >= 2 and batch == batch_size");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t cb = c->plane() * batch * c->csize(), rb = c->plane() * c->esize();
+    if ((r = ensure_buffer(c, &c->hx, &c->hx_bytes, P * cb, "cudaMalloc(cpra_run_host x)"))) return r;
+    if ((r = ensure_buffer(c, &c->hA, &c->hA_bytes, P * rb, "cudaMalloc(cpra_run_host A)"))) return r;
+    if ((r = ensure_buffer(c, &c->hS, &c->hS_bytes, P * rb, "cudaMalloc(cpra_run_host S)"))) return r;
+    if (!c->copy_stream)
+        CPRA_CHECK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    while (c->run_events.size() < 2 * P + 1) {
+        cudaEvent_t e;
+        CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        c->run_events.push_back(e);
+    }
+    const cudaEvent_t* ready = c->run_events.data();
+    const cudaEvent_t* done = ready + P;
+    const cudaEvent_t start = ready[2 * P];
+    char* hx = static_cast<char*>(c->hx);
+    char* xh = static_cast<char*>(x_host);
+    // uploads on the copy stream once the context's earlier work is done, angle
+    // by angle (x, A and S of angle p, then ready[p]); the driver waits for
+    // angle p + 1 before it runs angle p of the first episode
+    CPRA_CHECK_CUDA(cudaEventRecord(start, c->stream), "cpra_run_host");
+    CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, start, 0), "cpra_run_host");
+    for (uint64_t p = 0; p < P; ++p) {
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(hx + p * cb, xh + p * cb, cb, cudaMemcpyHostToDevice, c->copy_stream),
+                        "cpra_run_host");
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(static_cast<char*>(c->hA) + p * rb, static_cast<const char*>(A_host) + p * rb,
+                                        rb, cudaMemcpyHostToDevice, c->copy_stream),
+                        "cpra_run_host");
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(static_cast<char*>(c->hS) + p * rb, static_cast<const char*>(S_host) + p * rb,
+                                        rb, cudaMemcpyHostToDevice, c->copy_stream),
+                        "cpra_run_host");
+        CPRA_CHECK_CUDA(cudaEventRecord(ready[p], c->copy_stream), "cpra_run_host");
+    }
+    // downloads: angle p as soon as its final projection is done (all at the
+    // end without the final projection)
+    auto download = [&]() -> int {
+        for (uint64_t p = 0; p < P; ++p) {
+            if (final_step || p == 0) {
+                if (!final_step) CPRA_CHECK_CUDA(cudaEventRecord(done[0], c->stream), "cpra_run_host");
+                CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, done[final_step ? p : 0], 0), "cpra_run_host");
+            }
+            CPRA_CHECK_CUDA(cudaMemcpyAsync(xh + p * cb, hx + p * cb, cb, cudaMemcpyDeviceToHost, c->copy_stream),
+                            "cpra_run_host");
+        }
+        return CPRA_B200_OK;
+    };
+    r = cpra_run_impl(c, c->hx, c->hA, c->hS, P, batch, epi, iters, pre_iter, beta, final_step, err_host, ready,
+                      final_step ? done : nullptr, download);
+    const cudaError_t e = cudaStreamSynchronize(c->copy_stream);
+    if (r) return r;
+    CPRA_CHECK_CUDA(e, "cpra_run_host");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "cpra_run_host");
     return CPRA_B200_OK;
 }
 

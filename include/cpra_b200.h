@@ -148,6 +148,20 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* ctx, void* x, void* t1, void* t2, con
 int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S, uint64_t P, uint64_t batch,
                        int epi, int iters, int pre_iter, double beta, int final_step, void* err_host);
 
+/* Extension: cpra_b200_cpra_run on HOST buffers (x, A, S laid out as above),
+ * the whole ShrinkWrap_CPRA_MKL_Sample call of src/CPRA_MKL.cpp:35-140 with
+ * its data in host memory, as the reference's caller holds it.  Angle p's
+ * planes are uploaded on a context-owned copy stream and the first episode
+ * waits for angle p+1 only before it runs angle p; with the final projection,
+ * angle p's result is read back as soon as its projection is done.  x_host is
+ * overwritten with the result.  Pinned host buffers make the copies overlap
+ * the computation (pageable ones work, without overlap).  The device copies of
+ * x, A and S are context-owned.  Synchronous; results are bit-identical to
+ * cpra_b200_cpra_run on the same data. */
+int cpra_b200_cpra_run_host(cpra_b200_ctx* ctx, void* x_host, const void* A_host, const void* S_host, uint64_t P,
+                            uint64_t batch, int epi, int iters, int pre_iter, double beta, int final_step,
+                            void* err_host);
+
 /* Extension (project-defined, no counterpart in the reference): R-factor of
  * `batch` patterns x ([batch][m][n], the context's plane size) against their
  * modulus planes A (pattern b uses A + b*a_stride; 0: one shared plane):

@@ -494,6 +494,43 @@ def test_cpra_run_vs_reference(tb):
     assert not impl.cpra_run(x, dev(torch, G["cpra_A"]), dev(torch, G["cpra_S"]), P, B + 1, epi, it, pre, 0.9)
 
 
+@pytest.mark.parametrize("L,P,B,epi,it,pre,final,pinned,dtype",
+                         [(64, 4, 2, 2, 3, 1, True, True, "float32"), (128, 5, 3, 1, 2, 0, True, False, "float32"),
+                          (256, 3, 2, 2, 2, 1, False, True, "float32"), (32, 3, 2, 0, 2, 2, True, True, "float32"),
+                          (32, 4, 2, 2, 2, 1, True, True, "float64")])
+def test_cpra_run_host_bitwise(tb, L, P, B, epi, it, pre, final, pinned, dtype):
+    """cpra_b200_cpra_run_host (per-angle uploads overlapped with the first
+    episode, per-angle read-back after the final projection) writes the same
+    bits and the same errors as cpra_b200_cpra_run on device buffers, twice in
+    a row on one context, from pinned or pageable host memory."""
+    torch, cb = tb
+    rdt, cdt = (np.float32, np.complex64) if dtype == "float32" else (np.float64, np.complex128)
+    rng = np.random.default_rng(L + 11 * P + epi)
+    A = (rng.uniform(0, 30, (P, L * L)) * (rng.uniform(0, 1, (P, L * L)) > 0.1)).astype(rdt)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(rdt)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(cdt)
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B, dtype)
+    xr = dev(torch, x0)
+    err_r = np.zeros(P * B, rdt)
+    assert ref.cpra_run(xr, dev(torch, A.ravel()), dev(torch, S.ravel()), P, B, epi, it, pre, 0.9,
+                        final_step=final, err=err_r if epi else None) and ref.Sync()
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B, dtype)
+
+    def hbuf(a):
+        t = torch.from_numpy(np.ascontiguousarray(a).view(rdt).copy())
+        return t.pin_memory() if pinned else t
+
+    Ah, Sh = hbuf(A.ravel()), hbuf(S.ravel())
+    for _ in range(2):
+        xh = hbuf(x0)
+        err = np.zeros(P * B, rdt)
+        assert impl.cpra_run_host(xh, Ah, Sh, P, B, epi, it, pre, 0.9, final_step=final, err=err if epi else None)
+        np.testing.assert_array_equal(xh.numpy().view(cdt), host(xr))
+        np.testing.assert_array_equal(err, err_r)
+    assert not impl.cpra_run_host(hbuf(x0), Ah, Sh, 1, B, epi, it, pre, 0.9)
+    assert not impl.cpra_run_host(hbuf(x0), Ah, Sh, P, B + 1, epi, it, pre, 0.9)
+
+
 def _drop_in_binaries():
     from conftest import REPO
     d = REPO / "tests" / "cpp" / "_bin"
