@@ -26,7 +26,8 @@ __all__ = [
 
 OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
 F32, F64 = 0, 1
-OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_CHUNK, OPT_GRAPH = 1, 2, 3, 4, 5, 6, 7
+OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_CHUNK, OPT_GRAPH, OPT_LANES = \
+    1, 2, 3, 4, 5, 6, 7, 8
 
 _HERE = Path(__file__).resolve().parent
 
@@ -59,6 +60,7 @@ _SIGS = {
     "cpra_b200_create": [C.POINTER(C.c_void_p), C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64],
     "cpra_b200_destroy": [C.c_void_p],
     "cpra_b200_set_option": [C.c_void_p, C.c_int, C.c_int64],
+    "cpra_b200_get_option": [C.c_void_p, C.c_int, C.POINTER(C.c_int64)],
     "cpra_b200_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
     "cpra_b200_alloc": [C.c_void_p, C.POINTER(C.c_void_p), C.c_uint64, C.c_int],
     "cpra_b200_free": [C.c_void_p, C.c_void_p],
@@ -197,6 +199,11 @@ class B200Impl:
 
     def set_option(self, option: int, value: int) -> bool:
         return _check(lib().cpra_b200_set_option(self._h, option, int(value)), "set_option")
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        _check(lib().cpra_b200_get_option(self._h, option, C.byref(v)), "get_option")
+        return v.value
 
     def stream(self) -> int:
         s = C.c_void_p()

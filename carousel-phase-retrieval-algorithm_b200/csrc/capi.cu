@@ -140,6 +140,20 @@ struct BucketLane {
     uint64_t scratch_bytes = 0;
 };
 
+// A stream of the carousel driver's wavefront schedule with its own t1, t2,
+// old (drv, 3 planes of the batch) and work scratch; ev[p] marks angle p of
+// the lane's latest episode done.  Lane 0 is the context's own stream and
+// buffers.
+struct RunLane {
+    cudaStream_t stream = nullptr;
+    void* drv = nullptr;
+    uint64_t drv_bytes = 0;
+    void* work = nullptr;
+    uint64_t work_bytes = 0;
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t join = nullptr;
+};
+
 struct cpra_b200_ctx {
     bool dbl = false;
     uint64_t m = 1, n = 1, l = 1, batch = 1;
@@ -185,6 +199,10 @@ struct cpra_b200_ctx {
     uint64_t refine_bytes = 0;
     void* best_sums = nullptr;
     uint64_t best_bytes = 0;
+    // cpra_b200_cpra_run's lanes (CPRA_B200_OPT_LANES: 0 automatic)
+    std::vector<RunLane> run_lanes;
+    cudaEvent_t lane_fork = nullptr;
+    int lanes_opt = 0;
     // cpra_b200_cpra_run_host: device copies of x, A, S, the copy stream and events
     void* hx = nullptr;
     uint64_t hx_bytes = 0;
@@ -652,6 +670,15 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     if (c->refine_buf) cudaFree(c->refine_buf);
     if (c->best_sums) cudaFree(c->best_sums);
     if (c->atab) cudaFree(c->atab);
+    for (RunLane& lane : c->run_lanes) {
+        if (lane.stream) cudaStreamSynchronize(lane.stream);
+        if (lane.drv) cudaFree(lane.drv);
+        if (lane.work) cudaFree(lane.work);
+        for (cudaEvent_t e : lane.ev) cudaEventDestroy(e);
+        if (lane.join) cudaEventDestroy(lane.join);
+        if (lane.stream) cudaStreamDestroy(lane.stream);
+    }
+    if (c->lane_fork) cudaEventDestroy(c->lane_fork);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->hx) cudaFree(c->hx);
     if (c->hA) cudaFree(c->hA);
@@ -696,6 +723,10 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
         case CPRA_B200_OPT_HIO_CHUNK:
             if (value < 0) return fail(CPRA_B200_EARG, "hio chunk must be >= 0");
             c->hio_chunk = (uint64_t)value;
+            break;
+        case CPRA_B200_OPT_LANES:
+            if (value < 0 || value > CPRA_B200_MAX_LANES) return fail(CPRA_B200_EARG, "lanes must be 0..16");
+            c->lanes_opt = (int)value;
             break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
@@ -1463,6 +1494,69 @@ int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, ui
     return CPRA_B200_OK;
 }
 
+// Lanes of cpra_run's wavefront schedule: with CPRA_B200_OPT_LANES 0, as many
+// as it takes for the angles running side by side to fill the GPU's resident
+// CTA slots once (one lane when one angle's launch already does).
+int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
+    if (c->lanes_opt > 0) return c->lanes_opt;
+    if (!c->fusion || !dm_fusable(c)) return 1;
+    uint64_t ctas, per_sm;
+    if (dm_fused_supported(c->dbl, c->m, c->n)) {
+        ctas = batch;
+        per_sm = (uint64_t)dm_fused_ctas_per_sm(c->m);
+    } else {
+        ctas = dm_large_row_ctas(c->m, batch);
+        per_sm = (uint64_t)dm_large_ctas_per_sm(c->m);
+    }
+    const uint64_t slots = per_sm * (uint64_t)sm_count();
+    if (ctas == 0 || ctas >= slots) return 1;
+    return (int)std::min<uint64_t>(8, (slots + ctas - 1) / ctas);
+}
+
+int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
+    CTX_OR_RETURN(c);
+    if (!value) return fail(CPRA_B200_EARG, "get_option: null value");
+    switch (option) {
+        case CPRA_B200_OPT_FUSION: *value = c->fusion ? 1 : 0; break;
+        case CPRA_B200_OPT_SPACE_MODE: *value = c->space_mode; break;
+        case CPRA_B200_OPT_DATA_MODE: *value = c->data_mode; break;
+        case CPRA_B200_OPT_SEED: *value = (int64_t)c->seed; break;
+        case CPRA_B200_OPT_KERNEL_TIMING: *value = c->timing ? 1 : 0; break;
+        case CPRA_B200_OPT_HIO_CHUNK: *value = (int64_t)c->hio_chunk; break;
+        case CPRA_B200_OPT_GRAPH: *value = c->graphs ? 1 : 0; break;
+        case CPRA_B200_OPT_LANES: *value = run_lanes_for(c, c->batch); break;
+        default: return fail(CPRA_B200_EARG, "unknown option");
+    }
+    return CPRA_B200_OK;
+}
+
+// lanes 1..W-1 with their streams, scratch and per-angle events (lane 0 is the
+// context's own stream and buffers)
+int ensure_lanes(cpra_b200_ctx* c, int W, uint64_t drv_bytes, uint64_t work_bytes, uint64_t P) {
+    if (W <= 1) return CPRA_B200_OK;
+    if (c->run_lanes.size() < (size_t)W) c->run_lanes.resize(W);
+    if (!c->lane_fork)
+        CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming), "cudaEventCreate");
+    for (int k = 0; k < W; ++k) {
+        RunLane& lane = c->run_lanes[k];
+        if (k > 0) {
+            if (!lane.stream)
+                CPRA_CHECK_CUDA(cudaStreamCreateWithFlags(&lane.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            if (!lane.join)
+                CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&lane.join, cudaEventDisableTiming), "cudaEventCreate");
+            int r = ensure_buffer(c, &lane.drv, &lane.drv_bytes, drv_bytes, "cudaMalloc(lane buffers)");
+            if (!r) r = ensure_buffer(c, &lane.work, &lane.work_bytes, work_bytes, "cudaMalloc(lane work)");
+            if (r) return r;
+        }
+        while (lane.ev.size() < P) {
+            cudaEvent_t e;
+            CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+            lane.ev.push_back(e);
+        }
+    }
+    return CPRA_B200_OK;
+}
+
 // The carousel driver on device buffers.  ready (optional, P events): angle
 // p's plane of x is complete once ready[p] has fired; the first episode (and
 // the pre-iterations) wait for each plane they read, just before its first
@@ -1517,16 +1611,15 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     }
     // scratch of the fused large-plane iterations and of non-power-of-two
     // transforms, reserved before any work is enqueued (and before a capture)
-    if (dm_fusable(c) && !dm_fused_supported(c->dbl, c->m, c->n)) {
-        r = ensure_work(c, dm_large_scratch_bytes(c->m, c->n, batch, 0));
-        if (r) return r;
-    }
-    r = ensure_work(c, batch * MN * c->csize());
+    uint64_t work_need = batch * MN * c->csize();
+    if (dm_fusable(c) && !dm_fused_supported(c->dbl, c->m, c->n))
+        work_need = std::max(work_need, dm_large_scratch_bytes(c->m, c->n, batch, 0));
+    r = ensure_work(c, work_need);
     if (r) return r;
+    // lanes of the wavefront schedule, each with its own scratch
+    const int W = std::max(1, std::min(run_lanes_for(c, batch), epi));
+    if ((r = ensure_lanes(c, W, 3 * cb, work_need, P))) return r;
     char* base = static_cast<char*>(x);
-    char* t1 = static_cast<char*>(c->drv);
-    char* t2 = t1 + cb;
-    char* old = t2 + cb;
     const char* Ab = static_cast<const char*>(A);
     const char* Sb = static_cast<const char*>(S);
     const uint64_t rb = MN * c->esize();
@@ -1534,11 +1627,48 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     // src/CPRA_MKL.cpp:98,103,109,110: coefficients in double from a T beta, passed as T
     const DmCoef coef = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
                          c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
-    auto pattern = [&](uint64_t p, uint64_t cp) {
+    // a lane's t1, t2, old and its scope: lane k > 0 runs on its own stream
+    // with its own work buffer (swapped into the context while it is issued)
+    struct LaneBufs {
+        char *t1, *t2, *old;
+    };
+    auto bufs = [&](int k) {
+        char* d = static_cast<char*>(k == 0 ? c->drv : c->run_lanes[k].drv);
+        return LaneBufs{d, d + cb, d + 2 * cb};
+    };
+    struct LaneScope {
+        cpra_b200_ctx* c;
+        RunLane* lane;
+        cudaStream_t stream;
+        void* work;
+        uint64_t work_bytes;
+        LaneScope(cpra_b200_ctx* c_, int k) : c(c_), lane(k ? &c_->run_lanes[k] : nullptr) {
+            stream = c->stream;
+            work = c->work;
+            work_bytes = c->work_bytes;
+            if (lane) {
+                c->stream = lane->stream;
+                c->work = lane->work;
+                c->work_bytes = lane->work_bytes;
+            }
+        }
+        ~LaneScope() {
+            if (lane) {
+                lane->work = c->work;
+                lane->work_bytes = c->work_bytes;
+                c->stream = stream;
+                c->work = work;
+                c->work_bytes = work_bytes;
+            }
+        }
+    };
+    char* t1 = bufs(0).t1;
+    char* t2 = bufs(0).t2;
+    auto pattern = [&](uint64_t p, uint64_t cp, const LaneBufs& lb) {
         DmPattern d;
         d.x = xp(p);
-        d.t1 = t1;
-        d.t2 = t2;
+        d.t1 = lb.t1;
+        d.t2 = lb.t2;
         d.A = Ab + rb * cp;
         d.S = Sb + rb * cp;
         d.num = MNB;
@@ -1563,12 +1693,15 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     if (pre_iter > 0) {
         CPRA_CHECK_CUDA(copy(t1, xp(0)), "cpra_run");
         CPRA_CHECK_CUDA(copy(t2, xp(0)), "cpra_run");
-        if ((r = dm_any(c, pattern(0, 0), pre_iter))) return r;
+        if ((r = dm_any(c, pattern(0, 0, bufs(0)), pre_iter))) return r;
     }
     // one angle of an episode (src/CPRA_MKL.cpp:63-123)
-    auto run_angle = [&](int e, uint64_t p) -> int {
+    auto run_angle = [&](int e, uint64_t p, const LaneBufs& lb) -> int {
         int r = CPRA_B200_OK;
-        const DmPattern pat = pattern(p, p);
+        char* t1 = lb.t1;
+        char* t2 = lb.t2;
+        char* old = lb.old;
+        const DmPattern pat = pattern(p, p, lb);
         const bool err_here = want_err && e == epi - 1;
         const bool fused = iters > 0 && dm_fusable(c);
         if (fused && (!err_here || iters >= 2)) {
@@ -1609,9 +1742,10 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
         return CPRA_B200_OK;
     };
     // final projection of one angle (:126-140)
-    auto final_projection = [&](uint64_t p) -> int {
+    auto final_projection = [&](uint64_t p, const LaneBufs& lb) -> int {
         int r = CPRA_B200_OK;
-        const DmPattern pat = pattern(p, p);
+        char* t1 = lb.t1;
+        const DmPattern pat = pattern(p, p, lb);
         CPRA_CHECK_CUDA(copy(t1, xp(p)), "cpra_run");
         const Op seq[5] = {{OpKind::Fwd2D, t1, nullptr, 0, 0, 0, 0},
                            {OpKind::DataReal, t1, pat.A, MNB, batch, 0, 0},
@@ -1628,19 +1762,55 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     // and nothing of the last episode reads x[p] after angle p + 1 has run, so
     // it is issued right there: the same operations on the same data as after
     // the loop (:126-140), with each angle's result complete early.
-    for (int e = 0; e < epi; ++e) {
-        const bool last = final_step && e == epi - 1;
-        for (uint64_t p = 0; p < P; ++p) {
-            if (e == 0 && (r = await(p + 1))) return r;
-            if ((r = run_angle(e, p))) return r;
-            if (last && p > 0 && (r = final_projection(p - 1))) return r;
+    //
+    // Angle p of episode e reads x[p-1], x[p], x[p+1] and writes x[p]: it
+    // needs angle p-1 of episode e and angle p+1 of episode e-1 done, and
+    // nothing else (every other order constraint follows from those two).
+    // With W > 1 lanes, episode e runs on lane e mod W and the angles are
+    // issued in wavefront order (p + 2e ascending), so angle p of episode e
+    // runs beside angle p-2 of episode e+1; each angle reads exactly the data
+    // it reads in the sequential order, so the results are the same bits.
+    auto issue = [&](int e, uint64_t p) -> int {
+        const int k = e % W;
+        LaneScope scope(c, k);
+        int r = CPRA_B200_OK;
+        if (e == 0 && (r = await(p + 1))) return r;
+        if (W > 1 && e > 0 && p + 1 < P && (e - 1) % W != k)
+            CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, c->run_lanes[(e - 1) % W].ev[p + 1], 0), "cpra_run");
+        const LaneBufs lb = bufs(k);
+        if ((r = run_angle(e, p, lb))) return r;
+        if (W > 1 && e + 1 < epi && p > 0 && (e + 1) % W != k)
+            CPRA_CHECK_CUDA(cudaEventRecord(c->run_lanes[k].ev[p], c->stream), "cpra_run");
+        if (final_step && e == epi - 1) {
+            if (p > 0 && (r = final_projection(p - 1, lb))) return r;
+            if (p == P - 1 && (r = final_projection(P - 1, lb))) return r;
         }
-        if (last && (r = final_projection(P - 1))) return r;
+        return CPRA_B200_OK;
+    };
+    if (W == 1) {
+        for (int e = 0; e < epi; ++e)
+            for (uint64_t p = 0; p < P; ++p)
+                if ((r = issue(e, p))) return r;
+    } else {
+        CPRA_CHECK_CUDA(cudaEventRecord(c->lane_fork, c->stream), "cpra_run");
+        for (int k = 1; k < W; ++k)
+            CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->run_lanes[k].stream, c->lane_fork, 0), "cpra_run");
+        const uint64_t steps = P + 2 * (uint64_t)(epi - 1);
+        for (uint64_t t = 0; t < steps; ++t)
+            for (int e = 0; e < epi; ++e) {
+                if (t < 2 * (uint64_t)e) break;
+                const uint64_t p = t - 2 * (uint64_t)e;
+                if (p < P && (r = issue(e, p))) return r;
+            }
+        for (int k = 1; k < W; ++k) {
+            CPRA_CHECK_CUDA(cudaEventRecord(c->run_lanes[k].join, c->run_lanes[k].stream), "cpra_run");
+            CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, c->run_lanes[k].join, 0), "cpra_run");
+        }
     }
     if (final_step && epi == 0) {
         if ((r = await(P - 1))) return r;
         for (uint64_t p = 0; p < P; ++p)
-            if ((r = final_projection(p))) return r;
+            if ((r = final_projection(p, bufs(0)))) return r;
     }
     if (want_err)
         CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_err, c->err_sums, sizeof(double) * 2 * P * batch,
@@ -1651,7 +1821,7 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     r = (ready || done) ? enqueue()
                         : run_maybe_graph(c,
                                           graph_key("cpra_run", x, A, S, P, batch, epi, iters, pre_iter, b,
-                                                    final_step, want_err, c->space_mode, c->data_mode, c->fusion),
+                                                    final_step, want_err, c->space_mode, c->data_mode, c->fusion, W),
                                           enqueue);
     if (r) return r;
     if (after_enqueue && (r = after_enqueue())) return r;

@@ -118,6 +118,9 @@ struct DmArgs {
 };
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
+// Resident CTAs of one angle's fused launch (k_dm: one per pattern) per SM,
+// and the CTA count of that launch: how much of the GPU one angle fills.
+int dm_fused_ctas_per_sm(uint64_t M);
 // The difference-map iteration with the 3D transforms (src/CONV_MKL.cpp:37-88)
 // on [batch][L][M][N] volumes, A and S one volume each (a_stride, s_stride
 // unused), `iters` times as ten axis passes per iteration; same bits as the
@@ -132,6 +135,9 @@ cudaError_t launch_dm3d_iterations(bool dbl, const DmArgs& a, double scale, cons
 bool dm_large_supported(bool dbl, uint64_t M, uint64_t N, int space_mode);
 uint64_t dm_large_scratch_bytes(uint64_t M, uint64_t N, uint64_t batch, uint64_t s_stride);
 cudaError_t launch_dm_large(const DmArgs& a, const void* tw, void* scratch, cudaStream_t st);
+// the row pass of one angle's large-plane iterations: CTAs per SM and per launch
+int dm_large_ctas_per_sm(uint64_t M);
+uint64_t dm_large_row_ctas(uint64_t M, uint64_t batch);
 
 // ---- central slices and the amplitude-loss adjoints (kernels_adj.cu) --------
 // slices out[p] ([P][N][M]) of the [L][N][M] volume V at angles ang[p]

@@ -249,7 +249,25 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <int L>
+int dm_occupancy() {
+    const size_t smem = DmPlan<L>::smem_bytes();
+    if (cudaFuncSetAttribute(k_dm<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dm<L>, 4 * L, smem) != cudaSuccess || n < 1) return 1;
+    return n;
+}
+
 }  // namespace
+
+int dm_fused_ctas_per_sm(uint64_t M) {
+    switch (M) {
+        case 32: return dm_occupancy<32>();
+        case 64: return dm_occupancy<64>();
+        case 128: return dm_occupancy<128>();
+        default: return 1;
+    }
+}
 
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N) {
     return !dbl && M == N && (M == 32 || M == 64 || M == 128);

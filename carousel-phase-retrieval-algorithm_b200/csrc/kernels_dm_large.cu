@@ -312,6 +312,26 @@ cudaError_t dml_launch(const DmArgs& a, const void* tw, void* Y, uint32_t* mask,
 
 }  // namespace
 
+namespace {
+template <int L>
+int dml_occupancy() {
+    using B = DmLP<L>;
+    if (cudaFuncSetAttribute(k_dml_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::row_smem()) !=
+        cudaSuccess)
+        return 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dml_rows<L>, B::NT, B::row_smem()) != cudaSuccess || n < 1)
+        return 1;
+    return n;
+}
+}  // namespace
+
+int dm_large_ctas_per_sm(uint64_t M) { return M == 256 ? dml_occupancy<256>() : M == 512 ? dml_occupancy<512>() : 1; }
+
+uint64_t dm_large_row_ctas(uint64_t M, uint64_t batch) {
+    return M == 256 ? batch * 256 / DmLP<256>::RL : M == 512 ? batch * 512 / DmLP<512>::RL : batch;
+}
+
 bool dm_large_supported(bool dbl, uint64_t M, uint64_t N, int space_mode) {
     return !dbl && M == N && (M == 256 || M == 512) && space_mode == SPACE_THRESHOLD;
 }

@@ -57,6 +57,12 @@ extern "C" {
                                     CUDA graph per distinct argument set and replay it on repeated calls */
 #define CPRA_B200_OPT_HIO_CHUNK 6  /* patterns per chunk of the 256/512 HIO line passes (bounds their scratch,
                                     12.125 bytes per pixel); 0 (default): the whole batch */
+#define CPRA_B200_OPT_LANES 8      /* streams of cpra_b200_cpra_run's wavefront schedule: angle p of episode e
+                                    runs beside angle p-2 of episode e+1 (it only waits for angle p-1 of its
+                                    episode and angle p+1 of the one before).  0 (default): as many as one
+                                    angle's launch leaves the GPU room for; 1: one stream, angle after angle;
+                                    k <= 16: k streams.  Same results in every case. */
+#define CPRA_B200_MAX_LANES 16
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 
@@ -70,6 +76,10 @@ const char* cpra_b200_last_error(void);
 /* Number of kernels this library has launched in this process (all contexts). */
 uint64_t cpra_b200_kernels_launched(void);
 int cpra_b200_set_option(cpra_b200_ctx* ctx, int option, int64_t value);
+/* Extension: reads an option back.  CPRA_B200_OPT_LANES reads the number of
+ * lanes cpra_b200_cpra_run uses for the context's batch (the automatic choice
+ * resolved; before the episode-count cap). */
+int cpra_b200_get_option(cpra_b200_ctx* ctx, int option, int64_t* value);
 /* The context's stream as a cudaStream_t (for interoperation). */
 int cpra_b200_get_stream(cpra_b200_ctx* ctx, void** stream);
 

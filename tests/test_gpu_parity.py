@@ -531,6 +531,48 @@ def test_cpra_run_host_bitwise(tb, L, P, B, epi, it, pre, final, pinned, dtype):
     assert not impl.cpra_run_host(hbuf(x0), Ah, Sh, P, B + 1, epi, it, pre, 0.9)
 
 
+@pytest.mark.parametrize("L,P,B,epi,it,pre,lanes,final,dtype",
+                         [(64, 7, 2, 3, 2, 1, 2, True, "float32"), (64, 6, 3, 4, 3, 0, 3, False, "float32"),
+                          (32, 5, 2, 5, 2, 1, 0, True, "float32"), (128, 3, 2, 4, 2, 1, 4, True, "float32"),
+                          (256, 5, 2, 3, 2, 1, 2, True, "float32"), (512, 3, 1, 2, 2, 0, 0, True, "float32"),
+                          (32, 4, 2, 3, 2, 1, 2, True, "float64")])
+def test_cpra_run_lanes_bitwise(tb, L, P, B, epi, it, pre, lanes, final, dtype):
+    """cpra_run's wavefront schedule (episode e on lane e mod W, angle p of
+    episode e beside angle p-2 of episode e+1) writes the same bits and the
+    same errors as one stream taking the angles in order: directly, replayed
+    from a CUDA graph, and through the host-buffer entry."""
+    torch, cb = tb
+    rdt, cdt = (np.float32, np.complex64) if dtype == "float32" else (np.float64, np.complex128)
+    rng = np.random.default_rng(L + 3 * P + 17 * epi)
+    A = (rng.uniform(0, 30, (P, L * L)) * (rng.uniform(0, 1, (P, L * L)) > 0.1)).astype(rdt)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(rdt)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(cdt)
+    Ad, Sd = dev(torch, A.ravel()), dev(torch, S.ravel())
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B, dtype)
+    assert ref.set_option(cb.OPT_LANES, 1)
+    xr = dev(torch, x0)
+    err_r = np.zeros(P * B, rdt)
+    assert ref.cpra_run(xr, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=final, err=err_r) and ref.Sync()
+    run = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B, dtype)
+    assert run.set_option(cb.OPT_LANES, lanes)
+    for graph in (0, 1, 1):
+        assert run.set_option(cb.OPT_GRAPH, graph)
+        x = dev(torch, x0)
+        err = np.zeros(P * B, rdt)
+        assert run.cpra_run(x, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=final, err=err) and run.Sync()
+        np.testing.assert_array_equal(host(x), host(xr))
+        np.testing.assert_array_equal(err, err_r)
+    assert run.set_option(cb.OPT_GRAPH, 0)
+    xh = torch.from_numpy(x0.view(rdt).copy()).pin_memory()
+    err = np.zeros(P * B, rdt)
+    assert run.cpra_run_host(xh, torch.from_numpy(A.ravel().copy()).pin_memory(),
+                             torch.from_numpy(S.ravel().copy()).pin_memory(), P, B, epi, it, pre, 0.9,
+                             final_step=final, err=err)
+    np.testing.assert_array_equal(xh.numpy().view(cdt), host(xr))
+    np.testing.assert_array_equal(err, err_r)
+    assert not run.set_option(cb.OPT_LANES, 17)
+
+
 def _drop_in_binaries():
     from conftest import REPO
     d = REPO / "tests" / "cpp" / "_bin"
