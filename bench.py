@@ -629,7 +629,8 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     run2d(1, 2)
     ms_one_lane, kt = run2d(epi, iters, timing=True)
     impl.set_option(cpra_b200.OPT_LANES, 0)
-    lanes = min(impl.get_option(cpra_b200.OPT_LANES), epi)
+    lanes = max(1, min(impl.get_option(cpra_b200.OPT_LANES), epi))
+    lanes = -(-epi // -(-epi // lanes))  # episodes spread evenly over the lanes
     run2d(1, 2)
     ms_direct = run2d(epi, iters)[0]
     impl.set_option(cpra_b200.OPT_GRAPH, 1)

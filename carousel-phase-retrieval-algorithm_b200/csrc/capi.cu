@@ -1496,7 +1496,8 @@ int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, ui
 
 // Lanes of cpra_run's wavefront schedule: with CPRA_B200_OPT_LANES 0, as many
 // as it takes for the angles running side by side to fill the GPU's resident
-// CTA slots once (one lane when one angle's launch already does).
+// CTA slots one and a half times (one lane when one angle's launch already
+// fills them once: then more lanes only compete for L2).
 int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
     if (c->lanes_opt > 0) return c->lanes_opt;
     if (!c->fusion || !dm_fusable(c)) return 1;
@@ -1510,7 +1511,16 @@ int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
     }
     const uint64_t slots = per_sm * (uint64_t)sm_count();
     if (ctas == 0 || ctas >= slots) return 1;
-    return (int)std::min<uint64_t>(8, (slots + ctas - 1) / ctas);
+    return (int)std::min<uint64_t>(CPRA_B200_MAX_LANES, (3 * slots + 2 * ctas - 1) / (2 * ctas));
+}
+
+// Lanes for `epi` episodes: at most `want`, and no more than it takes to give
+// each lane the same number of episodes as the busiest one has (a lane takes
+// its episodes one after another, so the busiest lane sets the time).
+int balanced_lanes(int want, int epi) {
+    const int w = std::max(1, std::min(want, epi));
+    const int per_lane = (epi + w - 1) / w;
+    return std::max(1, (epi + per_lane - 1) / per_lane);
 }
 
 int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
@@ -1617,7 +1627,7 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     r = ensure_work(c, work_need);
     if (r) return r;
     // lanes of the wavefront schedule, each with its own scratch
-    const int W = std::max(1, std::min(run_lanes_for(c, batch), epi));
+    const int W = balanced_lanes(run_lanes_for(c, batch), epi);
     if ((r = ensure_lanes(c, W, 3 * cb, work_need, P))) return r;
     char* base = static_cast<char*>(x);
     const char* Ab = static_cast<const char*>(A);

@@ -59,9 +59,12 @@ extern "C" {
                                     12.125 bytes per pixel); 0 (default): the whole batch */
 #define CPRA_B200_OPT_LANES 8      /* streams of cpra_b200_cpra_run's wavefront schedule: angle p of episode e
                                     runs beside angle p-2 of episode e+1 (it only waits for angle p-1 of its
-                                    episode and angle p+1 of the one before).  0 (default): as many as one
-                                    angle's launch leaves the GPU room for; 1: one stream, angle after angle;
-                                    k <= 16: k streams.  Same results in every case. */
+                                    episode and angle p+1 of the one before).  0 (default): enough to fill
+                                    the GPU's resident CTA slots 1.5 times when one angle's launch fills less
+                                    than all of them, else 1; 1: one stream, angle after angle; k <= 16: at
+                                    most k streams.  Episodes are spread evenly (no more lanes than it takes
+                                    to give each the busiest lane's episode count).  Same results in every
+                                    case. */
 #define CPRA_B200_MAX_LANES 16
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
