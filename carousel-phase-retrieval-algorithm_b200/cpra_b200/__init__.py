@@ -28,6 +28,7 @@ OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
 F32, F64 = 0, 1
 OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_CHUNK, OPT_GRAPH, OPT_LANES = \
     1, 2, 3, 4, 5, 6, 7, 8
+OPT_IO_CHUNK = 9
 
 _HERE = Path(__file__).resolve().parent
 
@@ -87,6 +88,12 @@ _SIGS = {
                            C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
     "cpra_b200_cpra_run_host": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                                 C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p],
+    "cpra_b200_read_matrix": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_uint64],
+    "cpra_b200_write_matrix": [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_uint64],
+    "cpra_b200_write_starts": [C.c_void_p, C.c_char_p, C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64,
+                               C.c_uint64, C.c_uint64],
+    "cpra_b200_cpra_files": [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, C.c_uint64,
+                             C.c_int, C.c_int, C.c_int, C.c_double],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -148,6 +155,17 @@ def _addr(a) -> int:
             raise ValueError("B200 operators take CUDA tensors (there is no CPU path)")
         return a.data_ptr()
     if hasattr(a, "ctypes"):  # numpy array: host pointer (ConvergeError's output only)
+        return a.ctypes.data
+    raise TypeError(f"cannot take the address of {type(a).__name__}")
+
+
+def _any_addr(a) -> int:
+    """Address of device, managed or host memory (the file I/O entries take any)."""
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if hasattr(a, "ctypes"):
         return a.ctypes.data
     raise TypeError(f"cannot take the address of {type(a).__name__}")
 
@@ -302,6 +320,39 @@ class B200Impl:
                                                     int(batch), int(epi), int(iters), int(pre_iter), float(beta),
                                                     1 if final_step else 0,
                                                     _host_addr(err) if err is not None else 0), "cpra_run_host")
+
+    # -- raw-file I/O (include/detail/CPRA.inl:8-48, src/CPRA_MKL.cpp:156-225) ------
+    def read_matrix(self, path, dst, count, elem_bytes=None) -> bool:
+        """ReadMatrixFromFile: ``count`` elements of a raw file into ``dst``
+        (device, managed or host); element size from the context's type."""
+        eb = (8 if self.dbl else 4) if elem_bytes is None else int(elem_bytes)
+        return _check(lib().cpra_b200_read_matrix(self._h, os.fsencode(path), _any_addr(dst), int(count), eb),
+                      "read_matrix")
+
+    def write_matrix(self, path, src, count, elem_bytes=None) -> bool:
+        """WriteMatrixToFile: ``count`` elements of ``src`` to a raw file."""
+        eb = (8 if self.dbl else 4) if elem_bytes is None else int(elem_bytes)
+        return _check(lib().cpra_b200_write_matrix(self._h, os.fsencode(path), _any_addr(src), int(count), eb),
+                      "write_matrix")
+
+    def write_starts(self, recon_prefix, err_prefix, file_index, x, err, P, batch, count=None) -> bool:
+        """The per-start output files of src/CPRA_MKL.cpp:186-209 for starts
+        0..count-1 of ``x`` [P][batch][m][n] (device) and host errors ``err``
+        [P][batch] (both prefixes' files, or only the reconstructions when
+        ``err_prefix`` and ``err`` are None)."""
+        count = batch if count is None else count
+        return _check(lib().cpra_b200_write_starts(
+            self._h, os.fsencode(recon_prefix), os.fsencode(err_prefix) if err_prefix is not None else None,
+            int(file_index), _addr(x), _host_addr(err) if err is not None else None, int(P), int(batch),
+            int(count)), "write_starts")
+
+    def cpra_files(self, a_path, s_path, recon_prefix, err_prefix, P, total, epi, iters, pre_iter, beta) -> bool:
+        """The reference program's main loop (src/CPRA_MKL.cpp:156-225) from
+        the constraint files to the per-start output files."""
+        return _check(lib().cpra_b200_cpra_files(self._h, os.fsencode(a_path), os.fsencode(s_path),
+                                                 os.fsencode(recon_prefix), os.fsencode(err_prefix), int(P),
+                                                 int(total), int(epi), int(iters), int(pre_iter), float(beta)),
+                      "cpra_files")
 
     def hio_shrinkwrap(self, x, A, S, batch, iters, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5,
                        threshold=0.1, positivity=False, a_stride=None, s_stride=None, estimate=None) -> bool:

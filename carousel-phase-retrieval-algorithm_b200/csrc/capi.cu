@@ -26,6 +26,7 @@
 #include <mutex>
 #include <string>
 #include <functional>
+#include <thread>
 #include <vector>
 
 using namespace cpra_b200;
@@ -199,6 +200,22 @@ struct cpra_b200_ctx {
     uint64_t refine_bytes = 0;
     void* best_sums = nullptr;
     uint64_t best_bytes = 0;
+    // raw-file I/O: two pinned staging chunks (CPRA_B200_OPT_IO_CHUNK bytes
+    // each), their events, and cpra_b200_cpra_files' device buffers (A, S,
+    // the starts, the gathered real parts)
+    void* io_pinned[2] = {nullptr, nullptr};
+    uint64_t io_pinned_bytes = 0;
+    cudaEvent_t io_ev[2] = {nullptr, nullptr};
+    cudaEvent_t io_ready = nullptr;
+    uint64_t io_chunk = 64ull << 20;
+    void* io_dev = nullptr;
+    uint64_t io_dev_bytes = 0;
+    void* io_A = nullptr;
+    uint64_t io_A_bytes = 0;
+    void* io_S = nullptr;
+    uint64_t io_S_bytes = 0;
+    void* io_x = nullptr;
+    uint64_t io_x_bytes = 0;
     // cpra_b200_cpra_run's lanes (CPRA_B200_OPT_LANES: 0 automatic)
     std::vector<RunLane> run_lanes;
     cudaEvent_t lane_fork = nullptr;
@@ -679,6 +696,13 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
         if (lane.stream) cudaStreamDestroy(lane.stream);
     }
     if (c->lane_fork) cudaEventDestroy(c->lane_fork);
+    for (int k = 0; k < 2; ++k) {
+        if (c->io_pinned[k]) cudaFreeHost(c->io_pinned[k]);
+        if (c->io_ev[k]) cudaEventDestroy(c->io_ev[k]);
+    }
+    if (c->io_ready) cudaEventDestroy(c->io_ready);
+    for (void* b : {c->io_dev, c->io_A, c->io_S, c->io_x})
+        if (b) cudaFree(b);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->hx) cudaFree(c->hx);
     if (c->hA) cudaFree(c->hA);
@@ -727,6 +751,10 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
         case CPRA_B200_OPT_LANES:
             if (value < 0 || value > CPRA_B200_MAX_LANES) return fail(CPRA_B200_EARG, "lanes must be 0..16");
             c->lanes_opt = (int)value;
+            break;
+        case CPRA_B200_OPT_IO_CHUNK:
+            if (value < 4096) return fail(CPRA_B200_EARG, "io chunk must be >= 4096 bytes");
+            c->io_chunk = (uint64_t)value;
             break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
@@ -1535,6 +1563,7 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
         case CPRA_B200_OPT_HIO_CHUNK: *value = (int64_t)c->hio_chunk; break;
         case CPRA_B200_OPT_GRAPH: *value = c->graphs ? 1 : 0; break;
         case CPRA_B200_OPT_LANES: *value = run_lanes_for(c, c->batch); break;
+        case CPRA_B200_OPT_IO_CHUNK: *value = (int64_t)c->io_chunk; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1917,4 +1946,241 @@ int cpra_b200_cpra_run_host(cpra_b200_ctx* c, void* x_host, const void* A_host, 
     return CPRA_B200_OK;
 }
 
+
+// ---- raw-file I/O (include/detail/CPRA.inl:8-48; src/CPRA_MKL.cpp:156-225) ---
+// Files hold elements of T back to back, no header.  Copies between a file and
+// memory (device, managed or host) go through two pinned chunks on the copy
+// stream: the file side of one chunk overlaps the copy of the other.  These
+// helpers report errors through `msg` only, so that cpra_b200_cpra_files'
+// writer thread can use them.
+
+int io_prepare(cpra_b200_ctx* c) {
+    if (!c->copy_stream)
+        CPRA_CHECK_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!c->io_ready) CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&c->io_ready, cudaEventDisableTiming), "cudaEventCreate");
+    for (int k = 0; k < 2; ++k) {
+        if (!c->io_ev[k])
+            CPRA_CHECK_CUDA(cudaEventCreateWithFlags(&c->io_ev[k], cudaEventDisableTiming), "cudaEventCreate");
+        if (c->io_pinned_bytes != c->io_chunk && c->io_pinned[k]) {
+            cudaFreeHost(c->io_pinned[k]);
+            c->io_pinned[k] = nullptr;
+        }
+        if (!c->io_pinned[k]) CPRA_CHECK_CUDA(cudaMallocHost(&c->io_pinned[k], c->io_chunk), "cudaMallocHost(io)");
+    }
+    c->io_pinned_bytes = c->io_chunk;
+    return CPRA_B200_OK;
+}
+
+// copy_stream waits for the work already on the context's stream
+int io_after_stream(cpra_b200_ctx* c) {
+    CPRA_CHECK_CUDA(cudaEventRecord(c->io_ready, c->stream), "cudaEventRecord");
+    CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->copy_stream, c->io_ready, 0), "cudaStreamWaitEvent");
+    return CPRA_B200_OK;
+}
+
+int file_to_mem(cpra_b200_ctx* c, FILE* f, char* dst, uint64_t bytes, std::string& msg) {
+    bool used[2] = {false, false};
+    uint64_t off = 0;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; off < bytes && e == cudaSuccess; k ^= 1) {
+        const uint64_t len = std::min(c->io_chunk, bytes - off);
+        if (used[k] && (e = cudaEventSynchronize(c->io_ev[k])) != cudaSuccess) break;
+        if (std::fread(c->io_pinned[k], 1, len, f) != len) {
+            cudaStreamSynchronize(c->copy_stream);
+            msg = "short file: fewer bytes than the requested elements";
+            return CPRA_B200_EARG;
+        }
+        if ((e = cudaMemcpyAsync(dst + off, c->io_pinned[k], len, cudaMemcpyDefault, c->copy_stream)) != cudaSuccess)
+            break;
+        e = cudaEventRecord(c->io_ev[k], c->copy_stream);
+        used[k] = true;
+        off += len;
+    }
+    const cudaError_t es = cudaStreamSynchronize(c->copy_stream);
+    if (e == cudaSuccess) e = es;
+    if (e != cudaSuccess) {
+        msg = std::string("file read copy: ") + cudaGetErrorString(e);
+        return CPRA_B200_ECUDA;
+    }
+    return CPRA_B200_OK;
+}
+
+int mem_to_file(cpra_b200_ctx* c, const char* src, uint64_t bytes, FILE* f, std::string& msg) {
+    uint64_t issued = 0, written = 0, pend[2] = {0, 0};
+    cudaError_t e = cudaSuccess;
+    auto issue = [&](int k) {
+        pend[k] = std::min(c->io_chunk, bytes - issued);
+        e = cudaMemcpyAsync(c->io_pinned[k], src + issued, pend[k], cudaMemcpyDefault, c->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->io_ev[k], c->copy_stream);
+        issued += pend[k];
+    };
+    for (int k = 0; k < 2 && issued < bytes && e == cudaSuccess; ++k) issue(k);
+    for (int k = 0; written < bytes && e == cudaSuccess; k ^= 1) {
+        if ((e = cudaEventSynchronize(c->io_ev[k])) != cudaSuccess) break;
+        if (std::fwrite(c->io_pinned[k], 1, pend[k], f) != pend[k]) {
+            cudaStreamSynchronize(c->copy_stream);
+            msg = "file write failed";
+            return CPRA_B200_EARG;
+        }
+        written += pend[k];
+        if (issued < bytes) issue(k);
+    }
+    const cudaError_t es = cudaStreamSynchronize(c->copy_stream);
+    if (e == cudaSuccess) e = es;
+    if (e != cudaSuccess) {
+        msg = std::string("file write copy: ") + cudaGetErrorString(e);
+        return CPRA_B200_ECUDA;
+    }
+    return CPRA_B200_OK;
+}
+
+// `path` <- `bytes` of memory; the file is created or overwritten
+int write_file(cpra_b200_ctx* c, const std::string& path, const void* src, uint64_t bytes, bool host, std::string& msg) {
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) {
+        msg = "cannot open " + path + " for writing";
+        return CPRA_B200_EARG;
+    }
+    int r = CPRA_B200_OK;
+    if (host) {
+        if (std::fwrite(src, 1, bytes, f) != bytes) {
+            msg = "file write failed: " + path;
+            r = CPRA_B200_EARG;
+        }
+    } else {
+        r = mem_to_file(c, static_cast<const char*>(src), bytes, f, msg);
+    }
+    if (std::fclose(f) != 0 && !r) {
+        msg = "file close failed: " + path;
+        r = CPRA_B200_EARG;
+    }
+    return r;
+}
+
+// the output files of starts [0, count) of x's gathered real parts (dev,
+// [count][P][MN] of T) and of their errors (err [P][B] of T, host; may be
+// null): <recon>.<index + i> and <errp>.<index + i>
+int write_start_files(cpra_b200_ctx* c, const char* dev, const void* err, uint64_t P, uint64_t B, uint64_t count,
+                      const std::string& recon, const std::string& errp, uint64_t index, std::string& msg) {
+    const uint64_t es = c->esize(), per = P * c->plane() * es;
+    std::vector<char> e(P * es);
+    for (uint64_t i = 0; i < count; ++i) {
+        const std::string sfx = "." + std::to_string(index + i);
+        int r = write_file(c, recon + sfx, dev + i * per, per, false, msg);
+        if (r) return r;
+        if (!err) continue;
+        // src/CPRA_MKL.cpp:195-196: per_error[p] = error[p * n + i]
+        for (uint64_t p = 0; p < P; ++p)
+            std::memcpy(e.data() + p * es, static_cast<const char*>(err) + (p * B + i) * es, es);
+        if ((r = write_file(c, errp + sfx, e.data(), P * es, true, msg))) return r;
+    }
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_read_matrix(cpra_b200_ctx* c, const char* path, void* dst, uint64_t count, uint64_t elem_bytes) {
+    CTX_OR_RETURN(c);
+    if (!path || !dst) return fail(CPRA_B200_EARG, "read_matrix: null pointer");
+    // include/detail/CPRA.inl:11-21: a missing file and a zero size are errors
+    if (count == 0 || elem_bytes == 0) return fail(CPRA_B200_EARG, "read_matrix: zero size");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(CPRA_B200_EARG, std::string("read_matrix: cannot open ") + path);
+    std::string msg;
+    r = io_prepare(c);
+    if (!r) r = io_after_stream(c);
+    if (!r) r = file_to_mem(c, f, static_cast<char*>(dst), count * elem_bytes, msg);
+    std::fclose(f);
+    if (r && !msg.empty()) return fail(r, "read_matrix: " + msg + " (" + path + ")");
+    return r;
+}
+
+int cpra_b200_write_matrix(cpra_b200_ctx* c, const char* path, const void* src, uint64_t count, uint64_t elem_bytes) {
+    CTX_OR_RETURN(c);
+    if (!path || !src) return fail(CPRA_B200_EARG, "write_matrix: null pointer");
+    if (count == 0 || elem_bytes == 0) return fail(CPRA_B200_EARG, "write_matrix: zero size");  // CPRA.inl:39-43
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    std::string msg;
+    r = io_prepare(c);
+    if (!r) r = io_after_stream(c);
+    if (!r) r = write_file(c, path, src, count * elem_bytes, false, msg);
+    if (r && !msg.empty()) return fail(r, "write_matrix: " + msg);
+    return r;
+}
+
+int cpra_b200_write_starts(cpra_b200_ctx* c, const char* recon_prefix, const char* err_prefix, uint64_t file_index,
+                           const void* x, const void* err_host, uint64_t P, uint64_t batch, uint64_t count) {
+    CTX_OR_RETURN(c);
+    if (!recon_prefix || !x) return fail(CPRA_B200_EARG, "write_starts: null pointer");
+    if (P == 0 || batch == 0 || count == 0 || count > batch)
+        return fail(CPRA_B200_EARG, "write_starts: P, batch >= 1 and 1 <= count <= batch");
+    if ((err_prefix == nullptr) != (err_host == nullptr))
+        return fail(CPRA_B200_EARG, "write_starts: err_prefix and err_host go together");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t MN = c->plane();
+    if ((r = ensure_buffer(c, &c->io_dev, &c->io_dev_bytes, count * P * MN * c->esize(), "cudaMalloc(io)"))) return r;
+    if ((r = io_prepare(c))) return r;
+    CPRA_CHECK_CUDA(launch_real_starts(c->dbl, x, c->io_dev, MN, P, batch, 0, count, c->stream), "write_starts");
+    if ((r = io_after_stream(c))) return r;
+    std::string msg;
+    r = write_start_files(c, static_cast<const char*>(c->io_dev), err_host, P, batch, count, recon_prefix,
+                          err_prefix ? err_prefix : "", file_index, msg);
+    if (r) return fail(r, "write_starts: " + msg);
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_cpra_files(cpra_b200_ctx* c, const char* a_path, const char* s_path, const char* recon_prefix,
+                         const char* err_prefix, uint64_t P, uint64_t total, int epi, int iters, int pre_iter,
+                         double beta) {
+    CTX_OR_RETURN(c);
+    if (!a_path || !s_path || !recon_prefix || !err_prefix) return fail(CPRA_B200_EARG, "cpra_files: null pointer");
+    if (P < 2) return fail(CPRA_B200_EARG, "cpra_files: P >= 2");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t MN = c->plane(), B = c->batch, es = c->esize();
+    // src/CPRA_MKL.cpp:160-170: the modulus and support planes [P][m][n]
+    if ((r = ensure_buffer(c, &c->io_A, &c->io_A_bytes, P * MN * es, "cudaMalloc(io A)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_S, &c->io_S_bytes, P * MN * es, "cudaMalloc(io S)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_x, &c->io_x_bytes, P * B * MN * c->csize(), "cudaMalloc(io x)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_dev, &c->io_dev_bytes, B * P * MN * es, "cudaMalloc(io)"))) return r;
+    if ((r = cpra_b200_read_matrix(c, a_path, c->io_A, P * MN, es))) return r;
+    if ((r = cpra_b200_read_matrix(c, s_path, c->io_S, P * MN, es))) return r;
+    // :172-224: N = max(batch, total) starts in batches of the context's
+    // batch size; a last partial batch runs whole and writes its first n
+    const uint64_t N = std::max<uint64_t>(B, total);
+    const bool with_err = epi > 0 && iters >= 1;
+    std::vector<char> err[2] = {std::vector<char>(P * B * es, 0), std::vector<char>(P * B * es, 0)};
+    std::thread writer;
+    int wr = CPRA_B200_OK;
+    std::string wmsg;
+    auto join = [&]() {
+        if (writer.joinable()) writer.join();
+        return wr;
+    };
+    uint64_t file_index = 1;
+    int k = 0;
+    for (uint64_t left = N; left > 0; k ^= 1) {
+        const uint64_t n = std::min(left, B);
+        r = cpra_b200_initialize(c, c->io_x, P * B * MN * 2);
+        if (!r)
+            r = cpra_run_impl(c, c->io_x, c->io_A, c->io_S, P, B, epi, iters, pre_iter, beta, 1,
+                              with_err ? err[k].data() : nullptr, nullptr, nullptr);
+        // the previous batch's files were written while this batch computed
+        if (join() && !r) r = fail(wr, "cpra_files: " + wmsg);
+        if (r) return r;
+        CPRA_CHECK_CUDA(launch_real_starts(c->dbl, c->io_x, c->io_dev, MN, P, B, 0, n, c->stream), "cpra_files");
+        if ((r = io_prepare(c)) || (r = io_after_stream(c))) return r;
+        writer = std::thread([c, n, P, B, file_index, &err, k, &wr, &wmsg, recon = std::string(recon_prefix),
+                              errp = std::string(err_prefix)]() {
+            wr = write_start_files(c, static_cast<const char*>(c->io_dev), err[k].data(), P, B, n, recon, errp,
+                                   file_index, wmsg);
+        });
+        file_index += n;
+        left -= n;
+    }
+    if (join()) return fail(wr, "cpra_files: " + wmsg);
+    return CPRA_B200_OK;
+}
 }  // extern "C"

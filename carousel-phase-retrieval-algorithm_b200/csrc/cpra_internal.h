@@ -61,6 +61,9 @@ cudaError_t launch_fftshift2d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_
 cudaError_t launch_fftshift3d(bool dbl, void* x, uint64_t M, uint64_t N, uint64_t L, uint64_t batch,
                               cudaStream_t st);
 cudaError_t launch_uniform(bool dbl, void* x, uint64_t num, uint64_t seed, uint64_t stream_id, cudaStream_t st);
+// real parts of starts first..first+count-1 of x [P][B][MN], per start: dst [count][P][MN]
+cudaError_t launch_real_starts(bool dbl, const void* x, void* dst, uint64_t MN, uint64_t P, uint64_t B, uint64_t first,
+                               uint64_t count, cudaStream_t st);
 // ||old_i|| and ||new_i|| over `span` elements at stride `stride` for i < batch,
 // accumulated in double into sums[2*batch] (deterministic two-level reduction
 // through `partials`, >= batch * CONVERGE_BLOCKS * 2 doubles).

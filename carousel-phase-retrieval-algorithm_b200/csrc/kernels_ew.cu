@@ -80,6 +80,32 @@ __global__ void k_merge(const Cx<T>* src, Cx<T>* dst, T alpha, T beta, uint64_t 
     for (uint64_t i = gtid(); i < num; i += gstride()) dst[i] = merge_apply(src[i], dst[i], alpha, beta);
 }
 
+// Real parts of starts first..first+count-1 of a carousel run x [P][B][MN]
+// (complex), gathered per start: dst [count][P][MN] -- the per-start output
+// files of src/CPRA_MKL.cpp:186-209 (ComplexToReal, then each start's P planes).
+template <typename T>
+__global__ void k_real_starts(const Cx<T>* __restrict__ x, T* __restrict__ dst, uint64_t MN, uint64_t P, uint64_t B,
+                              uint64_t first, uint64_t count) {
+    const uint64_t total = count * P * MN;
+    for (uint64_t e = gtid(); e < total; e += gstride()) {
+        const uint64_t j = e % MN, plane = e / MN;
+        dst[e] = x[((plane % P) * B + first + plane / P) * MN + j].x;
+    }
+}
+
+// the same, four pixels per thread (MN % 4 == 0; x and dst 16-byte aligned):
+// two 16-byte loads of (re, im, re, im), one 16-byte store of the reals
+__global__ void k_real_starts4(const float4* __restrict__ x, float4* __restrict__ dst, uint64_t MN4, uint64_t P,
+                               uint64_t B, uint64_t first, uint64_t count) {
+    const uint64_t total = count * P * MN4;
+    for (uint64_t e = gtid(); e < total; e += gstride()) {
+        const uint64_t j = e % MN4, plane = e / MN4;
+        const float4* s = x + 2 * (((plane % P) * B + first + plane / P) * MN4 + j);
+        const float4 a = s[0], b = s[1];
+        dst[e] = make_float4(a.x, a.z, b.x, b.z);
+    }
+}
+
 template <typename T>
 __global__ void k_scale(Cx<T>* __restrict__ x, T f, uint64_t num) {
     for (uint64_t i = gtid(); i < num; i += gstride()) x[i] = cscale(x[i], f);
@@ -429,6 +455,25 @@ cudaError_t launch_merge_add(bool dbl, const void* src, void* dst, double alpha,
     else
         k_merge<float><<<g, EW_THREADS, 0, st>>>((const Cx<float>*)src, (Cx<float>*)dst, (float)alpha,
                                                  (float)beta, num);
+    count_launches();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_real_starts(bool dbl, const void* x, void* dst, uint64_t MN, uint64_t P, uint64_t B, uint64_t first,
+                               uint64_t count, cudaStream_t st) {
+    const uint64_t total = count * P * MN;
+    if (total == 0) return cudaSuccess;
+    const bool vec = !dbl && MN % 4 == 0 && (reinterpret_cast<uintptr_t>(x) & 15u) == 0 &&
+                     (reinterpret_cast<uintptr_t>(dst) & 15u) == 0;
+    if (vec)
+        k_real_starts4<<<ew_grid(total / 4, EW_THREADS), EW_THREADS, 0, st>>>((const float4*)x, (float4*)dst, MN / 4,
+                                                                             P, B, first, count);
+    else if (dbl)
+        k_real_starts<double><<<ew_grid(total, EW_THREADS), EW_THREADS, 0, st>>>((const Cx<double>*)x, (double*)dst,
+                                                                                MN, P, B, first, count);
+    else
+        k_real_starts<float><<<ew_grid(total, EW_THREADS), EW_THREADS, 0, st>>>((const Cx<float>*)x, (float*)dst, MN,
+                                                                               P, B, first, count);
     count_launches();
     return cudaGetLastError();
 }

@@ -66,6 +66,8 @@ extern "C" {
                                     to give each the busiest lane's episode count).  Same results in every
                                     case. */
 #define CPRA_B200_MAX_LANES 16
+#define CPRA_B200_OPT_IO_CHUNK 9   /* bytes of each of the two pinned staging chunks of the file I/O entries
+                                    (default 64 MiB, at least 4096) */
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 
@@ -174,6 +176,50 @@ int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S
 int cpra_b200_cpra_run_host(cpra_b200_ctx* ctx, void* x_host, const void* A_host, const void* S_host, uint64_t P,
                             uint64_t batch, int epi, int iters, int pre_iter, double beta, int final_step,
                             void* err_host);
+
+/* Extension: the reference's raw-file reader Cpra::ReadMatrixFromFile
+ * (include/detail/CPRA.inl:8-28), `count` elements of `elem_bytes` each, no
+ * header, into dst (device, managed or host memory).  The file is read in
+ * pinned chunks, each chunk's read overlapping the copy of the one before.
+ * Errors, as the reference's: a missing file, a zero size; and a file shorter
+ * than count elements (the reference's fread leaves the rest unwritten and
+ * reports success).  Synchronous; ordered after the context's earlier work. */
+int cpra_b200_read_matrix(cpra_b200_ctx* ctx, const char* path, void* dst, uint64_t count, uint64_t elem_bytes);
+
+/* Extension: Cpra::WriteMatrixToFile (include/detail/CPRA.inl:30-48): `count`
+ * elements of `elem_bytes` each from src (device, managed or host memory) to
+ * a raw file, created or overwritten (the reference also prints a notice when
+ * it overwrites), through the same pinned chunks.  Synchronous. */
+int cpra_b200_write_matrix(cpra_b200_ctx* ctx, const char* path, const void* src, uint64_t count,
+                           uint64_t elem_bytes);
+
+/* Extension: the output files of src/CPRA_MKL.cpp:186-209 for starts
+ * 0..count-1 of a carousel run x ([P][batch][m][n] complex T, device memory)
+ * and its errors err_host ([P][batch] T, host memory, as cpra_b200_cpra_run
+ * returns them): for start i,
+ *   <recon_prefix>.<file_index + i>  the real parts of its P planes, [P][m][n] T;
+ *   <err_prefix>.<file_index + i>    its P errors, P elements of T
+ * (the reference writes sizeof(float)*P elements there, reading past its P
+ * errors; here the file holds the P errors only).  The real parts are
+ * gathered per start on the device, then streamed out through the pinned
+ * chunks.  err_prefix and err_host both null: no error files.  Synchronous. */
+int cpra_b200_write_starts(cpra_b200_ctx* ctx, const char* recon_prefix, const char* err_prefix, uint64_t file_index,
+                           const void* x, const void* err_host, uint64_t P, uint64_t batch, uint64_t count);
+
+/* Extension: the reference program's main loop (src/CPRA_MKL.cpp:156-225)
+ * without its command-line parser: reads the modulus and support planes
+ * ([P][m][n] T each) from a_path and s_path, then for max(batch, total)
+ * starts in batches of the context's batch size: Initialize the guesses
+ * ([P][batch][m][n], the context's seeded stream, one call per batch), run
+ * cpra_b200_cpra_run (final projection on; errors when epi >= 1 and
+ * iters >= 1, else zeros), and write each start's two files as
+ * cpra_b200_write_starts does, numbered from 1 across batches.  A last
+ * partial batch of n starts runs as a whole batch and writes its first n.
+ * Each batch's files are written by a host thread while the next batch
+ * computes.  Synchronous. */
+int cpra_b200_cpra_files(cpra_b200_ctx* ctx, const char* a_path, const char* s_path, const char* recon_prefix,
+                         const char* err_prefix, uint64_t P, uint64_t total, int epi, int iters, int pre_iter,
+                         double beta);
 
 /* Extension (project-defined, no counterpart in the reference): R-factor of
  * `batch` patterns x ([batch][m][n], the context's plane size) against their

@@ -44,6 +44,18 @@ def test_bindings_cover_every_symbol():
     assert not extra, f"declared but not bound in Python: {extra}"
 
 
+def test_bindings_cover_every_option():
+    """Every CPRA_B200_OPT_* of the header has a Python constant of the same value."""
+    import cpra_b200
+    opts = {}
+    for h in HEADERS:
+        for m in re.finditer(r"#define\s+CPRA_B200_(OPT_\w+)\s+(\d+)", h.read_text()):
+            opts[m.group(1)] = int(m.group(2))
+    assert "OPT_LANES" in opts and "OPT_IO_CHUNK" in opts
+    for name, value in opts.items():
+        assert getattr(cpra_b200, name, None) == value, name
+
+
 def test_no_cpu_fallback_in_package():
     """The product path has no CPU implementation: it never imports the oracle."""
     pkg = REPO / "carousel-phase-retrieval-algorithm_b200"
