@@ -1546,7 +1546,8 @@ int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
 // each lane the same number of episodes as the busiest one has (a lane takes
 // its episodes one after another, so the busiest lane sets the time).
 int balanced_lanes(int want, int epi) {
-    const int w = std::max(1, std::min(want, epi));
+    if (epi <= 1 || want <= 1) return 1;
+    const int w = std::min(want, epi);
     const int per_lane = (epi + w - 1) / w;
     return std::max(1, (epi + per_lane - 1) / per_lane);
 }

@@ -535,7 +535,8 @@ def test_cpra_run_host_bitwise(tb, L, P, B, epi, it, pre, final, pinned, dtype):
                          [(64, 7, 2, 3, 2, 1, 2, True, "float32"), (64, 6, 3, 4, 3, 0, 3, False, "float32"),
                           (32, 5, 2, 5, 2, 1, 0, True, "float32"), (128, 3, 2, 4, 2, 1, 4, True, "float32"),
                           (256, 5, 2, 3, 2, 1, 2, True, "float32"), (512, 3, 1, 2, 2, 0, 0, True, "float32"),
-                          (32, 4, 2, 3, 2, 1, 2, True, "float64")])
+                          (32, 4, 2, 3, 2, 1, 2, True, "float64"), (64, 3, 2, 0, 2, 1, 4, True, "float32"),
+                          (64, 3, 2, 1, 2, 1, 4, True, "float32")])
 def test_cpra_run_lanes_bitwise(tb, L, P, B, epi, it, pre, lanes, final, dtype):
     """cpra_run's wavefront schedule (episode e on lane e mod W, angle p of
     episode e beside angle p-2 of episode e+1) writes the same bits and the
