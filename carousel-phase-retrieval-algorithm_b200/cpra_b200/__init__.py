@@ -94,6 +94,10 @@ _SIGS = {
                                C.c_uint64, C.c_uint64],
     "cpra_b200_cpra_files": [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, C.c_uint64,
                              C.c_int, C.c_int, C.c_int, C.c_double],
+    "cpra_b200_conv_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int,
+                           C.c_void_p],
+    "cpra_b200_conv_files": [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, C.c_int,
+                             C.c_double],
     "cpra_b200_kernel_timing": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
     "cpra_b200_hio_shrinkwrap": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_uint64,
                                  C.c_int, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -313,6 +317,14 @@ class B200Impl:
                                                int(iters), int(pre_iter), float(beta), 1 if final_step else 0,
                                                _host_addr(err) if err is not None else 0), "cpra_run")
 
+    def conv_run(self, x, A, S, iters, beta, final_step=True, err=None) -> bool:
+        """The conventional 3D driver of src/CONV_MKL.cpp:10-88 on resident
+        volumes; ``err`` (host array of batch, optional) receives the last
+        iteration's convergence errors."""
+        return _check(lib().cpra_b200_conv_run(self._h, _addr(x), _addr(A), _addr(S), int(iters), float(beta),
+                                               1 if final_step else 0,
+                                               _host_addr(err) if err is not None else 0), "conv_run")
+
     def cpra_run_host(self, x, A, S, P, batch, epi, iters, pre_iter, beta, final_step=True, err=None) -> bool:
         """``cpra_run`` on host arrays (numpy or CPU tensors; pinned ones let the
         per-angle copies overlap the computation); ``x`` is overwritten."""
@@ -353,6 +365,13 @@ class B200Impl:
                                                  os.fsencode(recon_prefix), os.fsencode(err_prefix), int(P),
                                                  int(total), int(epi), int(iters), int(pre_iter), float(beta)),
                       "cpra_files")
+
+    def conv_files(self, a_path, s_path, recon_prefix, err_prefix, total, iters, beta) -> bool:
+        """The conventional program's main loop (src/CONV_MKL.cpp:103-172) from
+        the constraint volumes' files to per-start output files."""
+        return _check(lib().cpra_b200_conv_files(self._h, os.fsencode(a_path), os.fsencode(s_path),
+                                                 os.fsencode(recon_prefix), os.fsencode(err_prefix), int(total),
+                                                 int(iters), float(beta)), "conv_files")
 
     def hio_shrinkwrap(self, x, A, S, batch, iters, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5,
                        threshold=0.1, positivity=False, a_stride=None, s_stride=None, estimate=None) -> bool:

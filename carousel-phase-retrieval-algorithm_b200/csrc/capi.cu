@@ -1620,17 +1620,7 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     if (r) return take_deferred(c);
     const uint64_t MN = c->plane(), MNB = MN * batch;
     const uint64_t cb = MNB * c->csize();
-    if (c->drv_bytes < 3 * cb) {
-        ++c->epoch;
-        if (c->drv) {
-            cudaStreamSynchronize(c->stream);
-            cudaFree(c->drv);
-            c->drv = nullptr;
-            c->drv_bytes = 0;
-        }
-        CPRA_CHECK_CUDA(cudaMalloc(&c->drv, 3 * cb), "cudaMalloc(driver buffers)");
-        c->drv_bytes = 3 * cb;
-    }
+    if ((r = ensure_buffer(c, &c->drv, &c->drv_bytes, 3 * cb, "cudaMalloc(driver buffers)"))) return r;
     const bool want_err = err_host && epi > 0;
     if (want_err) {
         r = ensure_reduction(c, batch);
@@ -1948,6 +1938,123 @@ int cpra_b200_cpra_run_host(cpra_b200_ctx* c, void* x_host, const void* A_host, 
 }
 
 
+// The conventional 3D driver ShrinkWrap_CONV_MKL_Sample (src/CONV_MKL.cpp:10-88)
+// on device buffers: x holds the context's batch of [l][m][n] volumes, A and S
+// one volume each (broadcast over the batch, as the reference's calls do).
+//   t1 = t2 = x (:31-32); `iters` difference-map iterations with Forward3D /
+//   Backward3D (:35-67; fused into axis passes for power-of-two volumes);
+//   on the last one, the convergence error (:39-44, 70-77) when err_host is
+//   given; then, with final_step, the final projection (:80-88).
+static int conv_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S, int iters, double beta,
+                         int final_step, void* err_host) {
+    if (!x || !A || !S) return fail(CPRA_B200_EARG, "conv_run: null pointer");
+    if (iters < 0) return fail(CPRA_B200_EARG, "conv_run: negative count");
+    if (err_host && iters < 1) return fail(CPRA_B200_EARG, "conv_run: the error step needs iters >= 1");
+    if (err_host && c->batch > 65535) return fail(CPRA_B200_EUNSUP, "conv_run: batch_size above 65535");
+    const double b = c->round_t(beta);
+    if (b == 0.0) return fail(CPRA_B200_EARG, "conv_run: beta == 0");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
+        return fail(CPRA_B200_EUNSUP, "conv_run: each size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t B = c->batch, MN = c->plane(), vol = MN * c->l, num = vol * B, cb = num * c->csize();
+    if ((r = ensure_buffer(c, &c->drv, &c->drv_bytes, 3 * cb, "cudaMalloc(driver buffers)"))) return r;
+    const bool want_err = err_host != nullptr;
+    if (want_err && (r = ensure_reduction(c, B))) return r;
+    if ((r = ensure_work(c, cb))) return r;  // transforms of other sizes
+    char* t1 = static_cast<char*>(c->drv);
+    char* t2 = t1 + cb;
+    char* old = t2 + cb;
+    // src/CONV_MKL.cpp:47,53,64,65: the coefficients as the 2D driver's
+    const DmCoef coef = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
+                         c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
+    DmPattern pat;
+    pat.x = x;
+    pat.t1 = t1;
+    pat.t2 = t2;
+    pat.A = A;
+    pat.S = S;
+    pat.num = num;
+    pat.batch = B;
+    pat.c = coef;
+    pat.dim = 3;
+    auto copy = [&](void* dst, const void* src) {
+        return cudaMemcpyAsync(dst, src, cb, cudaMemcpyDeviceToDevice, c->stream);
+    };
+    auto iterate = [&](int n) -> int {
+        if (n <= 0) return CPRA_B200_OK;
+        if (fusable_shape3d(c)) return launch_fused(c, pat, n);
+        for (int i = 0; i < n; ++i) {
+            const Op seq[12] = {
+                {OpKind::Fwd3D, t1, nullptr, 0, 0, 0, 0},   {OpKind::DataReal, t1, A, num, B, 0, 0},
+                {OpKind::Bwd3D, t1, nullptr, 0, 0, 0, 0},   {OpKind::Merge, t1, x, num, 1, coef.a1, coef.b1},
+                {OpKind::Space, t1, S, num, B, 0, 0},       {OpKind::Space, t2, S, num, B, 0, 0},
+                {OpKind::Merge, t2, x, num, 1, coef.a2, coef.b2}, {OpKind::Fwd3D, t2, nullptr, 0, 0, 0, 0},
+                {OpKind::DataReal, t2, A, num, B, 0, 0},    {OpKind::Bwd3D, t2, nullptr, 0, 0, 0, 0},
+                {OpKind::Merge, x, t1, num, 1, coef.a3, coef.b3}, {OpKind::Merge, x, t2, num, 1, coef.a4, coef.b4}};
+            for (const Op& op : seq) {
+                const int rr = exec_op(c, op);
+                if (rr) return rr;
+            }
+        }
+        return CPRA_B200_OK;
+    };
+    auto enqueue = [&]() -> int {
+        int r = CPRA_B200_OK;
+        CPRA_CHECK_CUDA(copy(t1, x), "conv_run");
+        CPRA_CHECK_CUDA(copy(t2, x), "conv_run");
+        if ((r = iterate(want_err ? iters - 1 : iters))) return r;
+        if (want_err) {
+            CPRA_CHECK_CUDA(copy(old, x), "conv_run");
+            if ((r = iterate(1))) return r;
+            CPRA_CHECK_CUDA(copy(t1, x), "conv_run");
+            if ((r = exec_fft3d(c, old, false)) || (r = exec_fft3d(c, t1, false))) return r;
+            // ConvergeError (CUDA_Impl.inl:145-172): old <- t1 - old; norms over
+            // the first m*n elements of each volume (stride m*n*l)
+            CPRA_CHECK_CUDA(launch_merge_add(c->dbl, t1, old, 1.0, -1.0, num, c->stream), "conv_run");
+            CPRA_CHECK_CUDA(launch_norm_pairs(c->dbl, old, t1, MN, vol, B, c->partials, c->sums, c->stream),
+                            "conv_run");
+            CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost,
+                                            c->stream),
+                            "conv_run");
+        }
+        if (final_step) {
+            CPRA_CHECK_CUDA(copy(t1, x), "conv_run");
+            const Op seq[5] = {{OpKind::Fwd3D, t1, nullptr, 0, 0, 0, 0},
+                               {OpKind::DataReal, t1, A, num, B, 0, 0},
+                               {OpKind::Bwd3D, t1, nullptr, 0, 0, 0, 0},
+                               {OpKind::Merge, t1, x, num, 1, coef.a1, coef.b1},
+                               {OpKind::Space, t1, S, num, B, 0, 0}};
+            for (const Op& op : seq)
+                if ((r = exec_op(c, op))) return r;
+            CPRA_CHECK_CUDA(copy(x, t1), "conv_run");
+        }
+        return CPRA_B200_OK;
+    };
+    r = run_maybe_graph(c,
+                        graph_key("conv_run", x, A, S, iters, b, final_step, want_err, c->space_mode, c->data_mode,
+                                  c->fusion),
+                        enqueue);
+    if (r) return r;
+    if (want_err) {
+        CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "conv_run");
+        for (uint64_t i = 0; i < B; ++i) {
+            const double v = std::sqrt(c->host_sums[2 * i]) / std::sqrt(c->host_sums[2 * i + 1]);
+            if (c->dbl)
+                static_cast<double*>(err_host)[i] = v;
+            else
+                static_cast<float*>(err_host)[i] = (float)v;
+        }
+    }
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_conv_run(cpra_b200_ctx* c, void* x, const void* A, const void* S, int iters, double beta,
+                       int final_step, void* err_host) {
+    CTX_OR_RETURN(c);
+    return conv_run_impl(c, x, A, S, iters, beta, final_step, err_host);
+}
+
 // ---- raw-file I/O (include/detail/CPRA.inl:8-48; src/CPRA_MKL.cpp:156-225) ---
 // Files hold elements of T back to back, no header.  Copies between a file and
 // memory (device, managed or host) go through two pinned chunks on the copy
@@ -2062,8 +2169,9 @@ int write_file(cpra_b200_ctx* c, const std::string& path, const void* src, uint6
 // [count][P][MN] of T) and of their errors (err [P][B] of T, host; may be
 // null): <recon>.<index + i> and <errp>.<index + i>
 int write_start_files(cpra_b200_ctx* c, const char* dev, const void* err, uint64_t P, uint64_t B, uint64_t count,
-                      const std::string& recon, const std::string& errp, uint64_t index, std::string& msg) {
-    const uint64_t es = c->esize(), per = P * c->plane() * es;
+                      uint64_t elems_per_start, const std::string& recon, const std::string& errp, uint64_t index,
+                      std::string& msg) {
+    const uint64_t es = c->esize(), per = elems_per_start * es;
     std::vector<char> e(P * es);
     for (uint64_t i = 0; i < count; ++i) {
         const std::string sfx = "." + std::to_string(index + i);
@@ -2126,7 +2234,7 @@ int cpra_b200_write_starts(cpra_b200_ctx* c, const char* recon_prefix, const cha
     CPRA_CHECK_CUDA(launch_real_starts(c->dbl, x, c->io_dev, MN, P, batch, 0, count, c->stream), "write_starts");
     if ((r = io_after_stream(c))) return r;
     std::string msg;
-    r = write_start_files(c, static_cast<const char*>(c->io_dev), err_host, P, batch, count, recon_prefix,
+    r = write_start_files(c, static_cast<const char*>(c->io_dev), err_host, P, batch, count, P * MN, recon_prefix,
                           err_prefix ? err_prefix : "", file_index, msg);
     if (r) return fail(r, "write_starts: " + msg);
     return CPRA_B200_OK;
@@ -2173,15 +2281,63 @@ int cpra_b200_cpra_files(cpra_b200_ctx* c, const char* a_path, const char* s_pat
         if (r) return r;
         CPRA_CHECK_CUDA(launch_real_starts(c->dbl, c->io_x, c->io_dev, MN, P, B, 0, n, c->stream), "cpra_files");
         if ((r = io_prepare(c)) || (r = io_after_stream(c))) return r;
-        writer = std::thread([c, n, P, B, file_index, &err, k, &wr, &wmsg, recon = std::string(recon_prefix),
+        writer = std::thread([c, n, P, B, MN, file_index, &err, k, &wr, &wmsg, recon = std::string(recon_prefix),
                               errp = std::string(err_prefix)]() {
-            wr = write_start_files(c, static_cast<const char*>(c->io_dev), err[k].data(), P, B, n, recon, errp,
-                                   file_index, wmsg);
+            wr = write_start_files(c, static_cast<const char*>(c->io_dev), err[k].data(), P, B, n, P * MN, recon,
+                                   errp, file_index, wmsg);
         });
         file_index += n;
         left -= n;
     }
     if (join()) return fail(wr, "cpra_files: " + wmsg);
+    return CPRA_B200_OK;
+}
+
+int cpra_b200_conv_files(cpra_b200_ctx* c, const char* a_path, const char* s_path, const char* recon_prefix,
+                         const char* err_prefix, uint64_t total, int iters, double beta) {
+    CTX_OR_RETURN(c);
+    if (!a_path || !s_path || !recon_prefix || !err_prefix) return fail(CPRA_B200_EARG, "conv_files: null pointer");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t vol = c->plane() * c->l, B = c->batch, es = c->esize();
+    // src/CONV_MKL.cpp:108-118: the modulus and support volumes [l][m][n]
+    if ((r = ensure_buffer(c, &c->io_A, &c->io_A_bytes, vol * es, "cudaMalloc(io A)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_S, &c->io_S_bytes, vol * es, "cudaMalloc(io S)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_x, &c->io_x_bytes, B * vol * c->csize(), "cudaMalloc(io x)"))) return r;
+    if ((r = ensure_buffer(c, &c->io_dev, &c->io_dev_bytes, B * vol * es, "cudaMalloc(io)"))) return r;
+    if ((r = cpra_b200_read_matrix(c, a_path, c->io_A, vol, es))) return r;
+    if ((r = cpra_b200_read_matrix(c, s_path, c->io_S, vol, es))) return r;
+    // :119-165: max(batch, total) starts in batches; each start's volume
+    // (real parts) and error to <prefix>.<k>, k counting starts from 1
+    const uint64_t N = std::max<uint64_t>(B, total);
+    const bool with_err = iters >= 1;
+    std::vector<char> err[2] = {std::vector<char>(B * es, 0), std::vector<char>(B * es, 0)};
+    std::thread writer;
+    int wr = CPRA_B200_OK;
+    std::string wmsg;
+    auto join = [&]() {
+        if (writer.joinable()) writer.join();
+        return wr;
+    };
+    uint64_t file_index = 1;
+    int k = 0;
+    for (uint64_t left = N; left > 0; k ^= 1) {
+        const uint64_t n = std::min(left, B);
+        r = cpra_b200_initialize(c, c->io_x, B * vol * 2);
+        if (!r) r = conv_run_impl(c, c->io_x, c->io_A, c->io_S, iters, beta, 1, with_err ? err[k].data() : nullptr);
+        if (join() && !r) r = fail(wr, "conv_files: " + wmsg);
+        if (r) return r;
+        CPRA_CHECK_CUDA(launch_real_starts(c->dbl, c->io_x, c->io_dev, vol, 1, B, 0, n, c->stream), "conv_files");
+        if ((r = io_prepare(c)) || (r = io_after_stream(c))) return r;
+        writer = std::thread([c, n, B, vol, file_index, &err, k, &wr, &wmsg, recon = std::string(recon_prefix),
+                              errp = std::string(err_prefix)]() {
+            wr = write_start_files(c, static_cast<const char*>(c->io_dev), err[k].data(), 1, B, n, vol, recon, errp,
+                                   file_index, wmsg);
+        });
+        file_index += n;
+        left -= n;
+    }
+    if (join()) return fail(wr, "conv_files: " + wmsg);
     return CPRA_B200_OK;
 }
 }  // extern "C"

@@ -163,6 +163,20 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* ctx, void* x, void* t1, void* t2, con
 int cpra_b200_cpra_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S, uint64_t P, uint64_t batch,
                        int epi, int iters, int pre_iter, double beta, int final_step, void* err_host);
 
+/* Extension: the conventional 3D driver ShrinkWrap_CONV_MKL_Sample
+ * (src/CONV_MKL.cpp:10-88) on the context's batch of [l][m][n] volumes x
+ * (device), with one modulus volume A and one support volume S (broadcast
+ * over the batch): t1 = t2 = x, `iters` difference-map iterations with
+ * Forward3D/Backward3D (fused into axis passes for power-of-two volumes, else
+ * the 12 operator calls), and, if final_step != 0, the final projection.  If
+ * err_host is not null it receives the batch's convergence errors of the last
+ * iteration, computed as ConvergeError does (CUDA_Impl.inl:145-172: over the
+ * first m*n elements of each volume); the reference always computes them.
+ * Results are those of the reference's call sequence on this backend.  With
+ * err_host: synchronous; else asynchronous on the context's stream. */
+int cpra_b200_conv_run(cpra_b200_ctx* ctx, void* x, const void* A, const void* S, int iters, double beta,
+                       int final_step, void* err_host);
+
 /* Extension: cpra_b200_cpra_run on HOST buffers (x, A, S laid out as above),
  * the whole ShrinkWrap_CPRA_MKL_Sample call of src/CPRA_MKL.cpp:35-140 with
  * its data in host memory, as the reference's caller holds it.  Angle p's
@@ -220,6 +234,20 @@ int cpra_b200_write_starts(cpra_b200_ctx* ctx, const char* recon_prefix, const c
 int cpra_b200_cpra_files(cpra_b200_ctx* ctx, const char* a_path, const char* s_path, const char* recon_prefix,
                          const char* err_prefix, uint64_t P, uint64_t total, int epi, int iters, int pre_iter,
                          double beta);
+
+/* Extension: the conventional program's main loop (src/CONV_MKL.cpp:103-172)
+ * without its command-line parser: reads the modulus and support volumes
+ * ([l][m][n] T each), then for max(batch, total) starts in batches of the
+ * context's batch size: Initialize the guesses (one call per batch), run
+ * cpra_b200_conv_run (final projection on; errors when iters >= 1, else
+ * zeros), and write for each start k (from 1) <recon_prefix>.<k>, the real
+ * parts of its volume, and <err_prefix>.<k>, its error (one element of T).
+ * The reference writes one file per batch, holding only the batch's last
+ * start, and stores every start's error into a one-element buffer
+ * (:122, 141-146); here every start gets its own files.  Each batch's files
+ * are written by a host thread while the next batch computes.  Synchronous. */
+int cpra_b200_conv_files(cpra_b200_ctx* ctx, const char* a_path, const char* s_path, const char* recon_prefix,
+                         const char* err_prefix, uint64_t total, int iters, double beta);
 
 /* Extension (project-defined, no counterpart in the reference): R-factor of
  * `batch` patterns x ([batch][m][n], the context's plane size) against their

@@ -154,3 +154,39 @@ def test_cpra_files_matches_batches(tb, tmp_path, L, P, B, total, epi, it, pre):
     assert not (tmp_path / f"rec.{n_total + 1}").exists()
     assert not run.cpra_files(tmp_path / "nope.f32", tmp_path / "S.f32", tmp_path / "rec", tmp_path / "err", P,
                               total, epi, it, pre, 0.9)
+
+
+@pytest.mark.parametrize("M,N,L,B,total,iters", [(16, 16, 16, 2, 3, 2), (32, 16, 8, 3, 0, 1)])
+def test_conv_files_matches_batches(tb, tmp_path, M, N, L, B, total, iters):
+    """conv_files (src/CONV_MKL.cpp:103-172 without the parser) writes, for
+    every start of max(batch, total), its volume's real parts and its error,
+    exactly as Initialize + conv_run give them batch by batch."""
+    torch, cb = tb
+    rng = np.random.default_rng(M + N + L + total)
+    vol = M * N * L
+    A = (rng.uniform(0, 40, vol) * (rng.uniform(0, 1, vol) > 0.1)).astype(np.float32)
+    S = (rng.uniform(0, 1, vol) > 0.5).astype(np.float32)
+    A.tofile(tmp_path / "A.f32")
+    S.tofile(tmp_path / "S.f32")
+    run = cb.B200Impl(M, N, L, B)
+    assert run.set_option(cb.OPT_SEED, 5)
+    assert run.conv_files(tmp_path / "A.f32", tmp_path / "S.f32", tmp_path / "rec", tmp_path / "err", total, iters,
+                          0.9)
+    ref = cb.B200Impl(M, N, L, B)
+    assert ref.set_option(cb.OPT_SEED, 5)
+    Ad, Sd = torch.from_numpy(A).cuda(), torch.from_numpy(S).cuda()
+    x = torch.empty(B * vol, dtype=torch.complex64, device="cuda")
+    n_total = max(B, total)
+    done = 0
+    while done < n_total:
+        n = min(B, n_total - done)
+        err = np.zeros(B, np.float32)
+        assert ref.Initialize(torch.view_as_real(x), 2 * x.numel())
+        assert ref.conv_run(x, Ad, Sd, iters, 0.9, final_step=True, err=err) and ref.Sync()
+        xr = x.cpu().numpy().reshape(B, vol)
+        for i in range(n):
+            k = done + i + 1
+            np.testing.assert_array_equal(np.fromfile(tmp_path / f"rec.{k}", np.float32), xr[i].real)
+            np.testing.assert_array_equal(np.fromfile(tmp_path / f"err.{k}", np.float32), err[i:i + 1])
+        done += n
+    assert not (tmp_path / f"rec.{n_total + 1}").exists()

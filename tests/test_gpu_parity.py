@@ -979,6 +979,88 @@ def dm3d_per_call(impl, x, t1, t2, A, S, num, B, beta):
     impl.MergeAddData(t2, x, -1.0 * b, 1.0, num)
 
 
+def conv_driver_per_call(impl, torch, x, A, S, M, N, L, B, iters, beta, err, final):
+    """ShrinkWrap_CONV_MKL_Sample (src/CONV_MKL.cpp:30-88) one interface call
+    at a time, from the guesses already in x."""
+    num = M * N * L * B
+    nbytes = x.numel() * x.element_size()
+    b = float(np.float32(beta)) if x.dtype == torch.complex64 else float(beta)
+    t1, t2, old = (torch.empty_like(x) for _ in range(3))
+    impl.Memcpy(t1, x, nbytes)
+    impl.Memcpy(t2, x, nbytes)
+    for i in range(iters):
+        if err is not None and i == iters - 1:
+            impl.Memcpy(old, x, nbytes)
+        dm3d_per_call(impl, x, t1, t2, A, S, num, B, beta)
+        if err is not None and i == iters - 1:
+            impl.Memcpy(t1, x, nbytes)
+            impl.Forward3D(old)
+            impl.Forward3D(t1)
+            impl.ConvergeError(old, t1, err, M, N, L, B)
+    if final:
+        impl.Memcpy(t1, x, nbytes)
+        impl.Forward3D(t1)
+        impl.DataConstraint(t1, A, num, B)
+        impl.Backward3D(t1)
+        impl.MergeAddData(x, t1, -1.0 / b, 1.0 + 1.0 / b, num)
+        impl.SpaceConstraint(t1, S, num, B)
+        impl.Memcpy(x, t1, nbytes)
+    assert impl.Sync()
+
+
+@pytest.mark.parametrize("T,M,N,L,B,iters,with_err,final",
+                         [(np.float32, 16, 16, 16, 2, 3, True, True), (np.float32, 32, 16, 8, 2, 2, False, True),
+                          (np.float64, 16, 16, 16, 1, 2, True, True), (np.float32, 12, 12, 12, 1, 2, True, True),
+                          (np.float32, 16, 16, 16, 2, 1, True, False), (np.float32, 16, 16, 16, 1, 0, False, True)])
+def test_conv_run_equals_driver(tb, T, M, N, L, B, iters, with_err, final):
+    """cpra_b200_conv_run writes the same bits and errors as the reference's
+    conventional driver issued one call at a time with fusion off, directly
+    and replayed from a CUDA graph; and agrees with the oracle."""
+    torch, cb = tb
+    rng = np.random.default_rng(M * N * L + B + iters)
+    vol = M * N * L
+    cdt = np.complex64 if T == np.float32 else np.complex128
+    dtype = "float32" if T == np.float32 else "float64"
+    amps = (rng.uniform(0, 40, vol) * (rng.uniform(0, 1, vol) > 0.1)).astype(T)
+    sup = (rng.uniform(0, 1, vol) > 0.5).astype(T)
+    x0 = (rng.uniform(0, 1, vol * B) + 1j * rng.uniform(0, 1, vol * B)).astype(cdt)
+    A, S = dev(torch, amps), dev(torch, sup)
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
+    ref.set_option(cb.OPT_FUSION, 0)
+    xr = dev(torch, x0)
+    err_r = np.zeros(B, T) if with_err else None
+    conv_driver_per_call(ref, torch, xr, A, S, M, N, L, B, iters, 0.9, err_r, final)
+    run = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
+    for graph in (0, 1, 1):
+        assert run.set_option(cb.OPT_GRAPH, graph)
+        x = dev(torch, x0)
+        err = np.zeros(B, T) if with_err else None
+        assert run.conv_run(x, A, S, iters, 0.9, final_step=final, err=err) and run.Sync()
+        np.testing.assert_array_equal(host(x), host(xr))
+        if with_err:
+            np.testing.assert_array_equal(err, err_r)
+    # the oracle: the same driver on the FP64/FP32 restatement
+    o = O.OracleImpl(T, M, N, L, B)
+    xo, t1o, t2o = x0.copy(), x0.copy(), x0.copy()
+    bb = float(np.float32(0.9)) if T == np.float32 else 0.9
+    num = vol * B
+    for _ in range(iters):
+        o.Forward3D(t1o); o.DataConstraint(t1o, amps, num, B); o.Backward3D(t1o)
+        o.MergeAddData(xo, t1o, -1.0 / bb, 1.0 + 1.0 / bb, num); o.SpaceConstraint(t1o, sup, num, B)
+        o.SpaceConstraint(t2o, sup, num, B); o.MergeAddData(xo, t2o, 1.0 / bb, 1.0 - 1.0 / bb, num)
+        o.Forward3D(t2o); o.DataConstraint(t2o, amps, num, B); o.Backward3D(t2o)
+        o.MergeAddData(t1o, xo, bb, 1.0, num); o.MergeAddData(t2o, xo, -1.0 * bb, 1.0, num)
+    if final:
+        t1o = xo.copy()
+        o.Forward3D(t1o); o.DataConstraint(t1o, amps, num, B); o.Backward3D(t1o)
+        o.MergeAddData(xo, t1o, -1.0 / bb, 1.0 + 1.0 / bb, num); o.SpaceConstraint(t1o, sup, num, B)
+        xo = t1o
+    tol = (FP32_DM_TOL if T == np.float32 else 1e-12) * max(iters + final, 1)
+    assert O.rel_l2(host(xr), xo) < tol
+    assert not run.conv_run(x, A, S, -1, 0.9)
+    assert not run.conv_run(x, A, S, 0, 0.9, err=np.zeros(B, T))
+
+
 @pytest.mark.parametrize("T,M,N,L,B,iters", [(np.float32, 16, 16, 16, 1, 3), (np.float32, 32, 16, 8, 2, 2),
                                              (np.float64, 16, 16, 16, 1, 2), (np.float32, 12, 12, 12, 1, 2)])
 def test_dm3d_recorder_equals_per_call(tb, T, M, N, L, B, iters):
