@@ -53,8 +53,9 @@ extern "C" {
 #define CPRA_B200_OPT_DATA_MODE 3  /* 0 (default): MKL_Impl.inl:86-106 (A==0 unconstrained); 1: CUDA kernel */
 #define CPRA_B200_OPT_SEED 4       /* seed of cpra_b200_initialize's counter-based stream */
 #define CPRA_B200_OPT_KERNEL_TIMING 5 /* 1: bracket each fused launch with CUDA events (cpra_b200_kernel_timing) */
-#define CPRA_B200_OPT_GRAPH 7      /* 1: cpra_b200_cpra_run and cpra_b200_hio_batched record their launches as a
-                                    CUDA graph per distinct argument set and replay it on repeated calls */
+#define CPRA_B200_OPT_GRAPH 7      /* 1: cpra_b200_cpra_run, cpra_b200_conv_run and cpra_b200_hio_batched record
+                                    their launches as a CUDA graph per distinct argument set and replay it on
+                                    repeated calls */
 #define CPRA_B200_OPT_HIO_CHUNK 6  /* patterns per chunk of the 256/512 HIO line passes (bounds their scratch,
                                     12.125 bytes per pixel); 0 (default): the whole batch */
 #define CPRA_B200_OPT_LANES 8      /* streams of cpra_b200_cpra_run's wavefront schedule: angle p of episode e
