@@ -12,6 +12,7 @@
 //   * other even lengths: a direct O(L^2) DFT pass per axis.
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
+#include "line_pass.cuh"
 #include "ops_ew.cuh"
 
 namespace cpra_b200 {
@@ -124,7 +125,7 @@ template <typename T, int L, int TPL>
 __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ data, uint64_t Bo, uint64_t Bi,
                                                            uint64_t tiles_i, const Cx<T>* __restrict__ twg,
                                                            int inverse, int shift, int out_neg, T scale,
-                                                           int do_scale, AxisOp op) {
+                                                           int do_scale, AxisOp op, int vec) {
     constexpr int LINES = AXIS_THREADS / TPL;
     constexpr int PADL = TPL < 16 ? TPL : 0;
     constexpr int LSX = L + PADL;
@@ -134,7 +135,6 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
     Cx<T>* tw = buf + LINES * LSX;
     const int t = threadIdx.x;
-    F::fill_twiddles(tw, twg, t, AXIS_THREADS);
 
     const uint64_t tile = blockIdx.x;
     const bool contig = (Bi == 1);
@@ -145,23 +145,50 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         o0 = tile / tiles_i;
         i0 = (tile % tiles_i) * LINES;
     }
-    for (int e = t; e < LINES * L; e += AXIS_THREADS) {
-        int l, n;
-        uint64_t gidx;
-        bool ok;
-        if (contig) {
-            l = e / L;
-            n = e % L;
-            ok = (o0 + l) < Bo;
-            gidx = (o0 + l) * (uint64_t)L + n;
-        } else {
-            l = e % LINES;
-            n = e / LINES;
-            ok = (i0 + l) < Bi;
-            gidx = (o0 * L + n) * Bi + i0 + l;
+    // the tile by asynchronous copies, all in flight at once: float pairs of
+    // a contiguous tile in 16 bytes (vec: data 16-byte aligned; an even line
+    // pitch keeps every pair 16-byte aligned in shared memory), otherwise
+    // element by element (a strided tile is transposed into lines); lines
+    // past the end are zero-filled
+    const bool pairs = sizeof(T) == 4 && LSX % 2 == 0 && contig && vec;
+    if (pairs) {
+        for (int e = t; e < LINES * L / 2; e += AXIS_THREADS) {
+            const int l = (2 * e) / L, n = (2 * e) % L;
+            if ((o0 + l) < Bo) {
+                cp_async16(buf + l * LSX + n, data + (o0 + l) * (uint64_t)L + n);
+            } else {
+                buf[l * LSX + n] = Cx<T>{T(0), T(0)};
+                buf[l * LSX + n + 1] = Cx<T>{T(0), T(0)};
+            }
         }
-        buf[l * LSX + n] = ok ? data[gidx] : Cx<T>{T(0), T(0)};
+    } else {
+        for (int e = t; e < LINES * L; e += AXIS_THREADS) {
+            int l, n;
+            uint64_t gidx;
+            bool ok;
+            if (contig) {
+                l = e / L;
+                n = e % L;
+                ok = (o0 + l) < Bo;
+                gidx = (o0 + l) * (uint64_t)L + n;
+            } else {
+                l = e % LINES;
+                n = e / LINES;
+                ok = (i0 + l) < Bi;
+                gidx = (o0 * L + n) * Bi + i0 + l;
+            }
+            if (!ok) {
+                buf[l * LSX + n] = Cx<T>{T(0), T(0)};
+            } else if constexpr (sizeof(T) == 8) {
+                cp_async16(buf + l * LSX + n, data + gidx);
+            } else {
+                cp_async8(buf + l * LSX + n, data + gidx);
+            }
+        }
     }
+    cp_async_commit();
+    F::fill_twiddles(tw, twg, t, AXIS_THREADS);
+    cp_async_wait<0>();
     __syncthreads();
 
     const int line = t / TPL, q = t % TPL;
@@ -230,6 +257,15 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         buf[line * LSX + f] = w;
     }
     __syncthreads();
+    if (pairs) {
+        for (int e = t; e < LINES * L / 2; e += AXIS_THREADS) {
+            const int l = (2 * e) / L, n = (2 * e) % L;
+            if ((o0 + l) < Bo)
+                *reinterpret_cast<float4*>(data + (o0 + l) * (uint64_t)L + n) =
+                    *reinterpret_cast<const float4*>(buf + l * LSX + n);
+        }
+        return;
+    }
     for (int e = t; e < LINES * L; e += AXIS_THREADS) {
         int l, n;
         uint64_t gidx;
@@ -267,8 +303,9 @@ cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shi
     }
     if (tiles == 0) return cudaSuccess;
     if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+    const int vec = (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
     kf<<<(unsigned)tiles, AXIS_THREADS, smem, st>>>((Cx<T>*)x, Bo, Bi, tiles_i, (const Cx<T>*)tw, inverse ? 1 : 0,
-                                                    shift ? 1 : 0, out_neg, scale, do_scale ? 1 : 0, op);
+                                                    shift ? 1 : 0, out_neg, scale, do_scale ? 1 : 0, op, vec);
     count_launches();
     return cudaGetLastError();
 }
