@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
-    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d"], default="carousel",
-                    help="uneven / carousel3d: only that side measurement (one JSON line, for profiling runs)")
+    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d"], default="carousel",
+                    help="uneven / carousel3d / fft3d: only that side measurement (one JSON line, for profiling "
+                         "runs)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
     # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
@@ -348,6 +349,11 @@ def main():
                                  B=a.starts, epi=a.episodes, iters=a.iters, refine_steps=a.refine_steps,
                                  step_deg=a.angle_step, photons=a.photons, ellipsoids=a.ellipsoids,
                                  axes=tuple(float(v) for v in a.axes.split(",")))
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+    if a.case == "fft3d":
+        out = fft3d_ops(torch, cpra_b200, torch.device("cuda", local), n=a.size, reps=a.steps)
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -740,6 +746,47 @@ def plain2d(torch, cpra_b200, dev, B=16, n=128, iters=200, sw_every=20, reps=3):
 
 UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns): 512 patterns, 18,612,224 pixels
 HIO_BYTES_PER_PIXEL = 24  # read+write x (complex64) + read A, S (float32) per HIO pattern-iteration
+
+
+def fft3d_ops(torch, cpra_b200, dev, n=128, reps=5):
+    """The 3D operators on one n^3 complex64 volume: Forward3D (three axis
+    passes), Backward3D, and one fused iteration of the benchmark's 3D step
+    (constraint3d, five passes) and of the conventional difference map
+    (conv_run with one iteration: ten passes and the two start copies
+    t1 = t2 = x), each timed with CUDA events on the context's stream over
+    `reps` calls after warm-up.  Bytes are counted as 16 per voxel per pass
+    or copy (read and write)."""
+    impl = cpra_b200.B200Impl(n, n, n, 1)
+    st = torch.cuda.ExternalStream(impl.stream(), device=dev)
+    g = torch.Generator(device=dev).manual_seed(n)
+    vol = n ** 3
+    x = torch.rand(vol, dtype=torch.complex64, device=dev, generator=g)
+    C = torch.rand(vol, dtype=torch.complex64, device=dev, generator=g)
+    A = torch.rand(vol, device=dev, generator=g) * 10
+    S = (torch.rand(vol, device=dev, generator=g) > 0.5).float()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        impl.Sync()
+        ev[0].record(st)
+        for _ in range(reps):
+            fn()
+        ev[1].record(st)
+        impl.Sync()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    peak, peak_kind = measured_peak()
+    out = {"case": "fft3d", "volume": [n, n, n], "reps": reps, "peak_gbs": peak, "peak_kind": peak_kind}
+    for name, fn, passes in (("forward3d", lambda: impl.Forward3D(x), 3),
+                             ("backward3d", lambda: impl.Backward3D(x), 3),
+                             ("constraint3d_iteration", lambda: impl.constraint3d(x, C, S, 1), 5),
+                             ("conv_run_iteration", lambda: impl.conv_run(x, A, S, 1, 0.9, final_step=False), 12)):
+        ms = timed(fn)
+        gbs = passes * 16 * vol / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "axis_passes": passes, "gbs": gbs, "frac": gbs / peak}
+    return out
 
 
 def uneven_batch(torch, cpra_b200, dev, iters=100, sw_every=20, reps=2, sizes=UNEVEN_SIZES, per_op=True):
