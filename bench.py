@@ -779,10 +779,14 @@ def fft3d_ops(torch, cpra_b200, dev, n=128, reps=5):
 
     peak, peak_kind = measured_peak()
     out = {"case": "fft3d", "volume": [n, n, n], "reps": reps, "peak_gbs": peak, "peak_kind": peak_kind}
-    for name, fn, passes in (("forward3d", lambda: impl.Forward3D(x), 3),
-                             ("backward3d", lambda: impl.Backward3D(x), 3),
-                             ("constraint3d_iteration", lambda: impl.constraint3d(x, C, S, 1), 5),
-                             ("conv_run_iteration", lambda: impl.conv_run(x, A, S, 1, 0.9, final_step=False), 12)):
+    # the transforms alone are timed with fusion off: with it on, a Forward3D
+    # is held back (it may start a difference-map iteration) until the next call
+    for name, fn, passes, fusion in (("forward3d", lambda: impl.Forward3D(x), 3, 0),
+                                     ("backward3d", lambda: impl.Backward3D(x), 3, 0),
+                                     ("constraint3d_iteration", lambda: impl.constraint3d(x, C, S, 1), 5, 1),
+                                     ("conv_run_iteration",
+                                      lambda: impl.conv_run(x, A, S, 1, 0.9, final_step=False), 12, 1)):
+        impl.set_option(cpra_b200.OPT_FUSION, fusion)
         ms = timed(fn)
         gbs = passes * 16 * vol / (ms / 1e3) / 1e9
         out[name] = {"ms": ms, "axis_passes": passes, "gbs": gbs, "frac": gbs / peak}

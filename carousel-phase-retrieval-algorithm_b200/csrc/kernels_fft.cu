@@ -121,23 +121,44 @@ struct AxisOp {
     double a = 0.0, b = 0.0, a2 = 0.0, b2 = 0.0;  // merge coefficients (rounded to T by the caller)
 };
 
-template <typename T, int L, int TPL>
+// Shared tile of an axis pass: AXIS_THREADS / TPL lines of L elements.
+// Contiguous axes keep lines as rows of pitch LSX (TPL < 16: padded by TPL so
+// the lines of a half-warp fall on distinct bank pairs); strided axes keep
+// them as columns of pitch CSX (odd, or 4 mod 16 at TPL = 4), which keeps the
+// staging copies, the natural-order loads, the exchange and the outputs on
+// distinct bank pairs at every length but 512 and 1024 (2-way there).
+template <int L, int TPL>
+struct AxisTile {
+    static constexpr int LINES = AXIS_THREADS / TPL;
+    static constexpr int LSX = L + (TPL < 16 ? TPL : 0);
+    static constexpr int CSX = (TPL == 4) ? LINES + 4 : LINES + 1;
+    static constexpr int ELEMS = (LINES * LSX > L * CSX) ? LINES * LSX : L * CSX;
+};
+
+// PLAIN: no fused operation (op.kind == AXIS_PLAIN), compiled without its branches
+template <typename T, int L, int TPL, bool PLAIN>
 __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ data, uint64_t Bo, uint64_t Bi,
                                                            uint64_t tiles_i, const Cx<T>* __restrict__ twg,
                                                            int inverse, int shift, int out_neg, T scale,
                                                            int do_scale, AxisOp op, int vec) {
     constexpr int LINES = AXIS_THREADS / TPL;
-    constexpr int PADL = TPL < 16 ? TPL : 0;
-    constexpr int LSX = L + PADL;
     constexpr int R = L / TPL;
-        using F = LineFFT<T, L, TPL>;
+    using F = LineFFT<T, L, TPL>;
+    using G = AxisTile<L, TPL>;
+    constexpr int LSX = G::LSX, CSX = G::CSX;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
-    Cx<T>* tw = buf + LINES * LSX;
+    Cx<T>* tw = buf + G::ELEMS;
     const int t = threadIdx.x;
+    const Cx<T> zero = {T(0), T(0)};
 
     const uint64_t tile = blockIdx.x;
     const bool contig = (Bi == 1);
+    // element n of line l: rows [l][n] (pitch LSX) for a contiguous axis,
+    // columns [n][l] (pitch CSX) for a strided one, so that the staging copies
+    // (consecutive lines of one n) and the transforms both stay conflict-free
+    auto slot = [&](int l, int n) { return contig ? l * LSX + n : n * CSX + l; };
+    const int ss = contig ? 1 : CSX;  // slot stride along a line
     uint64_t o0 = 0, i0 = 0;
     if (contig) {
         o0 = tile * LINES;
@@ -145,6 +166,20 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         o0 = tile / tiles_i;
         i0 = (tile % tiles_i) * LINES;
     }
+    // Staging and write-back walk the tile in steps of AXIS_THREADS elements.
+    // Contiguous tiles: element e of the tile is global o0 * L + e.  Strided
+    // tiles: a thread keeps one line sl = t % LINES and visits n = sn + TPL j,
+    // so its global address advances by TPL * Bi per step.
+    const uint64_t g0 = o0 * (uint64_t)L;
+    const int sl = t % LINES, sn = t / LINES;
+    const bool sl_ok = (i0 + sl) < Bi;
+    const uint64_t sg = (o0 * L + sn) * Bi + i0 + sl, gstep = (uint64_t)TPL * Bi;
+    auto copy_in = [&](Cx<T>* d, const Cx<T>* src) {
+        if constexpr (sizeof(T) == 8)
+            cp_async16(d, src);
+        else
+            cp_async8(d, src);
+    };
     // the tile by asynchronous copies, all in flight at once: float pairs of
     // a contiguous tile in 16 bytes (vec: data 16-byte aligned; an even line
     // pitch keeps every pair 16-byte aligned in shared memory), otherwise
@@ -155,36 +190,27 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         for (int e = t; e < LINES * L / 2; e += AXIS_THREADS) {
             const int l = (2 * e) / L, n = (2 * e) % L;
             if ((o0 + l) < Bo) {
-                cp_async16(buf + l * LSX + n, data + (o0 + l) * (uint64_t)L + n);
+                cp_async16(buf + l * LSX + n, data + g0 + 2 * e);
             } else {
-                buf[l * LSX + n] = Cx<T>{T(0), T(0)};
-                buf[l * LSX + n + 1] = Cx<T>{T(0), T(0)};
+                buf[l * LSX + n] = zero;
+                buf[l * LSX + n + 1] = zero;
             }
         }
-    } else {
+    } else if (contig) {
         for (int e = t; e < LINES * L; e += AXIS_THREADS) {
-            int l, n;
-            uint64_t gidx;
-            bool ok;
-            if (contig) {
-                l = e / L;
-                n = e % L;
-                ok = (o0 + l) < Bo;
-                gidx = (o0 + l) * (uint64_t)L + n;
-            } else {
-                l = e % LINES;
-                n = e / LINES;
-                ok = (i0 + l) < Bi;
-                gidx = (o0 * L + n) * Bi + i0 + l;
-            }
-            if (!ok) {
-                buf[l * LSX + n] = Cx<T>{T(0), T(0)};
-            } else if constexpr (sizeof(T) == 8) {
-                cp_async16(buf + l * LSX + n, data + gidx);
-            } else {
-                cp_async8(buf + l * LSX + n, data + gidx);
-            }
+            const int l = e / L, n = e % L;
+            if ((o0 + l) < Bo)
+                copy_in(buf + l * LSX + n, data + g0 + e);
+            else
+                buf[l * LSX + n] = zero;
         }
+    } else if (sl_ok) {
+        const Cx<T>* src = data + sg;
+        Cx<T>* d = buf + sn * CSX + sl;
+#pragma unroll 4
+        for (int j = 0; j < R; ++j, src += gstep, d += TPL * CSX) copy_in(d, src);
+    } else {
+        for (int j = 0; j < R; ++j) buf[(sn + TPL * j) * CSX + sl] = zero;
     }
     cp_async_commit();
     F::fill_twiddles(tw, twg, t, AXIS_THREADS);
@@ -197,42 +223,48 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
     auto gindex = [&](int n) -> uint64_t {
         return contig ? (o0 + line) * (uint64_t)L + n : (o0 * L + n) * Bi + i0 + line;
     };
+    Cx<T>* lb = buf + slot(line, 0);  // this line's slots, stride ss
     Cx<T> v[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int n = q + TPL * k;
-        v[k] = buf[line * LSX + n];
-        if (op.kind == AXIS_T2_PROLOGUE && line_ok) {
-            const uint64_t gi = gindex(n);
-            const T sv = static_cast<const T*>(op.aux)[gi % op.aux_plane];
-            v[k] = merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], space_apply(v[k], sv, op.space_mode),
-                               (T)op.a, (T)op.b);
+        v[k] = lb[n * ss];
+        if constexpr (!PLAIN) {
+            if (op.kind == AXIS_T2_PROLOGUE && line_ok) {
+                const uint64_t gi = gindex(n);
+                const T sv = static_cast<const T*>(op.aux)[gi % op.aux_plane];
+                v[k] = merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], space_apply(v[k], sv, op.space_mode),
+                                   (T)op.a, (T)op.b);
+            }
         }
         if (shift) v[k] = csign(v[k], n);
     }
     Cx<T> o[R];
     if (inverse)
-        F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
+        F::template natural_to_split_flat<true>(v, o, lb, ss, tw, q);
     else
-        F::template natural_to_split_flat<false>(v, o, buf + line * LSX, 1, tw, q);
-    if (op.kind == AXIS_DC_ROUNDTRIP || op.kind == AXIS_DCR_ROUNDTRIP) {
+        F::template natural_to_split_flat<false>(v, o, lb, ss, tw, q);
+    if constexpr (!PLAIN) {
+        if (op.kind == AXIS_DC_ROUNDTRIP || op.kind == AXIS_DCR_ROUNDTRIP) {
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
-            const int f = F::pos(q, i);
-            Cx<T> w = o[i];
-            if (shift) w = csign(w, f + out_neg);
-            if (line_ok) {
-                const uint64_t ai = gindex(f) % op.aux_plane;
-                w = (op.kind == AXIS_DC_ROUNDTRIP) ? data_apply_complex(w, static_cast<const Cx<T>*>(op.aux)[ai])
-                                                   : data_apply(w, static_cast<const T*>(op.aux)[ai], op.data_mode);
+            for (int i = 0; i < R; ++i) {
+                const int f = F::pos(q, i);
+                Cx<T> w = o[i];
+                if (shift) w = csign(w, f + out_neg);
+                if (line_ok) {
+                    const uint64_t ai = gindex(f) % op.aux_plane;
+                    w = (op.kind == AXIS_DC_ROUNDTRIP)
+                            ? data_apply_complex(w, static_cast<const Cx<T>*>(op.aux)[ai])
+                            : data_apply(w, static_cast<const T*>(op.aux)[ai], op.data_mode);
+                }
+                if (shift) w = csign(w, f);  // the inverse pass's input flip
+                lb[f * ss] = w;
             }
-            if (shift) w = csign(w, f);  // the inverse pass's input flip
-            buf[line * LSX + f] = w;
-        }
-        __syncwarp();
+            __syncwarp();
 #pragma unroll
-        for (int k = 0; k < R; ++k) v[k] = buf[line * LSX + q + TPL * k];
-        F::template natural_to_split_flat<true>(v, o, buf + line * LSX, 1, tw, q);
+            for (int k = 0; k < R; ++k) v[k] = lb[(q + TPL * k) * ss];
+            F::template natural_to_split_flat<true>(v, o, lb, ss, tw, q);
+        }
     }
 #pragma unroll
     for (int i = 0; i < R; ++i) {
@@ -240,48 +272,42 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         Cx<T> w = o[i];
         if (do_scale) w = cscale(w, scale);
         if (shift) w = csign(w, f + out_neg);
-        if (line_ok) {
-            if (op.kind == AXIS_SPACE) {
-                w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
-            } else if (op.kind == AXIS_T1_EPILOGUE) {
-                const uint64_t gi = gindex(f);
-                w = space_apply(merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], w, (T)op.a, (T)op.b),
-                                static_cast<const T*>(op.aux)[gi % op.aux_plane], op.space_mode);
-            } else if (op.kind == AXIS_X_EPILOGUE) {
-                const uint64_t gi = gindex(f);
-                Cx<T>* X = static_cast<Cx<T>*>(op.x_in);
-                const Cx<T> x1 = merge_apply(static_cast<const Cx<T>*>(op.t1_in)[gi], X[gi], (T)op.a, (T)op.b);
-                X[gi] = merge_apply(w, x1, (T)op.a2, (T)op.b2);
+        if constexpr (!PLAIN) {
+            if (line_ok) {
+                if (op.kind == AXIS_SPACE) {
+                    w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
+                } else if (op.kind == AXIS_T1_EPILOGUE) {
+                    const uint64_t gi = gindex(f);
+                    w = space_apply(merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], w, (T)op.a, (T)op.b),
+                                    static_cast<const T*>(op.aux)[gi % op.aux_plane], op.space_mode);
+                } else if (op.kind == AXIS_X_EPILOGUE) {
+                    const uint64_t gi = gindex(f);
+                    Cx<T>* X = static_cast<Cx<T>*>(op.x_in);
+                    const Cx<T> x1 =
+                        merge_apply(static_cast<const Cx<T>*>(op.t1_in)[gi], X[gi], (T)op.a, (T)op.b);
+                    X[gi] = merge_apply(w, x1, (T)op.a2, (T)op.b2);
+                }
             }
         }
-        buf[line * LSX + f] = w;
+        lb[f * ss] = w;
     }
     __syncthreads();
     if (pairs) {
         for (int e = t; e < LINES * L / 2; e += AXIS_THREADS) {
             const int l = (2 * e) / L, n = (2 * e) % L;
             if ((o0 + l) < Bo)
-                *reinterpret_cast<float4*>(data + (o0 + l) * (uint64_t)L + n) =
-                    *reinterpret_cast<const float4*>(buf + l * LSX + n);
+                *reinterpret_cast<float4*>(data + g0 + 2 * e) = *reinterpret_cast<const float4*>(buf + l * LSX + n);
         }
-        return;
-    }
-    for (int e = t; e < LINES * L; e += AXIS_THREADS) {
-        int l, n;
-        uint64_t gidx;
-        bool ok;
-        if (contig) {
-            l = e / L;
-            n = e % L;
-            ok = (o0 + l) < Bo;
-            gidx = (o0 + l) * (uint64_t)L + n;
-        } else {
-            l = e % LINES;
-            n = e / LINES;
-            ok = (i0 + l) < Bi;
-            gidx = (o0 * L + n) * Bi + i0 + l;
+    } else if (contig) {
+        for (int e = t; e < LINES * L; e += AXIS_THREADS) {
+            const int l = e / L, n = e % L;
+            if ((o0 + l) < Bo) data[g0 + e] = buf[l * LSX + n];
         }
-        if (ok) data[gidx] = buf[l * LSX + n];
+    } else if (sl_ok) {
+        Cx<T>* dst = data + sg;
+        const Cx<T>* s = buf + sn * CSX + sl;
+#pragma unroll 4
+        for (int j = 0; j < R; ++j, dst += gstep, s += TPL * CSX) *dst = *s;
     }
 }
 
@@ -289,9 +315,8 @@ template <typename T, int L, int TPL>
 cudaError_t axis_fft_t(void* x, uint64_t Bo, uint64_t Bi, bool inverse, bool shift, int out_neg, T scale,
                        bool do_scale, const void* tw, cudaStream_t st, AxisOp op = AxisOp{}) {
     constexpr int LINES = AXIS_THREADS / TPL;
-    constexpr int PADL = TPL < 16 ? TPL : 0;
-    const size_t smem = sizeof(Cx<T>) * ((size_t)LINES * (L + PADL) + LineFFT<T, L, TPL>::TW_ENTRIES);
-    auto kf = k_axis_fft<T, L, TPL>;
+    const size_t smem = sizeof(Cx<T>) * ((size_t)AxisTile<L, TPL>::ELEMS + LineFFT<T, L, TPL>::TW_ENTRIES);
+    auto kf = (op.kind == AXIS_PLAIN) ? k_axis_fft<T, L, TPL, true> : k_axis_fft<T, L, TPL, false>;
     cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     uint64_t tiles_i = 1, tiles;
