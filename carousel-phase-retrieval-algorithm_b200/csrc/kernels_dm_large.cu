@@ -131,8 +131,8 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_first(const DmlDev p) {
 }
 
 // a tile of column lines of one plane (2 per pattern): forward column DFT,
-// DataConstraint with the pattern's A, inverse column DFT, in place
-template <int L>
+// DataConstraint with the pattern's A (mode DMODE), inverse column DFT, in place
+template <int L, int DMODE>
 __global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_cols(const DmlDev p) {
     using B = DmLP<L>;
     constexpr int CS = B::CS, AS = B::AS, LN = B::CL, NT = B::NT;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(DmLP<L>::NT, 3) k_dml_cols(const DmlDev p) {
 #pragma unroll
     for (int i = 0; i < B::R; ++i) {
         const int f = B::pos(q, i);
-        col[f * CS] = data_apply(o[i], As[f * AS + line], p.data_mode);
+        col[f * CS] = data_apply(o[i], As[f * AS + line], DMODE);
     }
     __syncwarp();
 #pragma unroll
@@ -267,7 +267,9 @@ cudaError_t dml_launch(const DmArgs& a, const void* tw, void* Y, uint32_t* mask,
                                   (int)B::row_smem())) != cudaSuccess ||
         (e = cudaFuncSetAttribute(k_dml_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)B::row_smem())) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(k_dml_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (e = cudaFuncSetAttribute(k_dml_cols<L, DATA_SKIP_ZERO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)B::col_smem())) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_dml_cols<L, DATA_ALWAYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)B::col_smem())) != cudaSuccess)
         return e;
     const uint64_t plane = (uint64_t)L * L;
@@ -303,7 +305,10 @@ cudaError_t dml_launch(const DmArgs& a, const void* tw, void* Y, uint32_t* mask,
     const unsigned col_ctas = (unsigned)(2 * a.batch * (L / B::CL));
     k_dml_first<L><<<row_ctas, B::NT, B::row_smem(), st>>>(d);
     for (int it = 0; it < a.iters; ++it) {
-        k_dml_cols<L><<<col_ctas, B::NT, B::col_smem(), st>>>(d);
+        if (a.data_mode == DATA_ALWAYS)
+            k_dml_cols<L, DATA_ALWAYS><<<col_ctas, B::NT, B::col_smem(), st>>>(d);
+        else
+            k_dml_cols<L, DATA_SKIP_ZERO><<<col_ctas, B::NT, B::col_smem(), st>>>(d);
         k_dml_rows<L><<<row_ctas, B::NT, B::row_smem(), st>>>(d, it + 1 == a.iters ? 1 : 0);
     }
     count_launches(2 + 2 * (uint64_t)a.iters);

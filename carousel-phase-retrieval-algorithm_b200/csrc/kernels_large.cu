@@ -120,11 +120,12 @@ __global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_rows_fwd(const
 // op 0: modulus projection with A (pattern b's plane at A + b * a_stride;
 // vec_a: its rows 16-byte aligned); op 1: multiply by gt[f] * gt[c] (and zero
 // vmax[0..nzero) for the blur pass)
-template <int L>
+template <int L, int OP, int DMODE>
 __global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_cols(Cx<float>* __restrict__ Y, const float* __restrict__ A,
                                                             uint64_t a_stride, const float* __restrict__ gtab,
-                                                            const Cx<float>* __restrict__ twg, int op, int data_mode,
+                                                            const Cx<float>* __restrict__ twg,
                                                             unsigned int* __restrict__ vzero, int nzero, int vec_a) {
+    constexpr int op = OP;
     using B = Big<L>;
     constexpr int CS = B::CS, AS = B::AS, LN = B::CL, NT = B::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -157,7 +158,10 @@ __global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_cols(Cx<float>
 #pragma unroll
     for (int i = 0; i < B::R; ++i) {
         const int f = B::pos(q, i);
-        o[i] = (op == 0) ? data_apply(o[i], As[f * AS + line], data_mode) : cscale(o[i], gt[f] * gt[c]);
+        if constexpr (OP == 0)
+            o[i] = data_apply(o[i], As[f * AS + line], DMODE);
+        else
+            o[i] = cscale(o[i], gt[f] * gt[c]);
     }
     if constexpr (!B::F::HALF) {
         // split layout in registers: the inverse runs straight from it
@@ -190,12 +194,13 @@ enum RowsMode : int { ROWS_HIO = 0, ROWS_HIO_NEXT = 1, ROWS_HIO_MAG = 2, ROWS_BL
 //   ROWS_ESTIMATE: x <- y inside the support, 0 elsewhere
 // Y's rows arrive by asynchronous copy first, x's and the support mask's
 // while the inverse transform runs.  vec_x: x rows 16-byte aligned.
-template <int L>
+template <int L, int MODE>
 __global__ void __launch_bounds__(Big<L>::NT, Big<L>::MINB) k_big_rows(Cx<float>* __restrict__ Y, Cx<float>* __restrict__ x,
                                                             const uint32_t* __restrict__ mask,
                                                             float* __restrict__ vout, unsigned int* __restrict__ vmax,
                                                             const Cx<float>* __restrict__ twg, float scale, float beta,
-                                                            int positivity, int mode, int vec_x) {
+                                                            int positivity, int vec_x) {
+    constexpr int mode = MODE;
     using B = Big<L>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<float>* Yt = reinterpret_cast<Cx<float>*>(smem_raw);
@@ -316,10 +321,17 @@ cudaError_t big_set_smem() {
     if ((e = cudaFuncSetAttribute(k_big_rows_fwd<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)B::row_smem())) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(k_big_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)B::row_smem())) != cudaSuccess)
+    for (auto k : {k_big_rows<L, ROWS_HIO>, k_big_rows<L, ROWS_HIO_NEXT>, k_big_rows<L, ROWS_HIO_MAG>,
+                   k_big_rows<L, ROWS_BLUR>, k_big_rows<L, ROWS_ESTIMATE>})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::row_smem())) !=
+            cudaSuccess)
+            return e;
+    if ((e = cudaFuncSetAttribute(k_big_cols<L, 0, DATA_SKIP_ZERO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)B::col_smem())) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_big_cols<L, 0, DATA_ALWAYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)B::col_smem())) != cudaSuccess)
         return e;
-    return cudaFuncSetAttribute(k_big_cols<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::col_smem());
+    return cudaFuncSetAttribute(k_big_cols<L, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::col_smem());
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -345,10 +357,34 @@ cudaError_t big_chunk(const HioArgs& a, uint64_t b0, uint64_t nb, const Cx<float
     const float scale = 1.0f / (float)plane, beta = (float)a.beta, thr = (float)a.threshold;
     const bool est = a.estimate != nullptr;
     auto cols = [&](int op, const float* gtab, unsigned int* vz) {
-        k_big_cols<L><<<col_ctas, NT, cs, st>>>(Y, A, a.a_stride, gtab, tw, op, a.data_mode, vz, (int)nb, va);
+        if (op == 1)
+            k_big_cols<L, 1, 0><<<col_ctas, NT, cs, st>>>(Y, A, a.a_stride, gtab, tw, vz, (int)nb, va);
+        else if (a.data_mode == DATA_ALWAYS)
+            k_big_cols<L, 0, DATA_ALWAYS><<<col_ctas, NT, cs, st>>>(Y, A, a.a_stride, gtab, tw, vz, (int)nb, va);
+        else
+            k_big_cols<L, 0, DATA_SKIP_ZERO><<<col_ctas, NT, cs, st>>>(Y, A, a.a_stride, gtab, tw, vz, (int)nb, va);
     };
     auto rows = [&](Cx<float>* dst, int mode, int pos, int vdst) {
-        k_big_rows<L><<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, mode, vdst);
+        switch (mode) {
+            case ROWS_HIO:
+                k_big_rows<L, ROWS_HIO><<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, vdst);
+                break;
+            case ROWS_HIO_NEXT:
+                k_big_rows<L, ROWS_HIO_NEXT>
+                    <<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, vdst);
+                break;
+            case ROWS_HIO_MAG:
+                k_big_rows<L, ROWS_HIO_MAG>
+                    <<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, vdst);
+                break;
+            case ROWS_BLUR:
+                k_big_rows<L, ROWS_BLUR><<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, vdst);
+                break;
+            default:
+                k_big_rows<L, ROWS_ESTIMATE>
+                    <<<row_ctas, NT, rs, st>>>(Y, dst, mask, V, vmax, tw, scale, beta, pos, vdst);
+                break;
+        }
     };
     k_big_pack<<<ew, 256, 0, st>>>(S, a.s_stride, plane, nb, mask);
     k_big_rows_fwd<L><<<row_ctas, NT, rs, st>>>(x, Y, tw, nullptr, nullptr, mask, thr, vx);

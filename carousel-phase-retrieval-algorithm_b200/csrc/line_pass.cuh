@@ -97,52 +97,59 @@ __device__ __forceinline__ void stage(void* dst, const void* src, uint32_t bytes
 // A column tile: rows n < L of LN consecutive complex at src + n * ld into
 // dst + n * CS (16-byte copies when CS is even, 8-byte copies otherwise), and
 // optionally LN floats per row of A at a + n * ld into as + n * AS (16-byte
-// copies when `avec` and AS % 4 == 0, else 4-byte copies).
+// copies when `avec` and AS % 4 == 0, else 4-byte copies).  `nt` (the CTA's
+// threads) is a multiple of the chunks per row, so every thread keeps one
+// chunk position k of a row and walks the rows n = t / chunks + (nt / chunks) j
+// by pointer steps.
 template <int L, int LN, int CS, int AS>
 __device__ __forceinline__ void stage_col_tile(Cx<float>* dst, const Cx<float>* src, float* as, const float* a,
                                                uint64_t ld, bool avec, int t, int nt) {
-    if constexpr (CS % 2 == 0) {
-        constexpr int CH = LN / 2;
-        for (int i = t; i < L * CH; i += nt) {
-            const int n = i / CH, k = i % CH;
-            cp_async16(dst + n * CS + 2 * k, src + (uint64_t)n * ld + 2 * k);
-        }
-    } else {
-        for (int i = t; i < L * LN; i += nt) {
-            const int n = i / LN, k = i % LN;
-            cp_async8(dst + n * CS + k, src + (uint64_t)n * ld + k);
+    constexpr int W = (CS % 2 == 0) ? 2 : 1;  // complex per copy
+    constexpr int CH = LN / W;
+    {
+        const int k = t % CH, n0 = t / CH, step = nt / CH;
+        const Cx<float>* s = src + (uint64_t)n0 * ld + W * k;
+        Cx<float>* d = dst + n0 * CS + W * k;
+        const uint64_t sstep = (uint64_t)step * ld;
+        for (int n = n0; n < L; n += step, s += sstep, d += step * CS) {
+            if constexpr (W == 2)
+                cp_async16(d, s);
+            else
+                cp_async8(d, s);
         }
     }
     if (!a) return;
     if (AS % 4 == 0 && avec) {
-        constexpr int CH = LN / 4;
-        for (int i = t; i < L * CH; i += nt) {
-            const int n = i / CH, k = i % CH;
-            cp_async16(as + n * AS + 4 * k, a + (uint64_t)n * ld + 4 * k);
-        }
+        constexpr int CA = LN / 4;
+        const int k = t % CA, n0 = t / CA, step = nt / CA;
+        const float* s = a + (uint64_t)n0 * ld + 4 * k;
+        float* d = as + n0 * AS + 4 * k;
+        const uint64_t sstep = (uint64_t)step * ld;
+        for (int n = n0; n < L; n += step, s += sstep, d += step * AS) cp_async16(d, s);
     } else {
-        for (int i = t; i < L * LN; i += nt) {
-            const int n = i / LN, k = i % LN;
-            cp_async4(as + n * AS + k, a + (uint64_t)n * ld + k);
-        }
+        const int k = t % LN, n0 = t / LN, step = nt / LN;
+        const float* s = a + (uint64_t)n0 * ld + k;
+        float* d = as + n0 * AS + k;
+        const uint64_t sstep = (uint64_t)step * ld;
+        for (int n = n0; n < L; n += step, s += sstep, d += step * AS) cp_async4(d, s);
     }
 }
 
-// the tile back: rows of LN complex from src + n * CS to dst + n * ld
+// the tile back: rows of LN complex from src + n * CS to dst + n * ld, by the
+// same per-thread walk
 template <int L, int LN, int CS>
 __device__ __forceinline__ void store_col_tile(Cx<float>* dst, const Cx<float>* src, uint64_t ld, int t, int nt) {
-    if constexpr (CS % 2 == 0) {
-        constexpr int CH = LN / 2;
-        for (int i = t; i < L * CH; i += nt) {
-            const int n = i / CH, k = i % CH;
-            *reinterpret_cast<float4*>(dst + (uint64_t)n * ld + 2 * k) =
-                *reinterpret_cast<const float4*>(src + n * CS + 2 * k);
-        }
-    } else {
-        for (int i = t; i < L * LN; i += nt) {
-            const int n = i / LN, k = i % LN;
-            dst[(uint64_t)n * ld + k] = src[n * CS + k];
-        }
+    constexpr int W = (CS % 2 == 0) ? 2 : 1;
+    constexpr int CH = LN / W;
+    const int k = t % CH, n0 = t / CH, step = nt / CH;
+    Cx<float>* d = dst + (uint64_t)n0 * ld + W * k;
+    const Cx<float>* s = src + n0 * CS + W * k;
+    const uint64_t dstep = (uint64_t)step * ld;
+    for (int n = n0; n < L; n += step, d += dstep, s += step * CS) {
+        if constexpr (W == 2)
+            *reinterpret_cast<float4*>(d) = *reinterpret_cast<const float4*>(s);
+        else
+            *d = *s;
     }
 }
 
