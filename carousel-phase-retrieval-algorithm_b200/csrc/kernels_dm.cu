@@ -11,8 +11,12 @@
 // writes its row in the same split positions (fft2d_cta.cuh), so the value a
 // thread produces for t1 is the value it consumes next.  Only x and t2 travel
 // through global memory (L2): the second half of each iteration already forms
-// the next iteration's a2*x + b2*S(t2), so each iteration reads x twice and
-// that one plane, and writes x and t2 once.  The fftshifts cancel in pairs
+// the next iteration's a2*x + b2*S(t2), so each iteration reads that one
+// plane and x, and writes x and t2 once.  The first half's update needs x a
+// second time; half of those values come from registers (the new x the
+// previous iteration left there, carried through the transforms in t1's
+// registers, which are free in that half), the other half from L2, loaded
+// together with the second half's t2.  The fftshifts cancel in pairs
 // around the modulus step (DataConstraint commutes with the (-1)^(i+j) sign
 // pattern), leaving sign flips on the input of each forward and the output of
 // each inverse transform.
@@ -62,10 +66,10 @@ struct DmPlan {
 
 __device__ __forceinline__ bool mask_keep(const uint32_t* mask, int idx) { return (mask[idx >> 5] >> (idx & 31)) & 1u; }
 
-// column forward transform, modulus projection, column inverse transform
-template <int L>
-__device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>* tw, const float* As, int c, int q,
-                                                int data_mode) {
+// column forward transform, modulus projection (DataConstraint mode DMODE),
+// column inverse transform
+template <int L, int DMODE>
+__device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>* tw, const float* As, int c, int q) {
     using P = Plane<float, L>;
     constexpr int AP = DmPlan<L>::AP;
     Cx<float> o[P::J][P::TPL];
@@ -75,12 +79,14 @@ __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>*
 #pragma unroll
         for (int s = 0; s < P::TPL; ++s) {
             const int f = P::split_pos(q, j, s);
-            o[j][s] = data_apply(o[j][s], As[f * AP + c], data_mode);
+            o[j][s] = data_apply(o[j][s], As[f * AP + c], DMODE);
         }
     P::template col_to_buf<true>(o, buf, tw, c, q);
 }
 
-template <int L>
+// SMODE / DMODE: the SpaceConstraint and DataConstraint modes, fixed at
+// compile time so that each instantiation carries only its own arithmetic.
+template <int L, int SMODE, int DMODE>
 __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     using P = Plane<float, L>;
     using D = DmPlan<L>;
@@ -101,8 +107,8 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
     for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
-    const bool use_mask = (p.space_mode == SPACE_THRESHOLD);
-    if (use_mask) {
+    constexpr bool use_mask = (SMODE == SPACE_THRESHOLD);
+    if constexpr (use_mask) {
         for (int i = t; i < L * L; i += P::NT) {
             const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
             if ((i & 31) == 0) mask[i >> 5] = keep;
@@ -110,8 +116,10 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     }
     // SpaceConstraint of element idx, from the mask or the support plane
     auto space = [&](Cx<float> z, int idx) -> Cx<float> {
-        if (use_mask) return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
-        return space_apply(z, S[idx], p.space_mode);
+        if constexpr (use_mask)
+            return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
+        else
+            return space_apply(z, S[idx], SMODE);
     };
     // every element this thread touches has index line*L + split_pos(q, j, s)
     auto at = [&](int j, int s) { return line * L + P::split_pos(q, j, s); };
@@ -126,18 +134,26 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
     // duplicating them overflows the instruction cache).  Between halves no
     // block barrier is needed: a row's slots in the plane buffer are only
     // touched by the four threads of that row, which share a warp.
+    Cx<float> o[J][TPL];
     for (int it = 0; it < p.iters; ++it) {
         const bool last = (it == p.iters - 1);
 #pragma unroll 1
         for (int ph = 0; ph < 2; ++ph) {
-            Cx<float> o[J][TPL];
             if (ph == 0) {
                 // t1 <- S( a1*x + b1*Backward2D(DataConstraint(Forward2D(t1))) )
                 if (it > 0) {
+                    // o[j < J/2] holds the previous iteration's new x there
+                    // (second half's last step); t1's registers take it over
 #pragma unroll
-                    for (int j = 0; j < J; ++j)
+                    for (int j = 0; j < J / 2; ++j)
 #pragma unroll
-                        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(Cx<float>{t1r[j][s], 0.0f});
+                        for (int s = 0; s < TPL; ++s) {
+                            const Cx<float> xv = o[j][s];
+                            o[j][s] = sgn(Cx<float>{t1r[j][s], 0.0f});
+                            o[j + J / 2][s] = sgn(Cx<float>{t1r[j + J / 2][s], 0.0f});
+                            t1r[j][s] = xv.x;
+                            t1r[j + J / 2][s] = xv.y;
+                        }
                 } else if (!p.init_from_x) {
 #pragma unroll
                     for (int j = 0; j < J; ++j)
@@ -163,6 +179,21 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
                             o[j][s] = sgn(xv);
                         }
                 }
+                // t1's registers are free until this half's last step: they
+                // carry the first J/2 split columns of this row's x (real
+                // parts in t1r[j], imaginary parts in t1r[j + J/2]); on the
+                // first iteration they are loaded now, so that the transforms
+                // hide the latency
+                if (it == 0) {
+#pragma unroll
+                    for (int j = 0; j < J / 2; ++j)
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) {
+                            const Cx<float> xv = X[at(j, s)];
+                            t1r[j][s] = xv.x;
+                            t1r[j + J / 2][s] = xv.y;
+                        }
+                }
             } else {
                 // t2 <- Backward2D(DataConstraint(Forward2D( a2*x + b2*S(t2) )))
                 // (from the second iteration on, T2 already holds a2*x + b2*S(t2);
@@ -174,17 +205,17 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
                         const int idx = at(j, s);
                         Cx<float> z;
                         if (it > 0) {
-                            z = T2[idx];
+                            z = o[j][s];  // loaded by the first half's last step
                         } else {
                             const Cx<float> xv = X[idx];
                             z = merge_apply(xv, space(p.init_from_x ? xv : T2[idx], idx), p.a2, p.b2);
                         }
-                        o[j][s] = sgn(z);
+                        o[j][s] = (it > 0) ? z : sgn(z);
                     }
             }
             P::template rows_split_to_buf<false>(o, buf, tw, line, q);
             __syncthreads();
-            modulus_columns<L>(buf, tw, As, line, q, p.data_mode);
+            modulus_columns<L, DMODE>(buf, tw, As, line, q);
             __syncthreads();
             P::template row_from_buf<true>(o, buf, tw, line, q);
             if (ph == 0) {
@@ -193,9 +224,13 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
 #pragma unroll
                     for (int s = 0; s < TPL; ++s) {
                         const Cx<float> val = sgn(cscale(o[j][s], p.scale));
-                        const Cx<float> m = space(merge_apply(X[at(j, s)], val, p.a1, p.b1), at(j, s));
+                        // j < J/2: x from t1's registers (read before t1r[j] is
+                        // overwritten; t1r[j + J/2] is overwritten later)
+                        const Cx<float> xv = (j < J / 2) ? Cx<float>{t1r[j][s], t1r[j + J / 2][s]} : X[at(j, s)];
+                        const Cx<float> m = space(merge_apply(xv, val, p.a1, p.b1), at(j, s));
                         t1r[j][s] = m.x;
                         if (last) T1[at(j, s)] = m;
+                        if (it > 0) o[j][s] = sgn(T2[at(j, s)]);
                     }
             } else {
 #pragma unroll
@@ -208,6 +243,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
                         const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
                         X[idx] = xn;
                         T2[idx] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                        if (j < J / 2) o[j][s] = xn;  // for the next iteration's first half
                     }
             }
         }
@@ -242,9 +278,14 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     d.space_mode = a.space_mode;
     d.data_mode = a.data_mode;
     const size_t smem = DmPlan<L>::smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_dm<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto k = (a.space_mode == SPACE_THRESHOLD)
+                 ? (a.data_mode == DATA_ALWAYS ? k_dm<L, SPACE_THRESHOLD, DATA_ALWAYS>
+                                               : k_dm<L, SPACE_THRESHOLD, DATA_SKIP_ZERO>)
+                 : (a.data_mode == DATA_ALWAYS ? k_dm<L, SPACE_POSITIVE_SCALED, DATA_ALWAYS>
+                                               : k_dm<L, SPACE_POSITIVE_SCALED, DATA_SKIP_ZERO>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_dm<L><<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
+    k<<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
     count_launches();
     return cudaGetLastError();
 }
@@ -252,9 +293,10 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
 template <int L>
 int dm_occupancy() {
     const size_t smem = DmPlan<L>::smem_bytes();
-    if (cudaFuncSetAttribute(k_dm<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
+    auto k = k_dm<L, SPACE_THRESHOLD, DATA_SKIP_ZERO>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dm<L>, 4 * L, smem) != cudaSuccess || n < 1) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 4 * L, smem) != cudaSuccess || n < 1) return 1;
     return n;
 }
 

@@ -15,8 +15,13 @@
 // sigma_start at the first update to sigma_end at the last).
 //
 // On chip: the plane buffer of the transforms, A and the support (a bit mask)
-// in shared memory; x goes through L2 (read twice, written once per iteration).
-// Optionally the kernel also writes the estimate S (.) P_M(x) of the final x.
+// in shared memory.  x goes through L2: each thread keeps the x values it
+// wrote at its own positions in registers for the next iteration's forward
+// transform, holds the first half of them through the transforms, and reads
+// only the second half back for the update (written once, read half per
+// iteration; a full read after each support update, whose blur reuses those
+// registers).  Optionally the kernel also writes the estimate S (.) P_M(x) of
+// the final x.
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
@@ -64,7 +69,10 @@ __device__ __forceinline__ void spectral_columns(Cx<float>* buf, const Cx<float>
     P::template col_to_buf<true>(o, buf, tw, c, q);
 }
 
-template <int L>
+// DMODE: the DataConstraint mode; POS: positivity inside the support.  Both
+// fixed at compile time so that each instantiation carries only its own
+// arithmetic.
+template <int L, int DMODE, bool POS>
 __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
     using P = Plane<float, L>;
     using H = HioPlan<L>;
@@ -90,20 +98,32 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
     const bool neg = ((line + q) & 1) != 0;
     auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
     auto inside = [&](int idx) { return (mask[idx >> 5] >> (idx & 31)) & 1u; };
-    const int dmode = p.data_mode;
     __syncthreads();
 
     int update = 0;
-    for (int it = 0; it < p.iters; ++it) {
-        Cx<float> o[J][TPL];
+    // o: this thread's x values at the top of each iteration
+    Cx<float> o[J][TPL];
+    auto load_x = [&]() {
 #pragma unroll
         for (int j = 0; j < J; ++j)
 #pragma unroll
-            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(X[at(j, s)]);
+            for (int s = 0; s < TPL; ++s) o[j][s] = X[at(j, s)];
+    };
+    load_x();
+    for (int it = 0; it < p.iters; ++it) {
+        // xh: the first J/2 split columns of x, kept through the transforms
+        Cx<float> xh[J / 2][TPL];
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                if (j < J / 2) xh[j][s] = o[j][s];
+                o[j][s] = sgn(o[j][s]);
+            }
         P::template rows_split_to_buf<false>(o, buf, tw, line, q);
         __syncthreads();
         spectral_columns<L>(buf, tw, line, q, [&](Cx<float> z, int f, int c) {
-            return data_apply(z, As[f * AP + c], dmode);
+            return data_apply(z, As[f * AP + c], DMODE);
         });
         __syncthreads();
         P::template row_from_buf<true>(o, buf, tw, line, q);
@@ -113,8 +133,8 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
             for (int s = 0; s < TPL; ++s) {
                 const int idx = at(j, s);
                 const Cx<float> y = sgn(cscale(o[j][s], p.scale));
-                const Cx<float> xv = X[idx];
-                const bool keep = inside(idx) && (!p.positivity || y.x >= 0.0f);
+                const Cx<float> xv = (j < J / 2) ? xh[j][s] : X[idx];
+                const bool keep = inside(idx) && (!POS || y.x >= 0.0f);
                 const Cx<float> xn = keep ? y : merge_apply(y, xv, -p.beta, 1.0f);
                 X[idx] = xn;
                 o[j][s] = xn;
@@ -163,6 +183,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
                     atomicOr(&mask[idx >> 5], 1u << (idx & 31));
                 }
         __syncthreads();  // red[] is reused by the next update
+        load_x();         // the blur overwrote o
     }
 #pragma unroll
     for (int j = 0; j < J; ++j)
@@ -171,7 +192,6 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
     if (!p.est) return;
     // the estimate: the modulus projection of the final x, restricted to the support
     Cx<float>* __restrict__ E = p.est + (size_t)blockIdx.x * L * L;
-    Cx<float> o[J][TPL];
 #pragma unroll
     for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -179,7 +199,7 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
     P::template rows_split_to_buf<false>(o, buf, tw, line, q);
     __syncthreads();
     spectral_columns<L>(buf, tw, line, q, [&](Cx<float> z, int f, int c) {
-        return data_apply(z, As[f * AP + c], dmode);
+        return data_apply(z, As[f * AP + c], DMODE);
     });
     __syncthreads();
     P::template row_from_buf<true>(o, buf, tw, line, q);
@@ -211,9 +231,12 @@ cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
     d.positivity = a.positivity;
     d.data_mode = a.data_mode;
     const size_t smem = HioPlan<L>::smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_hio<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const bool always = (a.data_mode == DATA_ALWAYS);
+    auto k = a.positivity ? (always ? k_hio<L, DATA_ALWAYS, true> : k_hio<L, DATA_SKIP_ZERO, true>)
+                          : (always ? k_hio<L, DATA_ALWAYS, false> : k_hio<L, DATA_SKIP_ZERO, false>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_hio<L><<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
+    k<<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
     count_launches();
     return cudaGetLastError();
 }

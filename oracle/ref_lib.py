@@ -7,8 +7,10 @@ and operates in place on contiguous numpy arrays.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -61,6 +63,25 @@ def set_threads(n: int) -> int:
     return lib().cpra_ref_set_threads(int(n))
 
 
+@contextlib.contextmanager
+def _c_stdout_to_stderr():
+    """The reference's constructor and destructor report DFTI failures with
+    printf (include/MKL_Impl.hpp:28-79, 167-179; its 3D descriptor is built
+    from the 2D length array and the shim refuses it).  Those lines go to
+    stderr here, so that a caller's stdout carries only its own output."""
+    libc = C.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def _p(a: np.ndarray):
     assert a.flags["C_CONTIGUOUS"], "reference wrappers need contiguous arrays"
     return a.ctypes.data_as(C.c_void_p)
@@ -73,12 +94,18 @@ class RefImpl:
         self.T = np.dtype(T).type
         self.dbl = 1 if self.T == np.float64 else 0
         self.m, self.n, self.l, self.batch = int(m), int(n), int(l), int(batch_size)
-        self.h = lib().cpra_ref_create(self.dbl, self.m, self.n, self.l, self.batch)
+        L = lib()
+        with _c_stdout_to_stderr():
+            self.h = L.cpra_ref_create(self.dbl, self.m, self.n, self.l, self.batch)
 
     def __del__(self):
+        # the reference's destructor prints its last DFTI status twice
+        # (include/MKL_Impl.hpp:167-179): routed to stderr like the constructor's
         try:
             if self.h:
-                lib().cpra_ref_destroy(self.dbl, self.h)
+                L = lib()
+                with _c_stdout_to_stderr():
+                    L.cpra_ref_destroy(self.dbl, self.h)
                 self.h = None
         except Exception:
             pass

@@ -54,8 +54,10 @@ def test_reference_arm_under_torchrun_two_ranks():
     env = dict(os.environ, OMP_NUM_THREADS="1")
     r = subprocess.run(cmd, cwd=REPO, capture_output=True, text=True, timeout=300, env=env)
     assert r.returncode == 0, r.stderr[-2000:]
-    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
-    assert len(lines) == 1, r.stdout
+    # stdout carries exactly the one JSON line (the reference's own printf
+    # diagnostics go to stderr)
+    lines = [l for l in r.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1 and lines[0].startswith("{"), r.stdout
     d = json.loads(lines[0])
     assert d["impl"] == "reference"
     assert "unavailable" in d or (d["value"] > 0 and d["n_gpus"] == 2)
