@@ -49,9 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
-    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d"], default="carousel",
-                    help="uneven / carousel3d / fft3d: only that side measurement (one JSON line, for profiling "
-                         "runs)")
+    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d", "plain2d"], default="carousel",
+                    help="uneven / carousel3d / fft3d / plain2d: only that side measurement (one JSON line, for "
+                         "profiling runs)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
     # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
@@ -349,6 +349,11 @@ def main():
                                  B=a.starts, epi=a.episodes, iters=a.iters, refine_steps=a.refine_steps,
                                  step_deg=a.angle_step, photons=a.photons, ellipsoids=a.ellipsoids,
                                  axes=tuple(float(v) for v in a.axes.split(",")))
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+    if a.case == "plain2d":
+        out = plain2d(torch, cpra_b200, torch.device("cuda", local), reps=max(1, a.steps))
         if rank == 0:
             print(json.dumps(out), flush=True)
         return

@@ -15,13 +15,13 @@
 // sigma_start at the first update to sigma_end at the last).
 //
 // On chip: the plane buffer of the transforms, A and the support (a bit mask)
-// in shared memory.  x goes through L2: each thread keeps the x values it
-// wrote at its own positions in registers for the next iteration's forward
-// transform, holds the first half of them through the transforms, and reads
-// only the second half back for the update (written once, read half per
-// iteration; a full read after each support update, whose blur reuses those
-// registers).  Optionally the kernel also writes the estimate S (.) P_M(x) of
-// the final x.
+// in shared memory.  Each thread keeps the x values of its own positions in
+// registers for the next iteration's forward transform and holds the first
+// half of them through the transforms, so only the second half goes through
+// L2 (written and read once per iteration).  The first half is written before
+// each support update, whose blur reuses those registers (x is read back in
+// full after it), and after the last iteration.  Optionally the kernel also
+// writes the estimate S (.) P_M(x) of the final x.
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
@@ -127,6 +127,11 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
         });
         __syncthreads();
         P::template row_from_buf<true>(o, buf, tw, line, q);
+        const bool update_next = p.sw_every > 0 && p.blur && (it + 1) % p.sw_every == 0;
+        // the first half of x lives in registers from here to the next
+        // update; it goes to memory only before a support update (whose blur
+        // reuses the registers) and after the last iteration
+        const bool store_all = update_next || it + 1 == p.iters;
 #pragma unroll
         for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -136,10 +141,10 @@ __global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
                 const Cx<float> xv = (j < J / 2) ? xh[j][s] : X[idx];
                 const bool keep = inside(idx) && (!POS || y.x >= 0.0f);
                 const Cx<float> xn = keep ? y : merge_apply(y, xv, -p.beta, 1.0f);
-                X[idx] = xn;
+                if (j >= J / 2 || store_all) X[idx] = xn;
                 o[j][s] = xn;
             }
-        if (p.sw_every <= 0 || !p.blur || (it + 1) % p.sw_every != 0) continue;
+        if (!update_next) continue;
 
         // ---- shrinkwrap: v = |x| blurred, support = { v > thresh * max v } ----
         if (t < L) gt[t] = p.blur[(size_t)update * L + t];

@@ -665,6 +665,27 @@ def test_hio_iterations_vs_oracle(tb, L, B, iters, pos):
     np.testing.assert_array_equal(host(S), So.astype(np.float32))   # no update: support unchanged
 
 
+@pytest.mark.parametrize("L", [32, 64, 128])
+def test_hio_fused_split_calls_bitwise(tb, L):
+    """The fused HIO kernel carries x in registers from one iteration to the
+    next and writes half of it to memory only after its last iteration: 7
+    iterations in one call equal 3 + 4 iterations in two calls (which restart
+    from memory), bit for bit, with and without positivity."""
+    torch, cb = tb
+    B = 3
+    A, S0, x0 = _hio_inputs(L, B, seed=L + 11)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    Ad = dev(torch, A.ravel())
+    for pos in (False, True):
+        x1, S1 = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        assert impl.hio_shrinkwrap(x1, Ad, S1, B, 7, beta=0.9, sw_every=0, positivity=pos) and impl.Sync()
+        x2, S2 = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        assert impl.hio_shrinkwrap(x2, Ad, S2, B, 3, beta=0.9, sw_every=0, positivity=pos)
+        assert impl.hio_shrinkwrap(x2, Ad, S2, B, 4, beta=0.9, sw_every=0, positivity=pos) and impl.Sync()
+        assert torch.equal(torch.view_as_real(x1), torch.view_as_real(x2)), (L, pos)
+        assert torch.equal(S1, S2)
+
+
 def test_hio_shrinkwrap_support_vs_oracle(tb):
     """Support masks after shrinkwrap updates differ in <= 0.1% of pixels."""
     torch, cb = tb
