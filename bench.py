@@ -590,8 +590,10 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     carousel_gpu).  Timed by CUDA events on the contexts' streams:
       * the 2D stage: cpra_run, 10 episodes x 10 DM iterations per angle over B
         random starts, with the convergence error and the final projection
-        (the line-pass DM kernels at 256^2), pattern-iterations/s as a replay
-        of its CUDA graph (CPRA_B200_OPT_GRAPH; `value_direct` without) and the
+        (the line-pass DM kernels at 256^2) on the lane count the context's
+        autotuner measured (CPRA_B200_OPT_AUTOTUNE; `lanes_heuristic` is the
+        automatic choice), pattern-iterations/s as a replay of its CUDA graph
+        (CPRA_B200_OPT_GRAPH; `value_direct` without) and the
         roofline of the fused launches at 56 B per pattern-pixel; beside it the
         DM iteration as torch.fft (cuFFT) plus torch element-wise kernels on
         one angle's batch (per_op_compare);
@@ -633,16 +635,19 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
 
     # the roofline from per-launch CUDA events on a direct run with one lane
     # (launches one after another, so each event pair brackets one launch);
-    # the stage's time with the automatic lanes (CPRA_B200_OPT_LANES 0: one
+    # the stage's time with measured lanes (CPRA_B200_OPT_AUTOTUNE: one
     # angle's launch leaves the GPU part empty at B starts, so episodes run
-    # as a wavefront beside each other), direct and from graph replays
+    # as a wavefront beside each other; the first run of the key, untimed,
+    # times the lane counts), direct and from graph replays
     impl.set_option(cpra_b200.OPT_LANES, 1)
     run2d(1, 2)
     ms_one_lane, kt = run2d(epi, iters, timing=True)
     impl.set_option(cpra_b200.OPT_LANES, 0)
+    lanes_auto = impl.get_option(cpra_b200.OPT_LANES)
+    impl.set_option(cpra_b200.OPT_AUTOTUNE, 1)
+    run2d(epi, iters)
     lanes = max(1, min(impl.get_option(cpra_b200.OPT_LANES), epi))
     lanes = -(-epi // -(-epi // lanes))  # episodes spread evenly over the lanes
-    run2d(1, 2)
     ms_direct = run2d(epi, iters)[0]
     impl.set_option(cpra_b200.OPT_GRAPH, 1)
     run2d(epi, iters)
@@ -698,6 +703,7 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
                     f"patterns at {photons:.0e} photons; 2D stage {epi} episodes x {iters} DM iterations x {B} "
                     f"starts; best start; merge; {refine_steps} Adam steps",
         "stage2d": {"value": units / (ms2d / 1e3), "unit": METRIC, "ms": ms2d, "graph": True, "lanes": lanes,
+                    "lanes_heuristic": lanes_auto,
                     "value_one_lane": units / (ms_one_lane / 1e3),
                     "value_direct": units / (ms_direct / 1e3), "roofline": roof,
                     "per_op_path": per_op,

@@ -220,6 +220,11 @@ struct cpra_b200_ctx {
     std::vector<RunLane> run_lanes;
     cudaEvent_t lane_fork = nullptr;
     int lanes_opt = 0;
+    // CPRA_B200_OPT_AUTOTUNE: measured lane counts per run key, and the
+    // choice of the last cpra_b200_cpra_run that used the cache (0: none)
+    bool autotune = false;
+    std::vector<std::pair<std::string, int>> tune_cache;
+    int tuned_lanes = 0;
     // cpra_b200_cpra_run_host: device copies of x, A, S, the copy stream and events
     void* hx = nullptr;
     uint64_t hx_bytes = 0;
@@ -756,6 +761,7 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
             if (value < 4096) return fail(CPRA_B200_EARG, "io chunk must be >= 4096 bytes");
             c->io_chunk = (uint64_t)value;
             break;
+        case CPRA_B200_OPT_AUTOTUNE: c->autotune = value != 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1563,8 +1569,12 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
         case CPRA_B200_OPT_KERNEL_TIMING: *value = c->timing ? 1 : 0; break;
         case CPRA_B200_OPT_HIO_CHUNK: *value = (int64_t)c->hio_chunk; break;
         case CPRA_B200_OPT_GRAPH: *value = c->graphs ? 1 : 0; break;
-        case CPRA_B200_OPT_LANES: *value = run_lanes_for(c, c->batch); break;
+        case CPRA_B200_OPT_LANES:
+            *value = (c->autotune && c->lanes_opt == 0 && c->tuned_lanes > 0) ? c->tuned_lanes
+                                                                              : run_lanes_for(c, c->batch);
+            break;
         case CPRA_B200_OPT_IO_CHUNK: *value = (int64_t)c->io_chunk; break;
+        case CPRA_B200_OPT_AUTOTUNE: *value = c->autotune ? 1 : 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1597,6 +1607,74 @@ int ensure_lanes(cpra_b200_ctx* c, int W, uint64_t drv_bytes, uint64_t work_byte
     return CPRA_B200_OK;
 }
 
+static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
+                         int iters, int pre_iter, double beta, int final_step, void* err_host,
+                         const cudaEvent_t* ready, const cudaEvent_t* done,
+                         const std::function<int()>& after_enqueue = {});
+
+// CPRA_B200_OPT_AUTOTUNE: the lane count of cpra_run's wavefront schedule,
+// measured.  Every candidate (1 to 4 lanes and the automatic choice, as many
+// as the episodes allow after balancing) runs the same min(epi, 4) episodes
+// on a copy of x, timed by CUDA events on the context's stream, graphs off;
+// the largest candidate runs first and again at the end, so that its first
+// run carries the lanes' one-time set-up.  Lane counts change the schedule
+// only, never the results, so the choice is free.
+static int tune_lanes(cpra_b200_ctx* c, const void* x, const void* A, const void* S, uint64_t P, uint64_t batch,
+                      int epi, int iters, double beta, int* best_out) {
+    const uint64_t xbytes = P * batch * c->plane() * c->csize();
+    const int E = std::min(epi, 4);
+    std::vector<int> cand;
+    for (int w : {1, 2, 3, 4, run_lanes_for(c, batch)}) {
+        const int eff = balanced_lanes(std::min(w, CPRA_B200_MAX_LANES), E);
+        if (std::find(cand.begin(), cand.end(), eff) == cand.end()) cand.push_back(eff);
+    }
+    std::sort(cand.rbegin(), cand.rend());
+    if (cand.size() == 1) {
+        *best_out = cand[0];
+        return CPRA_B200_OK;
+    }
+    struct Restore {
+        cpra_b200_ctx* c;
+        int lanes;
+        bool graphs, timing;
+        void* trial = nullptr;
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        ~Restore() {
+            c->lanes_opt = lanes;
+            c->graphs = graphs;
+            c->timing = timing;
+            if (trial) {
+                cudaStreamSynchronize(c->stream);
+                cudaFree(trial);
+            }
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } g{c, c->lanes_opt, c->graphs, c->timing};
+    c->graphs = false;
+    c->timing = false;
+    CPRA_CHECK_CUDA(cudaMalloc(&g.trial, xbytes), "cudaMalloc(autotune copy of x)");
+    CPRA_CHECK_CUDA(cudaEventCreate(&g.ev[0]), "cudaEventCreate");
+    CPRA_CHECK_CUDA(cudaEventCreate(&g.ev[1]), "cudaEventCreate");
+    std::vector<float> ms(cand.size(), 0.0f);
+    for (size_t i = 0; i <= cand.size(); ++i) {
+        const size_t k = (i == cand.size()) ? 0 : i;
+        c->lanes_opt = cand[k];
+        CPRA_CHECK_CUDA(cudaMemcpyAsync(g.trial, x, xbytes, cudaMemcpyDeviceToDevice, c->stream), "autotune");
+        CPRA_CHECK_CUDA(cudaEventRecord(g.ev[0], c->stream), "autotune");
+        int r = cpra_run_impl(c, g.trial, A, S, P, batch, E, iters, 0, beta, 0, nullptr, nullptr, nullptr);
+        if (r) return r;
+        CPRA_CHECK_CUDA(cudaEventRecord(g.ev[1], c->stream), "autotune");
+        CPRA_CHECK_CUDA(cudaEventSynchronize(g.ev[1]), "autotune");
+        CPRA_CHECK_CUDA(cudaEventElapsedTime(&ms[k], g.ev[0], g.ev[1]), "autotune");
+    }
+    size_t best = 0;
+    for (size_t k = 1; k < cand.size(); ++k)
+        if (ms[k] < ms[best]) best = k;
+    *best_out = cand[best];
+    return CPRA_B200_OK;
+}
+
 // The carousel driver on device buffers.  ready (optional, P events): angle
 // p's plane of x is complete once ready[p] has fired; the first episode (and
 // the pre-iterations) wait for each plane they read, just before its first
@@ -1606,7 +1684,7 @@ int ensure_lanes(cpra_b200_ctx* c, int W, uint64_t drv_bytes, uint64_t work_byte
 static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S, uint64_t P, uint64_t batch, int epi,
                          int iters, int pre_iter, double beta, int final_step, void* err_host,
                          const cudaEvent_t* ready, const cudaEvent_t* done,
-                         const std::function<int()>& after_enqueue = {}) {
+                         const std::function<int()>& after_enqueue) {
     if (!x || !A || !S) return fail(CPRA_B200_EARG, "cpra_run: null pointer");
     if (P < 2) return fail(CPRA_B200_EARG, "cpra_run: P >= 2 (the carousel mix reads angles p-1 and p+1)");
     if (batch != c->batch) return fail(CPRA_B200_EARG, "cpra_run: batch must equal the context's batch_size");
@@ -1618,6 +1696,20 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
         return fail(CPRA_B200_EUNSUP, "cpra_run: each plane size must be 1 or even and at most 4096");
     int r = flush(c);
     if (r) return take_deferred(c);
+    // CPRA_B200_OPT_AUTOTUNE: the measured lane count of this run's key.  A
+    // host-buffer run (x still arriving) uses the cache but does not tune.
+    int tuned = 0;
+    if (c->autotune && c->lanes_opt == 0 && epi > 1 && !c->capturing) {
+        const std::string key = graph_key("lanes", c->m, c->n, batch, P, iters, c->fusion, c->space_mode,
+                                          c->data_mode, c->dbl);
+        for (const auto& e : c->tune_cache)
+            if (e.first == key) tuned = e.second;
+        if (!tuned && !ready) {
+            if ((r = tune_lanes(c, x, A, S, P, batch, epi, iters, beta, &tuned))) return r;
+            c->tune_cache.emplace_back(key, tuned);
+        }
+        c->tuned_lanes = tuned;
+    }
     const uint64_t MN = c->plane(), MNB = MN * batch;
     const uint64_t cb = MNB * c->csize();
     if ((r = ensure_buffer(c, &c->drv, &c->drv_bytes, 3 * cb, "cudaMalloc(driver buffers)"))) return r;
@@ -1647,7 +1739,7 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     r = ensure_work(c, work_need);
     if (r) return r;
     // lanes of the wavefront schedule, each with its own scratch
-    const int W = balanced_lanes(run_lanes_for(c, batch), epi);
+    const int W = balanced_lanes(tuned ? tuned : run_lanes_for(c, batch), epi);
     if ((r = ensure_lanes(c, W, 3 * cb, work_need, P))) return r;
     char* base = static_cast<char*>(x);
     const char* Ab = static_cast<const char*>(A);

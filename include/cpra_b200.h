@@ -69,6 +69,13 @@ extern "C" {
 #define CPRA_B200_MAX_LANES 16
 #define CPRA_B200_OPT_IO_CHUNK 9   /* bytes of each of the two pinned staging chunks of the file I/O entries
                                     (default 64 MiB, at least 4096) */
+#define CPRA_B200_OPT_AUTOTUNE 10  /* 1: with CPRA_B200_OPT_LANES 0, the first cpra_b200_cpra_run of each key
+                                    (plane size, batch, angles, iterations, fusion and modes) measures the
+                                    lane counts 1-4 and the automatic choice on a copy of x (min(epi, 4)
+                                    episodes each; the copy is allocated for the duration) and keeps the
+                                    fastest in the context's cache; later runs of that key use it, host-buffer
+                                    runs only once it is cached.  No tuning during a stream capture or for
+                                    epi < 2.  0 (default): the automatic choice.  Same results either way. */
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 
@@ -84,7 +91,8 @@ uint64_t cpra_b200_kernels_launched(void);
 int cpra_b200_set_option(cpra_b200_ctx* ctx, int option, int64_t value);
 /* Extension: reads an option back.  CPRA_B200_OPT_LANES reads the number of
  * lanes cpra_b200_cpra_run uses for the context's batch (the automatic choice
- * resolved; before the episode-count cap). */
+ * resolved, or with CPRA_B200_OPT_AUTOTUNE the last run's measured choice;
+ * before the episode-count cap). */
 int cpra_b200_get_option(cpra_b200_ctx* ctx, int option, int64_t* value);
 /* The context's stream as a cudaStream_t (for interoperation). */
 int cpra_b200_get_stream(cpra_b200_ctx* ctx, void** stream);

@@ -574,6 +574,45 @@ def test_cpra_run_lanes_bitwise(tb, L, P, B, epi, it, pre, lanes, final, dtype):
     assert not run.set_option(cb.OPT_LANES, 17)
 
 
+@pytest.mark.parametrize("L,P,B,epi", [(64, 6, 3, 5), (256, 3, 2, 3)])
+def test_cpra_run_autotune_bitwise(tb, L, P, B, epi):
+    """CPRA_B200_OPT_AUTOTUNE: the first run of a key times the lane counts
+    on a copy of x and caches the fastest.  The tuning run, a later run (which
+    launches only its own kernels) and a host-buffer run all write the bits
+    and errors of one stream taking the angles in order."""
+    torch, cb = tb
+    it, pre = 2, 1
+    rng = np.random.default_rng(L + P + epi)
+    A = (rng.uniform(0, 30, (P, L * L)) * (rng.uniform(0, 1, (P, L * L)) > 0.1)).astype(np.float32)
+    S = (rng.uniform(0, 1, (P, L * L)) > 0.45).astype(np.float32)
+    x0 = (rng.uniform(0, 1, P * B * L * L) + 1j * rng.uniform(0, 1, P * B * L * L)).astype(np.complex64)
+    Ad, Sd = dev(torch, A.ravel()), dev(torch, S.ravel())
+    ref = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert ref.set_option(cb.OPT_LANES, 1)
+    xr, err_r = dev(torch, x0), np.zeros(P * B, np.float32)
+    assert ref.cpra_run(xr, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=True, err=err_r) and ref.Sync()
+    run = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert run.get_option(cb.OPT_AUTOTUNE) == 0
+    assert run.set_option(cb.OPT_AUTOTUNE, 1) and run.get_option(cb.OPT_AUTOTUNE) == 1
+    launched = []
+    for _ in range(2):
+        x, err = dev(torch, x0), np.zeros(P * B, np.float32)
+        n0 = cb.kernels_launched()
+        assert run.cpra_run(x, Ad, Sd, P, B, epi, it, pre, 0.9, final_step=True, err=err) and run.Sync()
+        launched.append(cb.kernels_launched() - n0)
+        np.testing.assert_array_equal(host(x), host(xr))
+        np.testing.assert_array_equal(err, err_r)
+        assert 1 <= run.get_option(cb.OPT_LANES) <= 16
+    assert launched[1] < launched[0]  # the first run also ran the trials
+    xh = torch.from_numpy(x0.view(np.float32).copy()).pin_memory()
+    err = np.zeros(P * B, np.float32)
+    assert run.cpra_run_host(xh, torch.from_numpy(A.ravel().copy()).pin_memory(),
+                             torch.from_numpy(S.ravel().copy()).pin_memory(), P, B, epi, it, pre, 0.9,
+                             final_step=True, err=err)
+    np.testing.assert_array_equal(xh.numpy().view(np.complex64), host(xr))
+    np.testing.assert_array_equal(err, err_r)
+
+
 def _drop_in_binaries():
     from conftest import REPO
     d = REPO / "tests" / "cpp" / "_bin"
