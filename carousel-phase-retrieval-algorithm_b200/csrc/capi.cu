@@ -1530,13 +1530,18 @@ int cpra_b200_kernel_timing(cpra_b200_ctx* c, double* ms, uint64_t* launches, ui
 
 // Lanes of cpra_run's wavefront schedule: with CPRA_B200_OPT_LANES 0, as many
 // as it takes for the angles running side by side to fill the GPU's resident
-// CTA slots one and a half times (one lane when one angle's launch already
-// fills them once: then more lanes only compete for L2).
+// CTA slots one and a half times (one lane when one angle's launch of the
+// one-CTA-per-pattern kernel already fills them once: then more lanes only
+// compete for L2).  The line passes (256², 512²) take at least four: each
+// iteration is a column pass and a row pass that waits for all of it, and the
+// episodes beside them fill every pass boundary's drain and ramp (measured by
+// the autotuner: 4 lanes ahead of the slot count at 256² and 512², 16 starts).
 int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
     if (c->lanes_opt > 0) return c->lanes_opt;
     if (!c->fusion || !dm_fusable(c)) return 1;
     uint64_t ctas, per_sm;
-    if (dm_fused_supported(c->dbl, c->m, c->n)) {
+    const bool line_passes = !dm_fused_supported(c->dbl, c->m, c->n);
+    if (!line_passes) {
         ctas = batch;
         per_sm = (uint64_t)dm_fused_ctas_per_sm(c->m);
     } else {
@@ -1544,8 +1549,11 @@ int run_lanes_for(cpra_b200_ctx* c, uint64_t batch) {
         per_sm = (uint64_t)dm_large_ctas_per_sm(c->m);
     }
     const uint64_t slots = per_sm * (uint64_t)sm_count();
-    if (ctas == 0 || ctas >= slots) return 1;
-    return (int)std::min<uint64_t>(CPRA_B200_MAX_LANES, (3 * slots + 2 * ctas - 1) / (2 * ctas));
+    uint64_t w = 1;
+    if (ctas > 0 && ctas < slots)
+        w = std::min<uint64_t>(CPRA_B200_MAX_LANES, (3 * slots + 2 * ctas - 1) / (2 * ctas));
+    if (line_passes) w = std::max<uint64_t>(w, 4);
+    return (int)w;
 }
 
 // Lanes for `epi` episodes: at most `want`, and no more than it takes to give
