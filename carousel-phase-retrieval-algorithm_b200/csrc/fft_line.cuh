@@ -161,12 +161,16 @@ struct LineFFT {
             __syncwarp();
             const int m = q >> 1;
             const bool odd = (q & 1) != 0;
+            // a0 + sg * a1 as one fused multiply-add: the product by +-1 is
+            // exact, so it rounds exactly like cadd (even) or csub (odd)
+            const T sg = odd ? T(-1) : T(1);
             Cx<T> b[R];
 #pragma unroll
             for (int p = 0; p < R; ++p) {
                 const Cx<T> a0 = scratch[xslot<TPL>(m, p) * ss];
                 const Cx<T> a1 = scratch[xslot<TPL>(m, p + R) * ss];
-                b[p] = odd ? rot32<T, INV>(csub(a0, a1), p) : cadd(a0, a1);  // W_32^p (TPL = 32)
+                const Cx<T> d = {fma_rn(sg, a1.x, a0.x), fma_rn(sg, a1.y, a0.y)};
+                b[p] = odd ? rot32<T, INV>(d, p) : d;  // W_32^p (TPL = 32)
             }
             dft_regs<T, R, INV>(b);
 #pragma unroll

@@ -94,6 +94,15 @@ __device__ __forceinline__ void stage(void* dst, const void* src, uint32_t bytes
         for (uint32_t i = 4u * t; i < bytes; i += 4u * nt) cp_async4(d + i, s + i);
 }
 
+// First tile row of the thread with copy-row index r when a pass of the CTA
+// copies `step` rows.  With 32 rows per pass and 8 copies per row (512: odd
+// pitch 9, 8-byte complex and 4-byte A copies) a warp takes rows w, w + 8,
+// w + 16, w + 24 of each 32-row block: at pitch 9 their slots fall on
+// distinct bank pairs per half-warp (complex) and distinct banks (A), where
+// four consecutive rows would put two copies on one bank.  Any other step
+// keeps consecutive rows.  A bijection on 0..step-1 either way.
+__device__ __forceinline__ int tile_row(int r, int step) { return step == 32 ? (r >> 2) + 8 * (r & 3) : r; }
+
 // A column tile: rows n < L of LN consecutive complex at src + n * ld into
 // dst + n * CS (16-byte copies when CS is even, 8-byte copies otherwise), and
 // optionally LN floats per row of A at a + n * ld into as + n * AS (16-byte
@@ -107,7 +116,7 @@ __device__ __forceinline__ void stage_col_tile(Cx<float>* dst, const Cx<float>* 
     constexpr int W = (CS % 2 == 0) ? 2 : 1;  // complex per copy
     constexpr int CH = LN / W;
     {
-        const int k = t % CH, n0 = t / CH, step = nt / CH;
+        const int k = t % CH, step = nt / CH, n0 = (W == 1) ? tile_row(t / CH, step) : t / CH;
         const Cx<float>* s = src + (uint64_t)n0 * ld + W * k;
         Cx<float>* d = dst + n0 * CS + W * k;
         const uint64_t sstep = (uint64_t)step * ld;
@@ -127,7 +136,7 @@ __device__ __forceinline__ void stage_col_tile(Cx<float>* dst, const Cx<float>* 
         const uint64_t sstep = (uint64_t)step * ld;
         for (int n = n0; n < L; n += step, s += sstep, d += step * AS) cp_async16(d, s);
     } else {
-        const int k = t % LN, n0 = t / LN, step = nt / LN;
+        const int k = t % LN, step = nt / LN, n0 = tile_row(t / LN, step);
         const float* s = a + (uint64_t)n0 * ld + k;
         float* d = as + n0 * AS + k;
         const uint64_t sstep = (uint64_t)step * ld;
@@ -141,7 +150,7 @@ template <int L, int LN, int CS>
 __device__ __forceinline__ void store_col_tile(Cx<float>* dst, const Cx<float>* src, uint64_t ld, int t, int nt) {
     constexpr int W = (CS % 2 == 0) ? 2 : 1;
     constexpr int CH = LN / W;
-    const int k = t % CH, n0 = t / CH, step = nt / CH;
+    const int k = t % CH, step = nt / CH, n0 = (W == 1) ? tile_row(t / CH, step) : t / CH;
     Cx<float>* d = dst + (uint64_t)n0 * ld + W * k;
     const Cx<float>* s = src + n0 * CS + W * k;
     const uint64_t dstep = (uint64_t)step * ld;
