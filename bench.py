@@ -482,6 +482,19 @@ def main():
                 "avg_launch_ms": kms / klaunches, "launches": klaunches,
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
                 "share_of_step": kms / ms}
+        # secondary: the transforms' arithmetic (5 N log2 N flops per N-point
+        # complex transform, four 2D transforms per DM iteration) against the
+        # FP32 FMA rate of the SMs at the sampled clock (no tensor cores: no
+        # contraction on this path)
+        fft_flops = 4 * 5 * MN * np.log2(MN) * kpi / klaunches
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        fp32_peak = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else None
+        roof["secondary"] = {"bound": "fp32", "achieved": fft_flops / avg_s / 1e12, "unit": "TFLOP/s",
+                             "peak": fp32_peak,
+                             "frac": (fft_flops / avg_s / 1e12 / fp32_peak) if fp32_peak else None,
+                             "peak_kind": "SMs x 128 FP32 lanes x 2 (FMA) x sampled SM clock, not measured",
+                             "flops_per_launch": fft_flops}
 
     # R-factor of the result of the last step, per pattern, against its angle's modulus
     rf = np.concatenate([impl.rfactor(x[p * B * MN:(p + 1) * B * MN], A[p * MN:(p + 1) * MN], B) for p in range(P)])
