@@ -1661,7 +1661,14 @@ static int tune_lanes(cpra_b200_ctx* c, const void* x, const void* A, const void
     } g{c, c->lanes_opt, c->graphs, c->timing};
     c->graphs = false;
     c->timing = false;
-    CPRA_CHECK_CUDA(cudaMalloc(&g.trial, xbytes), "cudaMalloc(autotune copy of x)");
+    if (cudaMalloc(&g.trial, xbytes) != cudaSuccess) {
+        // no room for the copy: keep the heuristic's choice for this key (an
+        // out-of-memory error is not sticky; clear it)
+        cudaGetLastError();
+        g.trial = nullptr;
+        *best_out = run_lanes_for(c, batch);
+        return CPRA_B200_OK;
+    }
     CPRA_CHECK_CUDA(cudaEventCreate(&g.ev[0]), "cudaEventCreate");
     CPRA_CHECK_CUDA(cudaEventCreate(&g.ev[1]), "cudaEventCreate");
     std::vector<float> ms(cand.size(), 0.0f);

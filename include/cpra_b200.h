@@ -75,7 +75,8 @@ extern "C" {
                                     episodes each; the copy is allocated for the duration) and keeps the
                                     fastest in the context's cache; later runs of that key use it, host-buffer
                                     runs only once it is cached.  No tuning during a stream capture or for
-                                    epi < 2.  0 (default): the automatic choice.  Same results either way. */
+                                    epi < 2; if the copy cannot be allocated the key keeps the automatic
+                                    choice.  0 (default): the automatic choice.  Same results either way. */
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 
