@@ -855,7 +855,7 @@ def test_hio_batched_matches_per_size_calls(tb):
     single-size call with the same patterns (the buckets only share the
     device, not data)."""
     torch, cb = tb
-    sizes = [(64, 3), (128, 2), (256, 2), (512, 1)]
+    sizes = [(64, 3), (128, 2), (256, 2), (512, 3)]
     iters, sw = 12, 5
     data = {L: _hio_inputs(L, B, seed=L) for L, B in sizes}
     buckets, keep = [], []
