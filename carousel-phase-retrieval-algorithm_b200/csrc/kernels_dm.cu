@@ -86,8 +86,10 @@ __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>*
 
 // SMODE / DMODE: the SpaceConstraint and DataConstraint modes, fixed at
 // compile time so that each instantiation carries only its own arithmetic.
+// At 64^2 two CTAs share an SM (at most 128 registers, no spills; left
+// unbounded the kernel takes 155 and one CTA per SM).
 template <int L, int SMODE, int DMODE>
-__global__ void __launch_bounds__(4 * L, 1) k_dm(const DmDev p) {
+__global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) {
     using P = Plane<float, L>;
     using D = DmPlan<L>;
     constexpr int J = P::J, TPL = P::TPL;

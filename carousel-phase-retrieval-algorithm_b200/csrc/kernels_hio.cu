@@ -71,9 +71,10 @@ __device__ __forceinline__ void spectral_columns(Cx<float>* buf, const Cx<float>
 
 // DMODE: the DataConstraint mode; POS: positivity inside the support.  Both
 // fixed at compile time so that each instantiation carries only its own
-// arithmetic.
+// arithmetic.  At 64^2 three CTAs share an SM (at most 80 registers, no
+// spills; left unbounded the kernel takes 170 and one CTA per SM).
 template <int L, int DMODE, bool POS>
-__global__ void __launch_bounds__(4 * L, 1) k_hio(const HioDev p) {
+__global__ void __launch_bounds__(4 * L, (L == 64) ? 3 : 1) k_hio(const HioDev p) {
     using P = Plane<float, L>;
     using H = HioPlan<L>;
     constexpr int J = P::J, TPL = P::TPL, AP = H::AP;
