@@ -35,12 +35,21 @@ __device__ __forceinline__ double rsqrt_fast(double a) { return rsqrt(a); }
 // z <- A * z / |z|, which is std::polar(A, std::arg(z)) up to rounding (the
 // reciprocal square root is CUDA's rsqrt, a few ulp like the reference's
 // atan2/cos/sin; |z|^2 overflowing to infinity takes the hypot route).
+// a / |z| when |z|^2 overflows: out of line, so that the common path stays
+// a few instructions in every kernel that inlines data_apply
+template <typename T>
+__device__ __noinline__ T modulus_ratio_overflow(T a, T x, T y) { return div_rn(a, hypot(x, y)); }
+
 template <typename T>
 __device__ __forceinline__ Cx<T> data_apply(Cx<T> z, T a, int mode) {
     if (mode == DATA_SKIP_ZERO && a == T(0)) return z;
     const T n = add_rn(mul_rn(z.x, z.x), mul_rn(z.y, z.y));
     if (!(n > T(0))) return z;
-    const T r = isinf(n) ? div_rn(a, hypot(z.x, z.y)) : mul_rn(a, rsqrt_fast(n));
+    T r;
+    if (isinf(n))
+        r = modulus_ratio_overflow(a, z.x, z.y);
+    else
+        r = mul_rn(a, rsqrt_fast(n));
     return {mul_rn(z.x, r), mul_rn(z.y, r)};
 }
 
