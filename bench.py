@@ -46,7 +46,6 @@ def parse():
     ap.add_argument("--angles", type=int, default=90)
     ap.add_argument("--episodes", type=int, default=10)
     ap.add_argument("--iters", type=int, default=10)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
     ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d", "plain2d"], default="carousel",
@@ -151,37 +150,22 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (oracle/_ref: the reference's MklImpl<T> operators + DFTI shim)
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(A, S, size, iters, seconds, threads):
-    """pattern-iterations/s of the reference operator code on the host cores:
-    1 start, `iters` DM iterations per angle over as many angles as fit in
-    about `seconds`.  Returns (rate, sample_description, cores)."""
+def cpu_reference_run(A, S, x0, P, B, size, epi, iters, threads):
+    """The reference operator code (oracle/_ref: MklImpl<float> + the project
+    DFTI shim) through the whole carousel 2D stage on the host cores: the
+    reference driver's call order (src/CPRA_MKL.cpp:35-140) for B starts
+    x0 [P][B][size^2] complex64.  Returns (pattern-iterations/s, seconds,
+    x result, threads used) or None when oracle/_ref is not built."""
     sys.path.insert(0, str(REPO / "oracle"))
     import ref_lib
     if not ref_lib.available():
-        return None, "oracle/_ref not built", 0
+        return None
+    ref_lib.QUIET = True  # the reference constructor's DFTI status lines (rank-3 refusal)
     cores = ref_lib.set_threads(threads)
-    M = N = size
-    MN = M * N
-    rng = np.random.default_rng(0)
-    impl = ref_lib.RefImpl(np.float32, M, N, 1, 1)
-
-    def run(n_angles):
-        x = (rng.uniform(0, 1, MN) + 1j * rng.uniform(0, 1, MN)).astype(np.complex64)
-        t0 = time.perf_counter()
-        for p in range(n_angles):
-            q = p % A.shape[0]
-            t1, t2 = x.copy(), x.copy()
-            impl.dm_iterations(x, t1, t2, np.ascontiguousarray(A[q].ravel()), np.ascontiguousarray(S[q].ravel()),
-                               MN, 1, 0.9, iters)
-        return time.perf_counter() - t0
-
-    t = run(2)
-    per_angle = max(t / 2, 1e-4)
-    n = max(2, int(seconds / per_angle))
-    t = run(n)
-    rate = n * iters / t
-    return rate, f"1 start x {n} angles x {iters} DM iterations at {M}x{N} (reference MklImpl operators, " \
-                 f"project DFTI shim FFT)", cores
+    t0 = time.perf_counter()
+    x = ref_lib.cpra_sample(np.float32, size, size, 1, P, B, A, S, x0, epi, iters, 0, 0.9)
+    t = time.perf_counter() - t0
+    return P * B * epi * iters / t, t, x, cores
 
 
 # ---------------------------------------------------------------------------
@@ -282,40 +266,40 @@ def measured_peak():
 
 # ---------------------------------------------------------------------------
 def run_reference_arm(a, ws, rank):
-    """--impl reference: the reference's CPU operator code on this host's cores."""
+    """--impl reference: the reference's CPU operator code on this host's cores,
+    each step one start through the whole carousel 2D stage (all angles,
+    episodes and iterations of the configuration)."""
     if rank != 0:
         return
     from cpra_b200 import synth
-    d = synth.carousel(n=a.size, P=min(a.angles, 8))
-    threads = os.cpu_count() or 1
     sys.path.insert(0, str(REPO / "oracle"))
     import ref_lib
     if not ref_lib.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcpra_mklref.so is not built"}))
         return
-    cores = ref_lib.set_threads(threads)
+    d = synth.carousel(n=a.size, P=a.angles, seed=1)
+    threads = os.cpu_count() or 1
     M = N = a.size
     MN = M * N
-    impl = ref_lib.RefImpl(np.float32, M, N, 1, 1)
     rng = np.random.default_rng(0)
-    angles_per_step = 4
+    starts_per_step = 1
 
     def step():
-        x = (rng.uniform(0, 1, MN) + 1j * rng.uniform(0, 1, MN)).astype(np.complex64)
-        for p in range(angles_per_step):
-            t1, t2 = x.copy(), x.copy()
-            impl.dm_iterations(x, t1, t2, np.ascontiguousarray(d["A"][p].ravel()),
-                               np.ascontiguousarray(d["S"][p].ravel()), MN, 1, 0.9, a.iters)
+        x0 = (rng.uniform(0, 1, a.angles * MN) + 1j * rng.uniform(0, 1, a.angles * MN)).astype(np.complex64)
+        return cpu_reference_run(d["A"], d["S"], x0, a.angles, starts_per_step, a.size, a.episodes, a.iters,
+                                 threads)
 
+    cores = 0
     for _ in range(a.warmup):
-        step()
-    t0 = time.perf_counter()
+        cores = step()[3]
+    t = 0.0
     for _ in range(a.steps):
-        step()
-    t = time.perf_counter() - t0
-    units = a.steps * angles_per_step * a.iters
+        _, dt, _, cores = step()
+        t += dt
+    units = a.steps * starts_per_step * a.angles * a.episodes * a.iters
     rate = units / t
-    sample = f"1 start x {angles_per_step} angles x {a.iters} DM iterations per step at {M}x{N}"
+    sample = (f"{starts_per_step} start per step through the whole stage: {a.angles} angles x {a.episodes} episodes "
+              f"x {a.iters} DM iterations at {M}x{N}, final projection included")
     line = {
         "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -533,9 +517,12 @@ def main():
             result["carousel3d_adjoint"] = {"error": str(ex)[:200]}
 
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        rate, sample, cores = cpu_reference_rate(d["A"], d["S"], M, IT, a.cpu_seconds, os.cpu_count() or 1)
-        result["cpu_baseline"] = None if rate is None else {
-            "value": rate, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
+        try:
+            cpu = cpu_reference_compare(torch, cpra_b200, a, d, x0, x, A, dev)
+            result["cpu_baseline"] = cpu["cpu_baseline"]
+            result["rfactor_vs_reference"] = cpu["rfactor_vs_reference"]
+        except Exception as ex:  # the baseline must not sink the line
+            result["cpu_baseline"] = {"error": str(ex)[:200]}
 
     if rank == 0:
         print(json.dumps(result), flush=True)
@@ -543,6 +530,58 @@ def main():
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def cpu_reference_compare(torch, cpra_b200, a, d, x0, x, A, dev, starts=2, starts_8=1):
+    """The CPU baseline and the parity of the result at the benchmark's own
+    configuration: the first `starts` starts of the benchmark's initial guesses
+    go through the whole 2D stage on the reference operator code with all host
+    threads (its rate is `cpu_baseline`), and the first `starts_8` again at the
+    reference benchmark's 8 OpenMP threads (src/benchmark_mkl.cpp:258).  Their
+    results are compared with the same starts of the GPU run's result (x, from
+    x0): the mean R-factor over the angles per start, and the fraction of
+    pixels where the supports |x| > 0.1 max|x| of the final projections
+    differ."""
+    P, B, M = a.angles, a.starts, a.size
+    MN = M * M
+    starts = min(starts, B)
+    x0s = x0.view(P, B, MN)[:, :starts].contiguous().cpu().numpy().ravel()
+    run = cpu_reference_run(d["A"], d["S"], x0s, P, starts, M, a.episodes, a.iters, os.cpu_count() or 1)
+    if run is None:
+        return {"cpu_baseline": None, "rfactor_vs_reference": None}
+    rate, secs, x_ref, cores = run
+    x0_8 = x0.view(P, B, MN)[:, :starts_8].contiguous().cpu().numpy().ravel()
+    rate8, secs8, _, cores8 = cpu_reference_run(d["A"], d["S"], x0_8, P, starts_8, M, a.episodes, a.iters, 8)
+    cpu = {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference",
+           "sample": f"{starts} starts of the benchmark's initial guesses through the whole stage ({P} angles x "
+                     f"{a.episodes} episodes x {a.iters} DM iterations at {M}x{M}, final projection): "
+                     f"{secs:.1f} s on {cores} threads",
+           "threads_8": {"value": rate8, "unit": METRIC, "cores": cores8, "seconds": secs8,
+                         "sample": f"{starts_8} start, same stage, 8 OpenMP threads as in the reference "
+                                   f"benchmark"},
+           "note": "reference MklImpl<float> operators compiled unchanged; FFT from the project DFTI shim "
+                   "(oneMKL absent)"}
+    g = x.view(P, B, MN)[:, :starts].contiguous()
+    r = torch.from_numpy(x_ref).to(dev).view(P, starts, MN)
+    one = cpra_b200.B200Impl(M, M, 1, starts)
+    rf_g = np.stack([one.rfactor(g[p].reshape(-1), A[p * MN:(p + 1) * MN], starts) for p in range(P)])
+    rf_r = np.stack([one.rfactor(r[p].reshape(-1), A[p * MN:(p + 1) * MN], starts) for p in range(P)])
+    one.close()
+
+    def support(t):
+        m = t.abs().reshape(P * starts, MN)
+        return m > 0.1 * m.amax(dim=1, keepdim=True)
+
+    sup = float((support(g) != support(r)).float().mean().item())
+    mg, mr = rf_g.mean(axis=0), rf_r.mean(axis=0)
+    rel = np.abs(mg - mr) / mr
+    return {"cpu_baseline": cpu,
+            "rfactor_vs_reference": {
+                "starts": starts, "b200": mg.tolist(), "reference": mr.tolist(), "rel_diff": rel.tolist(),
+                "max_rel_diff": float(rel.max()), "support_mask_diff": sup,
+                "per_pattern_max_rel_diff": float(np.max(np.abs(rf_g - rf_r) / rf_r)),
+                "definition": "mean over the angles of sum | |Forward2D(x)| - A | / sum A (float64) per start; "
+                              "support |x| > 0.1 max|x| per plane of the final projection"}}
 
 
 def episode_3d(torch, cpra_b200, d, dev, iters3d=10):

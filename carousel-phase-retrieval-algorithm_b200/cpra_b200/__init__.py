@@ -21,7 +21,7 @@ from pathlib import Path
 __all__ = [
     "IMPL_TYPE", "CpraB200Error", "B200Impl", "NewCpraImpl", "library_path", "lib",
     "OK", "EARG", "ECUDA", "EUNSUP", "OPT_FUSION", "OPT_SPACE_MODE", "OPT_DATA_MODE", "OPT_SEED",
-    "OPT_KERNEL_TIMING", "OPT_HIO_CHUNK", "OPT_GRAPH", "OPT_LANES", "OPT_IO_CHUNK", "OPT_AUTOTUNE",
+    "OPT_KERNEL_TIMING", "OPT_HIO_CHUNK", "OPT_GRAPH", "OPT_LANES", "OPT_IO_CHUNK", "OPT_AUTOTUNE", "OPT_TMEM",
 ]
 
 OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
@@ -30,6 +30,7 @@ OPT_FUSION, OPT_SPACE_MODE, OPT_DATA_MODE, OPT_SEED, OPT_KERNEL_TIMING, OPT_HIO_
     1, 2, 3, 4, 5, 6, 7, 8
 OPT_IO_CHUNK = 9
 OPT_AUTOTUNE = 10
+OPT_TMEM = 11
 
 _HERE = Path(__file__).resolve().parent
 

@@ -243,6 +243,8 @@ struct cpra_b200_ctx {
     std::vector<GraphEntry> graph_cache;
     // patterns per chunk of the large-plane HIO passes (0: the whole batch)
     uint64_t hio_chunk = 0;
+    // CPRA_B200_OPT_TMEM: the 128 x 128 fused kernels keep their iterates in tensor memory
+    bool tmem = true;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -424,6 +426,7 @@ int launch_fused(cpra_b200_ctx* c, const DmPattern& p, int iters, int mix = MIX_
     a.iters = iters;
     a.space_mode = c->space_mode;
     a.data_mode = c->data_mode;
+    a.tmem = c->tmem ? 1 : 0;
     a.c = p.c;
     a.L = (p.dim == 3) ? c->l : 1;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -762,6 +765,7 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
             c->io_chunk = (uint64_t)value;
             break;
         case CPRA_B200_OPT_AUTOTUNE: c->autotune = value != 0; break;
+        case CPRA_B200_OPT_TMEM: c->tmem = value != 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1053,6 +1057,7 @@ int cpra_b200_dm_iterations(cpra_b200_ctx* c, void* x, void* t1, void* t2, const
     a.iters = iters;
     a.space_mode = c->space_mode;
     a.data_mode = c->data_mode;
+    a.tmem = c->tmem ? 1 : 0;
     a.c = {c->round_t(-1.0 / b), c->round_t(1.0 + 1.0 / b), c->round_t(1.0 / b), c->round_t(1.0 - 1.0 / b),
            c->round_t(b),        1.0,                         c->round_t(-1.0 * b), 1.0};
     return run_dm(c, a, "dm_iterations");
@@ -1183,6 +1188,7 @@ int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t 
     a.sw_every = updates > 0 ? h.sw_every : 0;
     a.positivity = h.positivity ? 1 : 0;
     a.data_mode = c->data_mode;
+    a.tmem = c->tmem ? 1 : 0;
     a.beta = c->round_t(h.beta);
     a.threshold = h.threshold;
     int r = ensure_twiddles(c, j.L);
@@ -1583,6 +1589,7 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
             break;
         case CPRA_B200_OPT_IO_CHUNK: *value = (int64_t)c->io_chunk; break;
         case CPRA_B200_OPT_AUTOTUNE: *value = c->autotune ? 1 : 0; break;
+        case CPRA_B200_OPT_TMEM: *value = c->tmem ? 1 : 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;

@@ -118,6 +118,7 @@ struct DmArgs {
     int data_mode;
     DmCoef c;
     uint64_t L = 1;  // 3D difference map: volumes [batch][L][M][N] (launch_dm3d_iterations)
+    int tmem = 1;    // 128 x 128: x and t2 resident in tensor memory (k_dm_tm) instead of L2 (k_dm)
 };
 bool dm_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_dm_iterations(bool dbl, const DmArgs& a, const void* tw, cudaStream_t st);
@@ -170,6 +171,7 @@ struct HioArgs {
     uint64_t M, N, batch;
     int iters, sw_every, positivity, data_mode;
     double beta, threshold;
+    int tmem = 1;  // 128 x 128: the half of x that k_hio sends through L2 stays in tensor memory
 };
 bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st);

@@ -27,6 +27,7 @@
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
+#include "tmem.cuh"
 
 namespace cpra_b200 {
 
@@ -252,6 +253,211 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) 
     }
 }
 
+// The 128 x 128 kernel with x and t2 resident in tensor memory.
+//
+// Every thread reads and writes x, t1 and t2 only at its own row's split
+// positions (line*L + split_pos(q, j, s)), so these planes are thread-private
+// for the whole launch.  k_dm keeps t1 in registers and sends x and t2 through
+// L2 because the register file is full; here they live in the SM's 256 KB of
+// tensor memory instead, which is exactly one pattern's x and t2 (2 x 128 KB):
+// warp w's threads own lane 32*(w % 4) + lane id, columns (w / 4)*128 .. +127;
+// x at columns 0..63 of that strip (element (j, s) at 8j + 2s, re then im),
+// t2 at 64..127.  Global memory is read when the launch starts (x with the
+// carousel mix, t1 and t2, or t1 = t2 = x) and written once after the last
+// iteration (x, t1, t2), so a launch of `iters` iterations moves each plane
+// through L2/HBM once instead of once per iteration.  The arithmetic is
+// k_dm's, step for step: both write the same bits.
+//
+// 512 columns are allocated per CTA; the 208 KB of shared memory allow one
+// CTA per SM, so the allocation never waits for another CTA.
+template <int SMODE, int DMODE>
+__global__ void __launch_bounds__(512, 1) k_dm_tm(const DmDev p) {
+    constexpr int L = 128;
+    using P = Plane<float, L>;
+    using D = DmPlan<L>;
+    constexpr int J = P::J, TPL = P::TPL;
+    static_assert(TPL == 4 && J == 8 && P::NT == 512, "one 4-value tensor-memory group per (j, all s)");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t tm_base;
+    Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
+    float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::a_bytes());
+    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::a_bytes() + P::tw_bytes());
+    const int t = threadIdx.x, line = t >> 2, q = t & 3, warp = t >> 5;
+    if (warp == 0) tm_alloc(&tm_base, 512);
+    P::F::fill_twiddles(tw, p.tw, t, P::NT);
+    const size_t base = (size_t)blockIdx.x * L * L;
+    Cx<float>* __restrict__ X = p.x + base;
+    Cx<float>* __restrict__ T1 = p.t1 + base;
+    Cx<float>* __restrict__ T2 = p.t2 + base;
+    const Cx<float>* __restrict__ XP = p.xprev + (p.xprev ? base : 0);
+    const Cx<float>* __restrict__ XN = p.xnext + (p.xnext ? base : 0);
+    const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
+    const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
+    for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
+    constexpr bool use_mask = (SMODE == SPACE_THRESHOLD);
+    if constexpr (use_mask) {
+        for (int i = t; i < L * L; i += P::NT) {
+            const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
+            if ((i & 31) == 0) mask[i >> 5] = keep;
+        }
+    }
+    auto space = [&](Cx<float> z, int idx) -> Cx<float> {
+        if constexpr (use_mask)
+            return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
+        else
+            return space_apply(z, S[idx], SMODE);
+    };
+    auto at = [&](int j, int s) { return line * L + P::split_pos(q, j, s); };
+    const bool neg = ((line + q) & 1) != 0;
+    auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
+    tm_fence_before_sync();
+    __syncthreads();
+    tm_fence_after_sync();
+    // this thread's strip: x at xa + 8j, t2 (raw before the first iteration,
+    // then a2*x + b2*S(t2)) at ta + 8j
+    const uint32_t xa = tm_lane_addr(tm_base, warp, (warp >> 2) * 128);
+    const uint32_t ta = xa + 64;
+    float t1r[J][TPL];
+    Cx<float> o[J][TPL];
+    for (int it = 0; it < p.iters; ++it) {
+        const bool last = (it == p.iters - 1);
+#pragma unroll 1
+        for (int ph = 0; ph < 2; ++ph) {
+            if (ph == 0) {
+                if (it > 0) {
+                    // o[j < J/2] holds the previous iteration's new x there;
+                    // t1's registers take it over (as in k_dm)
+#pragma unroll
+                    for (int j = 0; j < J / 2; ++j)
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) {
+                            const Cx<float> xv = o[j][s];
+                            o[j][s] = sgn(Cx<float>{t1r[j][s], 0.0f});
+                            o[j + J / 2][s] = sgn(Cx<float>{t1r[j + J / 2][s], 0.0f});
+                            t1r[j][s] = xv.x;
+                            t1r[j + J / 2][s] = xv.y;
+                        }
+                } else {
+                    // the launch's start: x (after the carousel mix) and t2
+                    // into tensor memory, t1 into the transform registers
+#pragma unroll
+                    for (int j = 0; j < J; ++j) {
+                        Cx<float> xs[TPL];
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) {
+                            const int idx = at(j, s);
+                            Cx<float> xv = X[idx];
+                            if (!p.init_from_x) {
+                            } else if (p.mix == MIX_FIRST) {
+                                xv = merge_apply(XN[idx], xv, 0.5f, 0.5f);
+                            } else if (p.mix == MIX_LAST) {
+                                xv = merge_apply(XP[idx], xv, 0.5f, 0.5f);
+                            } else if (p.mix == MIX_MIDDLE) {
+                                xv = merge_apply(XP[idx], xv, 0.5f, 0.0f);
+                                xv = merge_apply(XN[idx], xv, 0.5f, 1.0f);
+                            }
+                            xs[s] = xv;
+                            if (j < J / 2) {
+                                t1r[j][s] = xv.x;
+                                t1r[j + J / 2][s] = xv.y;
+                            }
+                        }
+                        tm_st4(xa + 8 * j, xs);
+                        if (p.init_from_x) {
+#pragma unroll
+                            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(xs[s]);
+                        } else {
+#pragma unroll
+                            for (int s = 0; s < TPL; ++s) {
+                                o[j][s] = sgn(T1[at(j, s)]);
+                                xs[s] = T2[at(j, s)];
+                            }
+                            tm_st4(ta + 8 * j, xs);
+                        }
+                    }
+                }
+            } else if (it == 0) {
+                // t2 <- a2*x + b2*S(t2) (t2 = x on an angle's start); from the
+                // second iteration on the first half's last step loaded it
+#pragma unroll
+                for (int j = 0; j < J; ++j) {
+                    Cx<float> xv[TPL];
+                    tm_ld4(xa + 8 * j, xv);
+                    if (p.init_from_x) {
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) o[j][s] = xv[s];
+                    } else {
+                        tm_ld4(ta + 8 * j, o[j]);
+                    }
+#pragma unroll
+                    for (int s = 0; s < TPL; ++s)
+                        o[j][s] = sgn(merge_apply(xv[s], space(o[j][s], at(j, s)), p.a2, p.b2));
+                }
+            }
+            P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+            __syncthreads();
+            modulus_columns<L, DMODE>(buf, tw, As, line, q);
+            __syncthreads();
+            P::template row_from_buf<true>(o, buf, tw, line, q);
+            if (ph == 0) {
+                // t1 <- S(a1*x + b1*t1'); o[j] then takes the second half's
+                // input a2*x + b2*S(t2) from tensor memory once consumed
+#pragma unroll
+                for (int j = 0; j < J; ++j) {
+                    Cx<float> xr[TPL];
+                    if (j >= J / 2) tm_ld4(xa + 8 * j, xr);
+#pragma unroll
+                    for (int s = 0; s < TPL; ++s) {
+                        const Cx<float> val = sgn(cscale(o[j][s], p.scale));
+                        const Cx<float> xv = (j < J / 2) ? Cx<float>{t1r[j][s], t1r[j + J / 2][s]} : xr[s];
+                        const Cx<float> m = space(merge_apply(xv, val, p.a1, p.b1), at(j, s));
+                        t1r[j][s] = m.x;
+                        if (last) T1[at(j, s)] = m;
+                    }
+                    if (it > 0) {
+                        tm_ld4(ta + 8 * j, o[j]);
+#pragma unroll
+                        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(o[j][s]);
+                    }
+                }
+            } else {
+                // x <- a3*t1 + b3*x; x <- a4*t2 + b4*x; the next iteration's
+                // a2*x + b2*S(t2); the new x stays in o[j] (j < J/2 carry it
+                // into the next first half)
+#pragma unroll
+                for (int j = 0; j < J; ++j) {
+                    Cx<float> xr[TPL];
+                    tm_ld4(xa + 8 * j, xr);
+#pragma unroll
+                    for (int s = 0; s < TPL; ++s) {
+                        const int idx = at(j, s);
+                        const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
+                        const Cx<float> x1 = merge_apply(Cx<float>{t1r[j][s], 0.0f}, xr[s], p.a3, p.b3);
+                        const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
+                        if (last) {
+                            X[idx] = xn;
+                            T2[idx] = t2n;
+                        } else {
+                            xr[s] = merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                        }
+                        o[j][s] = xn;
+                    }
+                    if (!last) {
+                        tm_st4(xa + 8 * j, o[j]);
+                        tm_st4(ta + 8 * j, xr);
+                    }
+                }
+            }
+        }
+    }
+    tm_wait_st();
+    tm_fence_before_sync();
+    __syncthreads();
+    tm_fence_after_sync();
+    if (warp == 0) tm_free(tm_base, 512);
+}
+
 template <int L>
 cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     DmDev d;
@@ -285,6 +491,14 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
                                                : k_dm<L, SPACE_THRESHOLD, DATA_SKIP_ZERO>)
                  : (a.data_mode == DATA_ALWAYS ? k_dm<L, SPACE_POSITIVE_SCALED, DATA_ALWAYS>
                                                : k_dm<L, SPACE_POSITIVE_SCALED, DATA_SKIP_ZERO>);
+    if constexpr (L == 128) {
+        if (a.tmem)
+            k = (a.space_mode == SPACE_THRESHOLD)
+                    ? (a.data_mode == DATA_ALWAYS ? k_dm_tm<SPACE_THRESHOLD, DATA_ALWAYS>
+                                                  : k_dm_tm<SPACE_THRESHOLD, DATA_SKIP_ZERO>)
+                    : (a.data_mode == DATA_ALWAYS ? k_dm_tm<SPACE_POSITIVE_SCALED, DATA_ALWAYS>
+                                                  : k_dm_tm<SPACE_POSITIVE_SCALED, DATA_SKIP_ZERO>);
+    }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<(unsigned)a.batch, 4 * L, smem, st>>>(d);

@@ -18,6 +18,9 @@ import numpy as np
 _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "_ref" / "libcpra_mklref.so"
 _lib = None
+# True: the reference's constructor/destructor status lines (below) are
+# discarded instead of going to stderr
+QUIET = False
 
 
 def available() -> bool:
@@ -67,19 +70,23 @@ def set_threads(n: int) -> int:
 def _c_stdout_to_stderr():
     """The reference's constructor and destructor report DFTI failures with
     printf (include/MKL_Impl.hpp:28-79, 167-179; its 3D descriptor is built
-    from the 2D length array and the shim refuses it).  Those lines go to
-    stderr here, so that a caller's stdout carries only its own output."""
+    from the 2D length array and the shim refuses it, "shim DFTI: unsupported
+    configuration").  Those lines go to stderr here, so that a caller's stdout
+    carries only its own output, or nowhere with QUIET set."""
     libc = C.CDLL(None)
     sys.stdout.flush()
     libc.fflush(None)
     saved = os.dup(1)
+    sink = os.open(os.devnull, os.O_WRONLY) if QUIET else 2
     try:
-        os.dup2(2, 1)
+        os.dup2(sink, 1)
         yield
     finally:
         libc.fflush(None)
         os.dup2(saved, 1)
         os.close(saved)
+        if QUIET:
+            os.close(sink)
 
 
 def _p(a: np.ndarray):
@@ -154,8 +161,9 @@ def cpra_sample(T, M, N, L, P, B, A, S, x0, epi, iters, pre_iter, beta):
     A = np.ascontiguousarray(np.asarray(A, T).ravel())
     S = np.ascontiguousarray(np.asarray(S, T).ravel())
     err = np.zeros(P * B, T)
-    ok = lib().cpra_ref_cpra_sample(dbl, M, N, L, P, B, _p(A), _p(S), _p(x), epi, iters, pre_iter,
-                                    float(beta), _p(err))
+    with _c_stdout_to_stderr():
+        ok = lib().cpra_ref_cpra_sample(dbl, M, N, L, P, B, _p(A), _p(S), _p(x), epi, iters, pre_iter,
+                                        float(beta), _p(err))
     if not ok:
         raise ValueError("cpra_ref_cpra_sample rejected its arguments")
     return x
