@@ -150,11 +150,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU reference (oracle/_ref: the reference's MklImpl<T> operators + DFTI shim)
 # ---------------------------------------------------------------------------
-def cpu_reference_run(A, S, x0, P, B, size, epi, iters, threads):
+def cpu_reference_run(A, S, x0, P, B, size, epi, iters, threads, T=np.float32):
     """The reference operator code (oracle/_ref: MklImpl<float> + the project
     DFTI shim) through the whole carousel 2D stage on the host cores: the
     reference driver's call order (src/CPRA_MKL.cpp:35-140) for B starts
-    x0 [P][B][size^2] complex64.  Returns (pattern-iterations/s, seconds,
+    x0 [P][B][size^2] complex64, in the precision T (the reference builds
+    MklImpl<float> and MklImpl<double>).  Returns (pattern-iterations/s, seconds,
     x result, threads used) or None when oracle/_ref is not built."""
     sys.path.insert(0, str(REPO / "oracle"))
     import ref_lib
@@ -163,7 +164,7 @@ def cpu_reference_run(A, S, x0, P, B, size, epi, iters, threads):
     ref_lib.QUIET = True  # the reference constructor's DFTI status lines (rank-3 refusal)
     cores = ref_lib.set_threads(threads)
     t0 = time.perf_counter()
-    x = ref_lib.cpra_sample(np.float32, size, size, 1, P, B, A, S, x0, epi, iters, 0, 0.9)
+    x = ref_lib.cpra_sample(T, size, size, 1, P, B, A, S, x0, epi, iters, 0, 0.9)
     t = time.perf_counter() - t0
     return P * B * epi * iters / t, t, x, cores
 
@@ -550,6 +551,8 @@ def cpu_reference_compare(torch, cpra_b200, a, d, x0, x, A, dev, starts=2, start
     if run is None:
         return {"cpu_baseline": None, "rfactor_vs_reference": None}
     rate, secs, x_ref, cores = run
+    x_ref64 = cpu_reference_run(d["A"], d["S"], x0s, P, starts, M, a.episodes, a.iters, os.cpu_count() or 1,
+                                T=np.float64)[2]
     x0_8 = x0.view(P, B, MN)[:, :starts_8].contiguous().cpu().numpy().ravel()
     rate8, secs8, _, cores8 = cpu_reference_run(d["A"], d["S"], x0_8, P, starts_8, M, a.episodes, a.iters, 8)
     cpu = {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference",
@@ -563,9 +566,11 @@ def cpu_reference_compare(torch, cpra_b200, a, d, x0, x, A, dev, starts=2, start
                    "(oneMKL absent)"}
     g = x.view(P, B, MN)[:, :starts].contiguous()
     r = torch.from_numpy(x_ref).to(dev).view(P, starts, MN)
+    r64 = torch.from_numpy(x_ref64.astype(np.complex64)).to(dev).view(P, starts, MN)
     one = cpra_b200.B200Impl(M, M, 1, starts)
     rf_g = np.stack([one.rfactor(g[p].reshape(-1), A[p * MN:(p + 1) * MN], starts) for p in range(P)])
     rf_r = np.stack([one.rfactor(r[p].reshape(-1), A[p * MN:(p + 1) * MN], starts) for p in range(P)])
+    rf_64 = np.stack([one.rfactor(r64[p].reshape(-1), A[p * MN:(p + 1) * MN], starts) for p in range(P)])
     one.close()
 
     def support(t):
@@ -573,15 +578,26 @@ def cpu_reference_compare(torch, cpra_b200, a, d, x0, x, A, dev, starts=2, start
         return m > 0.1 * m.amax(dim=1, keepdim=True)
 
     sup = float((support(g) != support(r)).float().mean().item())
-    mg, mr = rf_g.mean(axis=0), rf_r.mean(axis=0)
+    sup64 = float((support(g) != support(r64)).float().mean().item())
+    sup_ref = float((support(r) != support(r64)).float().mean().item())
+    mg, mr, m64 = rf_g.mean(axis=0), rf_r.mean(axis=0), rf_64.mean(axis=0)
     rel = np.abs(mg - mr) / mr
+    rel64 = np.abs(mg - m64) / m64
+    ref_rel = np.abs(mr - m64) / m64
     return {"cpu_baseline": cpu,
             "rfactor_vs_reference": {
-                "starts": starts, "b200": mg.tolist(), "reference": mr.tolist(), "rel_diff": rel.tolist(),
-                "max_rel_diff": float(rel.max()), "support_mask_diff": sup,
-                "per_pattern_max_rel_diff": float(np.max(np.abs(rf_g - rf_r) / rf_r)),
-                "definition": "mean over the angles of sum | |Forward2D(x)| - A | / sum A (float64) per start; "
-                              "support |x| > 0.1 max|x| per plane of the final projection"}}
+                "starts": starts, "b200": mg.tolist(), "reference": mr.tolist(), "reference_f64": m64.tolist(),
+                "rel_diff": rel.tolist(), "max_rel_diff": float(rel.max()),
+                "rel_diff_vs_f64": rel64.tolist(), "reference_f32_vs_f64": ref_rel.tolist(),
+                "mean_rel_diff": float(abs(mg.mean() - mr.mean()) / mr.mean()),
+                "mean_rel_diff_vs_f64": float(abs(mg.mean() - m64.mean()) / m64.mean()),
+                "support_mask_diff": sup, "support_mask_diff_vs_f64": sup64,
+                "support_mask_diff_reference_f32_vs_f64": sup_ref,
+                "definition": "mean over the angles of sum | |Forward2D(x)| - A | / sum A (float64) per start, "
+                              "from the same initial guesses through the reference operators in float "
+                              "(reference) and double (reference_f64); support |x| > 0.1 max|x| per plane of "
+                              "the final projection; the iteration is chaotic, so the reference's own float "
+                              "and double builds differ by comparable amounts"}}
 
 
 def episode_3d(torch, cpra_b200, d, dev, iters3d=10):
