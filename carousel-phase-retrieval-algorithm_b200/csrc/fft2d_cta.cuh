@@ -1,9 +1,16 @@
 // One L x L complex plane resident in one CTA's shared memory.
 //
-// 4*L threads; thread t works on line t/4 (a row in row passes, a column in
-// column passes) as rank q = t%4 of a 4-thread group inside one warp.  The
-// plane lives in `buf` with row stride LS = L + 4 (padding that keeps the
-// natural-order row and column accesses of a half-warp on distinct banks).
+// TPL*L threads (TPL = 4, or 8 for the float 128 x 128 plane); thread t works
+// on one line (a row in row passes, a column in column passes) as rank
+// q = t % TPL of a TPL-thread group inside one warp.  The plane lives in `buf`
+// with row stride LS, padding that keeps every pass's accesses of a half-warp
+// on distinct banks:
+//   TPL = 4: LS = L + 4; a warp's 8 groups take 8 consecutive lines in both
+//            passes;
+//   TPL = 8: LS = L + 2; a column pass's warp takes 4 consecutive columns,
+//            a row pass's warp takes rows r, r + 4, r + 8, r + 12 (the two
+//            rows of a half-warp are 4 apart, so their 8 + 8 slots fall on
+//            16 distinct bank pairs at this stride).
 //
 // The per-operator transforms (Forward2D / Backward2D) and the fused
 // difference-map kernel are built from the same four steps below, so they
@@ -17,14 +24,25 @@
 
 namespace cpra_b200 {
 
-template <typename T, int L>
+template <typename T, int L, int TPL_ = 4>
 struct Plane {
-    static constexpr int TPL = 4;
+    static constexpr int TPL = TPL_;
+    static_assert(TPL == 4 || TPL == 8, "4 or 8 threads per line");
     static constexpr int R = L / TPL;
     static constexpr int J = R / TPL;
-    static constexpr int LS = L + TPL;
+    static constexpr int LS = (TPL == 8) ? L + 2 : L + TPL;
     static constexpr int NT = L * TPL;
     using F = LineFFT<T, L, TPL>;
+
+    // the line of thread t in row passes and in column passes, and its rank
+    __device__ __forceinline__ static int row_of(int t) {
+        if constexpr (TPL == 8)
+            return ((t >> 7) << 4) + ((t >> 5) & 3) + 4 * ((t >> 3) & 3);
+        else
+            return t / TPL;
+    }
+    __device__ __forceinline__ static int col_of(int t) { return t / TPL; }
+    __device__ __forceinline__ static int rank_of(int t) { return t % TPL; }
 
     static constexpr int TW_ENTRIES = F::TW_ENTRIES;
 
@@ -85,6 +103,13 @@ struct Plane {
         F::template natural_to_split<INV>(v, o, buf + r * LS, 1, tw, q);
     }
 };
+
+// Threads per line of the single-CTA plane transforms: 8 for the float
+// 128 x 128 plane (1024 threads, 16 values each), else 4.  Every kernel that
+// transforms such a plane (the per-operator transforms and the fused
+// difference map) uses this split, so they round identically.
+template <typename T, int L>
+__host__ __device__ constexpr int plane_tpl() { return (sizeof(T) == 4 && L == 128) ? 8 : 4; }
 
 // x * (-1)^n, exact
 template <typename T>

@@ -50,28 +50,46 @@ struct DmDev {
     int iters, space_mode, data_mode;
 };
 
-// Shared memory of one CTA: the plane buffer, A with row pitch L + 8 (the
-// column pass reads A[f][c] for 4 rows f and 8 columns c per warp: distinct
-// banks), the twiddle table, and the support as a bit mask (SpaceConstraint's
-// threshold test evaluated once per launch: bit set where the value is kept).
+// The plane of the fused kernel: the same thread split as the per-operator
+// transforms of this size (plane_tpl), so both round identically.
+template <int L>
+using DmP = Plane<float, L, plane_tpl<float, L>()>;
+
+// Shared memory of one CTA: the plane buffer, A with row pitch AP, the
+// twiddle table, and the support as a bit mask (SpaceConstraint's threshold
+// test evaluated once per launch: bit set where the value is kept), MP words
+// per row.  The column pass reads A[f][c] for the TPL ranks' rows f and the
+// warp's 32 / TPL columns c: AP = L + 8 (4 ranks x 8 columns) or L + 4
+// (8 ranks x 4 columns) puts them on distinct banks.  With 8 threads per line
+// a row pass's warp takes rows 4 apart, and a mask row pitch of L/32 + 1
+// words keeps their mask words on distinct banks.
 template <int L>
 struct DmPlan {
-    using P = Plane<float, L>;
-    static constexpr int AP = L + 8;
-    static constexpr int MASK_WORDS = L * L / 32;
+    using P = DmP<L>;
+    static constexpr int AP = (P::TPL == 8) ? L + 4 : L + 8;
+    static constexpr int MP = L / 32 + ((P::TPL == 8) ? 1 : 0);
+    static constexpr int MASK_WORDS = L * MP;
     static constexpr size_t a_bytes() { return sizeof(float) * (size_t)L * AP; }
     static constexpr size_t smem_bytes() {
         return P::buf_bytes() + a_bytes() + P::tw_bytes() + sizeof(uint32_t) * MASK_WORDS;
     }
+    __device__ __forceinline__ static bool mask_keep(const uint32_t* mask, int idx) {
+        return (mask[(idx / L) * MP + (idx % L) / 32] >> (idx & 31)) & 1u;
+    }
+    // the CTA's threads fill the mask from the support plane S
+    __device__ __forceinline__ static void fill_mask(uint32_t* mask, const float* __restrict__ S, int t) {
+        for (int i = t; i < L * L; i += P::NT) {
+            const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
+            if ((i & 31) == 0) mask[(i / L) * MP + (i % L) / 32] = keep;
+        }
+    }
 };
-
-__device__ __forceinline__ bool mask_keep(const uint32_t* mask, int idx) { return (mask[idx >> 5] >> (idx & 31)) & 1u; }
 
 // column forward transform, modulus projection (DataConstraint mode DMODE),
 // column inverse transform
 template <int L, int DMODE>
 __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>* tw, const float* As, int c, int q) {
-    using P = Plane<float, L>;
+    using P = DmP<L>;
     constexpr int AP = DmPlan<L>::AP;
     Cx<float> o[P::J][P::TPL];
     P::template col_from_buf<false>(o, buf, tw, c, q);
@@ -90,8 +108,8 @@ __device__ __forceinline__ void modulus_columns(Cx<float>* buf, const Cx<float>*
 // At 64^2 two CTAs share an SM (at most 128 registers, no spills; left
 // unbounded the kernel takes 155 and one CTA per SM).
 template <int L, int SMODE, int DMODE>
-__global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) {
-    using P = Plane<float, L>;
+__global__ void __launch_bounds__(DmP<L>::NT, (L == 64) ? 2 : 1) k_dm(const DmDev p) {
+    using P = DmP<L>;
     using D = DmPlan<L>;
     constexpr int J = P::J, TPL = P::TPL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -99,7 +117,7 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) 
     float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
     Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::a_bytes());
     uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::a_bytes() + P::tw_bytes());
-    const int t = threadIdx.x, line = t >> 2, q = t & 3;
+    const int t = threadIdx.x, line = P::row_of(t), col = P::col_of(t), q = P::rank_of(t);
     P::F::fill_twiddles(tw, p.tw, t, P::NT);
     const size_t base = (size_t)blockIdx.x * L * L;
     Cx<float>* __restrict__ X = p.x + base;
@@ -111,16 +129,11 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) 
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
     for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
     constexpr bool use_mask = (SMODE == SPACE_THRESHOLD);
-    if constexpr (use_mask) {
-        for (int i = t; i < L * L; i += P::NT) {
-            const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
-            if ((i & 31) == 0) mask[i >> 5] = keep;
-        }
-    }
+    if constexpr (use_mask) D::fill_mask(mask, S, t);
     // SpaceConstraint of element idx, from the mask or the support plane
     auto space = [&](Cx<float> z, int idx) -> Cx<float> {
         if constexpr (use_mask)
-            return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
+            return {D::mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
         else
             return space_apply(z, S[idx], SMODE);
     };
@@ -218,7 +231,7 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) 
             }
             P::template rows_split_to_buf<false>(o, buf, tw, line, q);
             __syncthreads();
-            modulus_columns<L, DMODE>(buf, tw, As, line, q);
+            modulus_columns<L, DMODE>(buf, tw, As, col, q);
             __syncthreads();
             P::template row_from_buf<true>(o, buf, tw, line, q);
             if (ph == 0) {
@@ -253,37 +266,40 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 2 : 1) k_dm(const DmDev p) 
     }
 }
 
-// The 128 x 128 kernel with x and t2 resident in tensor memory.
+// The 128 x 128 kernel with its iterates resident in tensor memory.
 //
 // Every thread reads and writes x, t1 and t2 only at its own row's split
-// positions (line*L + split_pos(q, j, s)), so these planes are thread-private
-// for the whole launch.  k_dm keeps t1 in registers and sends x and t2 through
-// L2 because the register file is full; here they live in the SM's 256 KB of
-// tensor memory instead, which is exactly one pattern's x and t2 (2 x 128 KB):
-// warp w's threads own lane 32*(w % 4) + lane id, columns (w / 4)*128 .. +127;
-// x at columns 0..63 of that strip (element (j, s) at 8j + 2s, re then im),
-// t2 at 64..127.  Global memory is read when the launch starts (x with the
-// carousel mix, t1 and t2, or t1 = t2 = x) and written once after the last
-// iteration (x, t1, t2), so a launch of `iters` iterations moves each plane
-// through L2/HBM once instead of once per iteration.  The arithmetic is
-// k_dm's, step for step: both write the same bits.
+// positions (row*L + split_pos(q, j, s)), so these planes are thread-private
+// for the whole launch.  They live in the SM's 256 KB of tensor memory, which
+// holds one pattern's x and t2 (2 x 128 KB) exactly; t1, real after the
+// support projection, takes t2's place between the first half's last step
+// (which reads t2) and the second half's last step (which writes it).  So a
+// thread's registers hold only the 16 values of its line segment, and the
+// CTA runs 1024 threads (8 per line, 32 warps per SM) where k_dm runs 512.
+// Warp w's threads own lane 32*(w % 4) + lane id, columns (w / 4)*64 .. +63:
+// x at 0..31 (element (j, s) at 2*(8j + s), re then im), t2 or t1 at 32..63.
+// Global memory is read when the launch starts (x with the carousel mix, t1
+// and t2, or t1 = t2 = x) and written after the last iteration (x, t1, t2),
+// so a launch of `iters` iterations moves each plane through L2/HBM once
+// instead of once per iteration.  The arithmetic is k_dm's, step for step:
+// both write the same bits.
 //
-// 512 columns are allocated per CTA; the 208 KB of shared memory allow one
+// 512 columns are allocated per CTA; the 199 KB of shared memory allow one
 // CTA per SM, so the allocation never waits for another CTA.
 template <int SMODE, int DMODE>
-__global__ void __launch_bounds__(512, 1) k_dm_tm(const DmDev p) {
+__global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
     constexpr int L = 128;
-    using P = Plane<float, L>;
+    using P = DmP<L>;
     using D = DmPlan<L>;
     constexpr int J = P::J, TPL = P::TPL;
-    static_assert(TPL == 4 && J == 8 && P::NT == 512, "one 4-value tensor-memory group per (j, all s)");
+    static_assert(TPL == 8 && J == 2 && P::NT == 1024, "two 8-value groups per thread, 32 warps");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t tm_base;
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
     float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
     Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::a_bytes());
     uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::a_bytes() + P::tw_bytes());
-    const int t = threadIdx.x, line = t >> 2, q = t & 3, warp = t >> 5;
+    const int t = threadIdx.x, row = P::row_of(t), col = P::col_of(t), q = P::rank_of(t), warp = t >> 5;
     if (warp == 0) tm_alloc(&tm_base, 512);
     P::F::fill_twiddles(tw, p.tw, t, P::NT);
     const size_t base = (size_t)blockIdx.x * L * L;
@@ -296,158 +312,143 @@ __global__ void __launch_bounds__(512, 1) k_dm_tm(const DmDev p) {
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
     for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
     constexpr bool use_mask = (SMODE == SPACE_THRESHOLD);
-    if constexpr (use_mask) {
-        for (int i = t; i < L * L; i += P::NT) {
-            const unsigned keep = __ballot_sync(0xffffffffu, !space_zero(S[i]));
-            if ((i & 31) == 0) mask[i >> 5] = keep;
-        }
-    }
+    if constexpr (use_mask) D::fill_mask(mask, S, t);
     auto space = [&](Cx<float> z, int idx) -> Cx<float> {
         if constexpr (use_mask)
-            return {mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
+            return {D::mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
         else
             return space_apply(z, S[idx], SMODE);
     };
-    auto at = [&](int j, int s) { return line * L + P::split_pos(q, j, s); };
-    const bool neg = ((line + q) & 1) != 0;
+    auto at = [&](int j, int s) { return row * L + P::split_pos(q, j, s); };
+    const bool neg = ((row + q) & 1) != 0;
     auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
     tm_fence_before_sync();
     __syncthreads();
     tm_fence_after_sync();
-    // this thread's strip: x at xa + 8j, t2 (raw before the first iteration,
-    // then a2*x + b2*S(t2)) at ta + 8j
-    const uint32_t xa = tm_lane_addr(tm_base, warp, (warp >> 2) * 128);
-    const uint32_t ta = xa + 64;
-    float t1r[J][TPL];
+    // this thread's strip; the values of (j, s) with s in [4h, 4h + 4) are
+    // group g = 2j + h: x at xa + 8g, t2 (or t1, 4 columns) at ta + 8g
+    const uint32_t xa = tm_lane_addr(tm_base, warp, (warp >> 2) * 64);
+    const uint32_t ta = xa + 32;
     Cx<float> o[J][TPL];
+    // the launch's start: x (after the carousel mix) and t2 into tensor
+    // memory, the first half's input t1 into o
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            Cx<float> xs[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int idx = at(j, 4 * h + u);
+                Cx<float> xv = X[idx];
+                if (!p.init_from_x) {
+                } else if (p.mix == MIX_FIRST) {
+                    xv = merge_apply(XN[idx], xv, 0.5f, 0.5f);
+                } else if (p.mix == MIX_LAST) {
+                    xv = merge_apply(XP[idx], xv, 0.5f, 0.5f);
+                } else if (p.mix == MIX_MIDDLE) {
+                    xv = merge_apply(XP[idx], xv, 0.5f, 0.0f);
+                    xv = merge_apply(XN[idx], xv, 0.5f, 1.0f);
+                }
+                xs[u] = xv;
+            }
+            tm_st4(xa + 8 * (2 * j + h), xs);
+            if (p.init_from_x) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) o[j][4 * h + u] = sgn(xs[u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = at(j, 4 * h + u);
+                    o[j][4 * h + u] = sgn(T1[idx]);
+                    xs[u] = T2[idx];
+                }
+                tm_st4(ta + 8 * (2 * j + h), xs);
+            }
+        }
     for (int it = 0; it < p.iters; ++it) {
         const bool last = (it == p.iters - 1);
 #pragma unroll 1
         for (int ph = 0; ph < 2; ++ph) {
+            // first half:  t1' = Backward2D(DataConstraint(Forward2D(t1)))
+            // second half: t2' = Backward2D(DataConstraint(Forward2D(a2*x + b2*S(t2))))
+            P::template rows_split_to_buf<false>(o, buf, tw, row, q);
+            __syncthreads();
+            modulus_columns<L, DMODE>(buf, tw, As, col, q);
+            __syncthreads();
+            P::template row_from_buf<true>(o, buf, tw, row, q);
             if (ph == 0) {
-                if (it > 0) {
-                    // o[j < J/2] holds the previous iteration's new x there;
-                    // t1's registers take it over (as in k_dm)
+                // t1 <- S(a1*x + b1*t1') into t2's columns once t2 is read;
+                // o takes the second half's input
 #pragma unroll
-                    for (int j = 0; j < J / 2; ++j)
+                for (int j = 0; j < J; ++j)
 #pragma unroll
-                        for (int s = 0; s < TPL; ++s) {
-                            const Cx<float> xv = o[j][s];
-                            o[j][s] = sgn(Cx<float>{t1r[j][s], 0.0f});
-                            o[j + J / 2][s] = sgn(Cx<float>{t1r[j + J / 2][s], 0.0f});
-                            t1r[j][s] = xv.x;
-                            t1r[j + J / 2][s] = xv.y;
+                    for (int h = 0; h < 2; ++h) {
+                        const int g = 2 * j + h;
+                        Cx<float> xr[4], tv[4];
+                        float t1v[4];
+                        tm_ld4(xa + 8 * g, xr);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int s = 4 * h + u;
+                            const Cx<float> val = sgn(cscale(o[j][s], p.scale));
+                            const Cx<float> m = space(merge_apply(xr[u], val, p.a1, p.b1), at(j, s));
+                            t1v[u] = m.x;
+                            if (last) T1[at(j, s)] = m;
                         }
-                } else {
-                    // the launch's start: x (after the carousel mix) and t2
-                    // into tensor memory, t1 into the transform registers
+                        if (it > 0) {
+                            // a2*x + b2*S(t2), formed by the previous iteration
+                            tm_ld4(ta + 8 * g, tv);
 #pragma unroll
-                    for (int j = 0; j < J; ++j) {
-                        Cx<float> xs[TPL];
-#pragma unroll
-                        for (int s = 0; s < TPL; ++s) {
-                            const int idx = at(j, s);
-                            Cx<float> xv = X[idx];
-                            if (!p.init_from_x) {
-                            } else if (p.mix == MIX_FIRST) {
-                                xv = merge_apply(XN[idx], xv, 0.5f, 0.5f);
-                            } else if (p.mix == MIX_LAST) {
-                                xv = merge_apply(XP[idx], xv, 0.5f, 0.5f);
-                            } else if (p.mix == MIX_MIDDLE) {
-                                xv = merge_apply(XP[idx], xv, 0.5f, 0.0f);
-                                xv = merge_apply(XN[idx], xv, 0.5f, 1.0f);
-                            }
-                            xs[s] = xv;
-                            if (j < J / 2) {
-                                t1r[j][s] = xv.x;
-                                t1r[j + J / 2][s] = xv.y;
-                            }
-                        }
-                        tm_st4(xa + 8 * j, xs);
-                        if (p.init_from_x) {
-#pragma unroll
-                            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(xs[s]);
+                            for (int u = 0; u < 4; ++u) o[j][4 * h + u] = sgn(tv[u]);
                         } else {
+                            // t2 from the buffer, or t2 = x on an angle's start
+                            if (p.init_from_x) {
 #pragma unroll
-                            for (int s = 0; s < TPL; ++s) {
-                                o[j][s] = sgn(T1[at(j, s)]);
-                                xs[s] = T2[at(j, s)];
+                                for (int u = 0; u < 4; ++u) tv[u] = xr[u];
+                            } else {
+                                tm_ld4(ta + 8 * g, tv);
                             }
-                            tm_st4(ta + 8 * j, xs);
+#pragma unroll
+                            for (int u = 0; u < 4; ++u)
+                                o[j][4 * h + u] =
+                                    sgn(merge_apply(xr[u], space(tv[u], at(j, 4 * h + u)), p.a2, p.b2));
                         }
+                        tm_st4r(ta + 8 * g, t1v);
                     }
-                }
-            } else if (it == 0) {
-                // t2 <- a2*x + b2*S(t2) (t2 = x on an angle's start); from the
-                // second iteration on the first half's last step loaded it
-#pragma unroll
-                for (int j = 0; j < J; ++j) {
-                    Cx<float> xv[TPL];
-                    tm_ld4(xa + 8 * j, xv);
-                    if (p.init_from_x) {
-#pragma unroll
-                        for (int s = 0; s < TPL; ++s) o[j][s] = xv[s];
-                    } else {
-                        tm_ld4(ta + 8 * j, o[j]);
-                    }
-#pragma unroll
-                    for (int s = 0; s < TPL; ++s)
-                        o[j][s] = sgn(merge_apply(xv[s], space(o[j][s], at(j, s)), p.a2, p.b2));
-                }
-            }
-            P::template rows_split_to_buf<false>(o, buf, tw, line, q);
-            __syncthreads();
-            modulus_columns<L, DMODE>(buf, tw, As, line, q);
-            __syncthreads();
-            P::template row_from_buf<true>(o, buf, tw, line, q);
-            if (ph == 0) {
-                // t1 <- S(a1*x + b1*t1'); o[j] then takes the second half's
-                // input a2*x + b2*S(t2) from tensor memory once consumed
-#pragma unroll
-                for (int j = 0; j < J; ++j) {
-                    Cx<float> xr[TPL];
-                    if (j >= J / 2) tm_ld4(xa + 8 * j, xr);
-#pragma unroll
-                    for (int s = 0; s < TPL; ++s) {
-                        const Cx<float> val = sgn(cscale(o[j][s], p.scale));
-                        const Cx<float> xv = (j < J / 2) ? Cx<float>{t1r[j][s], t1r[j + J / 2][s]} : xr[s];
-                        const Cx<float> m = space(merge_apply(xv, val, p.a1, p.b1), at(j, s));
-                        t1r[j][s] = m.x;
-                        if (last) T1[at(j, s)] = m;
-                    }
-                    if (it > 0) {
-                        tm_ld4(ta + 8 * j, o[j]);
-#pragma unroll
-                        for (int s = 0; s < TPL; ++s) o[j][s] = sgn(o[j][s]);
-                    }
-                }
             } else {
-                // x <- a3*t1 + b3*x; x <- a4*t2 + b4*x; the next iteration's
-                // a2*x + b2*S(t2); the new x stays in o[j] (j < J/2 carry it
-                // into the next first half)
+                // x <- a3*t1 + b3*x; x <- a4*t2' + b4*x; t2's columns take the
+                // next iteration's a2*x + b2*S(t2'); o takes its first half's
+                // input t1
 #pragma unroll
-                for (int j = 0; j < J; ++j) {
-                    Cx<float> xr[TPL];
-                    tm_ld4(xa + 8 * j, xr);
+                for (int j = 0; j < J; ++j)
 #pragma unroll
-                    for (int s = 0; s < TPL; ++s) {
-                        const int idx = at(j, s);
-                        const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
-                        const Cx<float> x1 = merge_apply(Cx<float>{t1r[j][s], 0.0f}, xr[s], p.a3, p.b3);
-                        const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
-                        if (last) {
-                            X[idx] = xn;
-                            T2[idx] = t2n;
-                        } else {
-                            xr[s] = merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                    for (int h = 0; h < 2; ++h) {
+                        const int g = 2 * j + h;
+                        Cx<float> xr[4], tn[4];
+                        float t1v[4];
+                        tm_ld4_4r(xa + 8 * g, ta + 8 * g, xr, t1v);
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int s = 4 * h + u;
+                            const int idx = at(j, s);
+                            const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
+                            const Cx<float> x1 = merge_apply(Cx<float>{t1v[u], 0.0f}, xr[u], p.a3, p.b3);
+                            const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
+                            if (last) {
+                                X[idx] = xn;
+                                T2[idx] = t2n;
+                            } else {
+                                xr[u] = xn;
+                                tn[u] = merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                            }
+                            o[j][s] = sgn(Cx<float>{t1v[u], 0.0f});
                         }
-                        o[j][s] = xn;
+                        if (!last) {
+                            tm_st4(xa + 8 * g, xr);
+                            tm_st4(ta + 8 * g, tn);
+                        }
                     }
-                    if (!last) {
-                        tm_st4(xa + 8 * j, o[j]);
-                        tm_st4(ta + 8 * j, xr);
-                    }
-                }
             }
         }
     }
@@ -501,7 +502,7 @@ cudaError_t dm_launch(const DmArgs& a, const void* tw, cudaStream_t st) {
     }
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<(unsigned)a.batch, 4 * L, smem, st>>>(d);
+    k<<<(unsigned)a.batch, DmP<L>::NT, smem, st>>>(d);
     count_launches();
     return cudaGetLastError();
 }
@@ -512,7 +513,7 @@ int dm_occupancy() {
     auto k = k_dm<L, SPACE_THRESHOLD, DATA_SKIP_ZERO>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, 4 * L, smem) != cudaSuccess || n < 1) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, DmP<L>::NT, smem) != cudaSuccess || n < 1) return 1;
     return n;
 }
 

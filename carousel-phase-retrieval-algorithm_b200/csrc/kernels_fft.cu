@@ -23,13 +23,14 @@ namespace {
 // one plane per CTA
 // ---------------------------------------------------------------------------
 template <typename T, int L, bool INV>
-__global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, const Cx<T>* __restrict__ twg,
-                                                     T scale, int s_neg) {
-    using P = Plane<T, L>;
+__global__ void __launch_bounds__(plane_tpl<T, L>() * L) k_plane_fft(Cx<T>* __restrict__ data,
+                                                                     const Cx<T>* __restrict__ twg, T scale,
+                                                                     int s_neg) {
+    using P = Plane<T, L, plane_tpl<T, L>()>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T>* buf = reinterpret_cast<Cx<T>*>(smem_raw);
     Cx<T>* tw = buf + L * P::LS;
-    const int t = threadIdx.x, line = t >> 2, q = t & 3;
+    const int t = threadIdx.x, row = P::row_of(t), col = P::col_of(t), q = P::rank_of(t);
     P::F::fill_twiddles(tw, twg, t, P::NT);
     Cx<T>* g = data + (size_t)blockIdx.x * L * L;
     __syncthreads();
@@ -40,17 +41,17 @@ __global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, c
 #pragma unroll
             for (int s = 0; s < P::TPL; ++s) {
                 const int n = P::split_pos(q, j, s);
-                o[j][s] = csign(g[line * L + n], line + n);
+                o[j][s] = csign(g[row * L + n], row + n);
             }
-        P::template rows_split_to_buf<false>(o, buf, tw, line, q);
+        P::template rows_split_to_buf<false>(o, buf, tw, row, q);
         __syncthreads();
-        P::template col_from_buf<false>(o, buf, tw, line, q);
+        P::template col_from_buf<false>(o, buf, tw, col, q);
 #pragma unroll
         for (int j = 0; j < P::J; ++j)
 #pragma unroll
             for (int s = 0; s < P::TPL; ++s) {
                 const int f = P::split_pos(q, j, s);
-                g[f * L + line] = csign(o[j][s], f + line + s_neg);
+                g[f * L + col] = csign(o[j][s], f + col + s_neg);
             }
     } else {
         Cx<T> o[P::J][P::TPL];
@@ -59,24 +60,24 @@ __global__ void __launch_bounds__(4 * L) k_plane_fft(Cx<T>* __restrict__ data, c
 #pragma unroll
             for (int s = 0; s < P::TPL; ++s) {
                 const int f = P::split_pos(q, j, s);
-                o[j][s] = csign(g[f * L + line], f + line + s_neg);
+                o[j][s] = csign(g[f * L + col], f + col + s_neg);
             }
-        P::template col_to_buf<true>(o, buf, tw, line, q);
+        P::template col_to_buf<true>(o, buf, tw, col, q);
         __syncthreads();
-        P::template row_from_buf<true>(o, buf, tw, line, q);
+        P::template row_from_buf<true>(o, buf, tw, row, q);
 #pragma unroll
         for (int j = 0; j < P::J; ++j)
 #pragma unroll
             for (int s = 0; s < P::TPL; ++s) {
                 const int f = P::split_pos(q, j, s);
-                g[line * L + f] = csign(cscale(o[j][s], scale), line + f);
+                g[row * L + f] = csign(cscale(o[j][s], scale), row + f);
             }
     }
 }
 
 template <typename T, int L>
 cudaError_t plane_fft(void* x, uint64_t batch, bool inverse, T scale, int s_neg, const void* tw, cudaStream_t st) {
-    using P = Plane<T, L>;
+    using P = Plane<T, L, plane_tpl<T, L>()>;
     const size_t smem = P::buf_bytes() + P::tw_bytes();
     auto kf = inverse ? k_plane_fft<T, L, true> : k_plane_fft<T, L, false>;
     cudaError_t e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -78,4 +78,33 @@ __device__ __forceinline__ void tm_ld4(uint32_t a, Cx<float> (&v)[4]) {
     for (int i = 0; i < 4; ++i) v[i] = {__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])};
 }
 
+// Four floats (4 columns) to tensor memory.
+__device__ __forceinline__ void tm_st4r(uint32_t a, const float (&v)[4]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(__float_as_uint(v[0])),
+                 "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3]))
+                 : "memory");
+}
+
+// Four complex floats (8 columns at a) and four floats (4 columns at b) from
+// tensor memory, one wait for both.
+__device__ __forceinline__ void tm_ld4_4r(uint32_t a, uint32_t b, Cx<float> (&u)[4], float (&v)[4]) {
+    uint32_t r[12];
+    asm volatile(
+        "{\n\t"
+        "tcgen05.wait::st.sync.aligned;\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%12];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x4.b32 {%8, %9, %10, %11}, [%13];\n\t"
+        "tcgen05.wait::ld.sync.aligned;\n\t"
+        "}"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11])
+        : "r"(a), "r"(b)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        u[i] = {__uint_as_float(r[2 * i]), __uint_as_float(r[2 * i + 1])};
+        v[i] = __uint_as_float(r[8 + i]);
+    }
+}
+
 }  // namespace cpra_b200
