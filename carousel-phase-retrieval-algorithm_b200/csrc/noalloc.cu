@@ -15,11 +15,15 @@
 // CPRA_B200_NOALLOC_MAX_BATCH * (2 * CONVERGE_BLOCKS + 1) doubles (264 KiB for
 // 256 members): every GPU that loads the library holds it until the process
 // exits.  Its device address is looked up once per device, on the first call
-// made with that device current (so that first call should come before any
-// stream capture).  All calls share the array: the partial sums are written in
-// full by every call before they are read, so nothing has to start at zero, but
-// two calls that overlap on the GPU (on different streams, or from different
-// host threads) race on it.
+// made with that device current.  CUDA loads a library's device code lazily,
+// so that first call is also when the array itself is placed in device
+// memory: make it at start-up, before a memory pool reserves the device and
+// before any stream capture, and later calls allocate nothing.  The address
+// stays valid for the life of the device's primary context; do not use the
+// entry point across cudaDeviceReset.  All calls share the array: the partial
+// sums are written in full by every call before they are read, so nothing has
+// to start at zero, but two calls that overlap on the GPU (on different
+// streams, or from different host threads) race on it.
 #include "cpra_b200.h"
 #include "cpra_internal.h"
 

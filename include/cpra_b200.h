@@ -381,8 +381,11 @@ int cpra_b200_kernel_timing(cpra_b200_ctx* ctx, double* ms, uint64_t* launches, 
  * into the library (a file-scope __device__ array of about 264 KiB that every
  * GPU loading the library holds until exit).  batch_size is limited to
  * CPRA_B200_NOALLOC_MAX_BATCH; larger batches are refused with CPRA_B200_EARG.
- * The scratch address is looked up on the first call made on each device, so
- * make that first call before any stream capture.  All calls share the scratch:
+ * The scratch address is looked up on the first call made on each device, and
+ * since CUDA loads a library's device code lazily, that call also places the
+ * array in device memory: make it at start-up, before a memory pool reserves
+ * the device and before any stream capture; later calls allocate nothing.  Do
+ * not use the entry point across cudaDeviceReset.  All calls share the scratch:
  * calls that overlap on the GPU (other streams, other host threads) race.
  * dtype is CPRA_B200_F32 or CPRA_B200_F64; stream is a cudaStream_t (NULL: the
  * default stream); the call returns after err_host is written. */

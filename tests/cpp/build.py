@@ -35,7 +35,11 @@ def compile_driver(name: str, extra: list[str]) -> Path:
     return exe
 
 
-def build(reference_include: str | None = "/root/reference/include") -> list[Path]:
+def build(reference_include: str | None = None) -> list[Path]:
+    if reference_include is None:
+        sys.path.insert(0, str(Path(__file__).resolve().parents[2] / "oracle"))
+        from reference_dir import reference_dir
+        reference_include = str(reference_dir() / "include")
     built = [compile_driver("drop_in_standalone", ["-DCPRA_B200_STANDALONE"])]
     if reference_include and (Path(reference_include) / "CPRA_Impl.hpp").exists():
         built.append(compile_driver("drop_in_ref_iface", ["-I", reference_include]))
@@ -44,7 +48,7 @@ def build(reference_include: str | None = "/root/reference/include") -> list[Pat
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-include", default="/root/reference/include")
+    ap.add_argument("--reference-include", default=None, help="default: the reference checkout's include/")
     a = ap.parse_args()
     for p in build(a.reference_include):
         print(p)

@@ -9,7 +9,9 @@ import pytest
 
 from conftest import REPO
 
-REF_INCLUDE = Path("/root/reference/include")
+from reference_dir import reference_dir
+
+REF_INCLUDE = reference_dir() / "include"
 TU = r'''
 #include "cpra_b200/B200_Impl.hpp"
 #include <memory>

@@ -48,9 +48,38 @@ def test_noalloc_converge_error_matches_regular_entry(cuda):
     for k, (M, N, L, B, dt) in enumerate([(32, 32, 2, 3, np.float32), (16, 8, 1, 7, np.float32),
                                           (8, 8, 4, 2, np.float64), (64, 64, 1, 256, np.float32)]):
         old_a, err_a, old_b, err_b = _run_both(torch, cb, M, N, L, B, dt, seed=11 + k)
-        np.testing.assert_array_equal(old_b, old_a)            # old <- new - old, element-wise exact
-        np.testing.assert_allclose(err_b, err_a, rtol=1e-6)    # the norm ratio, as the regular entry's tests use
+        np.testing.assert_array_equal(old_b, old_a)   # old <- new - old, element-wise exact
+        # both take IEEE double square roots and a division of the same FP64 sums
+        np.testing.assert_array_equal(err_b, err_a)
         assert np.all(np.isfinite(err_b)) and np.all(err_b > 0)
+
+
+def test_noalloc_converge_error_allocates_nothing(cuda):
+    """After the first call on the device (which loads the library's device
+    code and with it the scratch array), further calls leave the device's free
+    memory unchanged."""
+    import torch
+    import cpra_b200 as cb
+    M, N, L, B = 64, 64, 1, 256
+    g = torch.Generator(device="cuda").manual_seed(5)
+    new = torch.randn(M * N * L * B, dtype=torch.complex64, device="cuda", generator=g)
+    olds = [torch.randn(M * N * L * B, dtype=torch.complex64, device="cuda", generator=g) for _ in range(3)]
+    errs = [np.zeros(B, np.float32) for _ in range(4)]
+
+    def call(old, err):
+        rc = cb.lib().cpra_b200_converge_error_noalloc(F32, old.data_ptr(), new.data_ptr(),
+                                                       err.ctypes.data_as(ctypes.c_void_p), M, N, L, B, None)
+        assert rc == cb.OK, cb.last_error()
+
+    first = olds[0].clone()
+    torch.cuda.synchronize()
+    call(first, errs[3])
+    free_before = torch.cuda.mem_get_info()[0]
+    for old, err in zip(olds, errs):
+        call(old, err)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    np.testing.assert_array_equal(errs[0], errs[3])   # same inputs, same bits
 
 
 def test_noalloc_converge_error_refuses_batches_above_the_limit(cuda):
