@@ -266,6 +266,13 @@ __global__ void __launch_bounds__(DmP<L>::NT, (L == 64) ? 2 : 1) k_dm(const DmDe
     }
 }
 
+// The block index as a fresh read of %ctaid.x (not folded with earlier reads).
+__device__ __forceinline__ unsigned cta_index() {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(v));
+    return v;
+}
+
 // The 128 x 128 kernel with its iterates resident in tensor memory.
 //
 // Every thread reads and writes x, t1 and t2 only at its own row's split
@@ -392,9 +399,7 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
                         for (int u = 0; u < 4; ++u) {
                             const int s = 4 * h + u;
                             const Cx<float> val = sgn(cscale(o[j][s], p.scale));
-                            const Cx<float> m = space(merge_apply(xr[u], val, p.a1, p.b1), at(j, s));
-                            t1v[u] = m.x;
-                            if (last) T1[at(j, s)] = m;
+                            t1v[u] = space(merge_apply(xr[u], val, p.a1, p.b1), at(j, s)).x;
                         }
                         if (it > 0) {
                             // a2*x + b2*S(t2), formed by the previous iteration
@@ -418,8 +423,8 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
                     }
             } else {
                 // x <- a3*t1 + b3*x; x <- a4*t2' + b4*x; t2's columns take the
-                // next iteration's a2*x + b2*S(t2'); o takes its first half's
-                // input t1
+                // next iteration's a2*x + b2*S(t2') (after the last iteration
+                // t2' itself); o takes the next first half's input t1
 #pragma unroll
                 for (int j = 0; j < J; ++j)
 #pragma unroll
@@ -435,22 +440,41 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
                             const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
                             const Cx<float> x1 = merge_apply(Cx<float>{t1v[u], 0.0f}, xr[u], p.a3, p.b3);
                             const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
-                            if (last) {
-                                X[idx] = xn;
-                                T2[idx] = t2n;
-                            } else {
-                                xr[u] = xn;
-                                tn[u] = merge_apply(xn, space(t2n, idx), p.a2, p.b2);
-                            }
+                            xr[u] = xn;
+                            tn[u] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
                             o[j][s] = sgn(Cx<float>{t1v[u], 0.0f});
                         }
-                        if (!last) {
-                            tm_st4(xa + 8 * g, xr);
-                            tm_st4(ta + 8 * g, tn);
-                        }
+                        tm_st4(xa + 8 * g, xr);
+                        tm_st4(ta + 8 * g, tn);
                     }
             }
         }
+    }
+    // write-out: x and t2 from tensor memory, t1 (= SpaceConstraint's
+    // {value, 0}) from the first half's input in o
+    if (p.iters > 0) {
+        // the plane's addresses again from the block index (read anew, so that
+        // no pointer stays in a register through the iterations)
+        const size_t b2 = (size_t)cta_index() * L * L;
+        Cx<float>* __restrict__ Xo = p.x + b2;
+        Cx<float>* __restrict__ T1o = p.t1 + b2;
+        Cx<float>* __restrict__ T2o = p.t2 + b2;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int g = 2 * j + h;
+                Cx<float> xr[4], tv[4];
+                tm_ld4(xa + 8 * g, xr);
+                tm_ld4(ta + 8 * g, tv);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int idx = at(j, 4 * h + u);
+                    Xo[idx] = xr[u];
+                    T2o[idx] = tv[u];
+                    T1o[idx] = sgn(o[j][4 * h + u]);
+                }
+            }
     }
     tm_wait_st();
     tm_fence_before_sync();
