@@ -305,7 +305,6 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
     Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
     float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
     Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + D::a_bytes());
-    uint32_t* mask = reinterpret_cast<uint32_t*>(smem_raw + P::buf_bytes() + D::a_bytes() + P::tw_bytes());
     const int t = threadIdx.x, row = P::row_of(t), col = P::col_of(t), q = P::rank_of(t), warp = t >> 5;
     if (warp == 0) tm_alloc(&tm_base, 512);
     P::F::fill_twiddles(tw, p.tw, t, P::NT);
@@ -319,14 +318,23 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
     const float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
     for (int i = t; i < L * L; i += P::NT) As[(i / L) * D::AP + (i % L)] = A[i];
     constexpr bool use_mask = (SMODE == SPACE_THRESHOLD);
-    if constexpr (use_mask) D::fill_mask(mask, S, t);
-    auto space = [&](Cx<float> z, int idx) -> Cx<float> {
-        if constexpr (use_mask)
-            return {D::mask_keep(mask, idx) ? z.x : 0.0f, 0.0f};
-        else
-            return space_apply(z, S[idx], SMODE);
-    };
     auto at = [&](int j, int s) { return row * L + P::split_pos(q, j, s); };
+    // the threshold SpaceConstraint of this thread's 16 pixels, evaluated once
+    // per launch: bit 8j + s set where the value is kept
+    uint32_t keep_bits = 0;
+    if constexpr (use_mask) {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) keep_bits |= (space_zero(S[at(j, s)]) ? 0u : 1u) << (TPL * j + s);
+    }
+    // SpaceConstraint of element (j, s) of this thread
+    auto space = [&](Cx<float> z, int j, int s) -> Cx<float> {
+        if constexpr (use_mask)
+            return {((keep_bits >> (TPL * j + s)) & 1u) ? z.x : 0.0f, 0.0f};
+        else
+            return space_apply(z, S[at(j, s)], SMODE);
+    };
     const bool neg = ((row + q) & 1) != 0;
     auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
     tm_fence_before_sync();
@@ -375,7 +383,9 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
         }
     for (int it = 0; it < p.iters; ++it) {
         const bool last = (it == p.iters - 1);
-#pragma unroll 1
+        // the two halves unrolled: each transform pass is half of k_dm's code
+        // (16 values per thread), so both copies fit the instruction cache
+#pragma unroll
         for (int ph = 0; ph < 2; ++ph) {
             // first half:  t1' = Backward2D(DataConstraint(Forward2D(t1)))
             // second half: t2' = Backward2D(DataConstraint(Forward2D(a2*x + b2*S(t2))))
@@ -399,7 +409,7 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
                         for (int u = 0; u < 4; ++u) {
                             const int s = 4 * h + u;
                             const Cx<float> val = sgn(cscale(o[j][s], p.scale));
-                            t1v[u] = space(merge_apply(xr[u], val, p.a1, p.b1), at(j, s)).x;
+                            t1v[u] = space(merge_apply(xr[u], val, p.a1, p.b1), j, s).x;
                         }
                         if (it > 0) {
                             // a2*x + b2*S(t2), formed by the previous iteration
@@ -417,7 +427,7 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
 #pragma unroll
                             for (int u = 0; u < 4; ++u)
                                 o[j][4 * h + u] =
-                                    sgn(merge_apply(xr[u], space(tv[u], at(j, 4 * h + u)), p.a2, p.b2));
+                                    sgn(merge_apply(xr[u], space(tv[u], j, 4 * h + u), p.a2, p.b2));
                         }
                         tm_st4r(ta + 8 * g, t1v);
                     }
@@ -436,12 +446,11 @@ __global__ void __launch_bounds__(1024, 1) k_dm_tm(const DmDev p) {
 #pragma unroll
                         for (int u = 0; u < 4; ++u) {
                             const int s = 4 * h + u;
-                            const int idx = at(j, s);
                             const Cx<float> t2n = sgn(cscale(o[j][s], p.scale));
                             const Cx<float> x1 = merge_apply(Cx<float>{t1v[u], 0.0f}, xr[u], p.a3, p.b3);
                             const Cx<float> xn = merge_apply(t2n, x1, p.a4, p.b4);
                             xr[u] = xn;
-                            tn[u] = last ? t2n : merge_apply(xn, space(t2n, idx), p.a2, p.b2);
+                            tn[u] = last ? t2n : merge_apply(xn, space(t2n, j, s), p.a2, p.b2);
                             o[j][s] = sgn(Cx<float>{t1v[u], 0.0f});
                         }
                         tm_st4(xa + 8 * g, xr);
