@@ -114,6 +114,11 @@ _SIGS = {
     "cpra_b200_slice": [C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 + [C.c_void_p],
     "cpra_b200_slice_loss_grad": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                  + [C.c_void_p, C.c_void_p, C.c_void_p],
+    "cpra_b200_slice_orient": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4 + [C.c_void_p],
+    "cpra_b200_slice_loss_grad_orient": [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] * 4 + [C.c_void_p] * 4,
+    "cpra_b200_volume_loss_grad": [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] * 4 + [C.c_void_p] * 4,
+    "cpra_b200_refine_orient": [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+                               + [C.c_uint64] * 4 + [C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p],
     "cpra_b200_rfactor": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p],
     "cpra_b200_converge_error_noalloc": [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_uint64] * 4
                                         + [C.c_void_p],
@@ -418,6 +423,52 @@ class B200Impl:
                                                int(l), _addr(grad_V), loss.ctypes.data_as(C.c_void_p),
                                                ga.ctypes.data_as(C.c_void_p)), "slice_loss_grad")
         return float(loss[0]), ga
+
+    def slice_orient(self, V, angles, rot, m, n, p, l, out) -> bool:
+        """Central slices at tilts `angles` and in-plane rotations `rot`
+        (None: none) (project-defined)."""
+        return _check(lib().cpra_b200_slice_orient(self._h, _addr(V), _addr(angles), _addr(rot), int(m), int(n),
+                                                   int(p), int(l), _addr(out)), "slice_orient")
+
+    def slice_loss_grad_orient(self, V, angles, rot, A, m, n, p, l, grad_V):
+        """(loss, dL/dangles, dL/drot) for the two-parameter orientations;
+        grad_V is written."""
+        import numpy as np
+        loss = np.zeros(1, np.float64)
+        ga = np.zeros(int(p), np.float64)
+        gr = np.zeros(int(p), np.float64)
+        _check(lib().cpra_b200_slice_loss_grad_orient(self._h, _addr(V), _addr(angles), _addr(rot), _addr(A), int(m),
+                                                      int(n), int(p), int(l), _addr(grad_V),
+                                                      loss.ctypes.data_as(C.c_void_p), ga.ctypes.data_as(C.c_void_p),
+                                                      gr.ctypes.data_as(C.c_void_p)), "slice_loss_grad_orient")
+        return float(loss[0]), ga, gr
+
+    def volume_loss_grad(self, vol, angles, rot, A, m, n, p, l, grad_vol):
+        """(loss, dL/dangles, dL/drot) of a real-space volume through
+        Forward3D, the slice operator and the modulus loss; grad_vol (real,
+        device) is written."""
+        import numpy as np
+        loss = np.zeros(1, np.float64)
+        ga = np.zeros(int(p), np.float64)
+        gr = np.zeros(int(p), np.float64)
+        _check(lib().cpra_b200_volume_loss_grad(self._h, _addr(vol), _addr(angles), _addr(rot), _addr(A), int(m),
+                                                int(n), int(p), int(l), _addr(grad_vol),
+                                                loss.ctypes.data_as(C.c_void_p), ga.ctypes.data_as(C.c_void_p),
+                                                gr.ctypes.data_as(C.c_void_p)), "volume_loss_grad")
+        return float(loss[0]), ga, gr
+
+    def refine_orient(self, V, angles, rot, A, m, n, p, l, steps, real_space=False, lr_volume=1e-3, lr_angle=1e-3,
+                      lr_rot=1e-3):
+        """Adam steps on the volume (real-space with real_space), the tilts and
+        the in-plane rotations (rot None: not refined); returns the loss before
+        each step."""
+        import numpy as np
+        loss = np.zeros(max(int(steps), 1), np.float64)
+        _check(lib().cpra_b200_refine_orient(self._h, _addr(V), 1 if real_space else 0, _addr(angles), _addr(rot),
+                                             _addr(A), int(m), int(n), int(p), int(l), int(steps), float(lr_volume),
+                                             float(lr_angle), float(lr_rot), loss.ctypes.data_as(C.c_void_p)),
+               "refine_orient")
+        return loss[:int(steps)]
 
     def constraint3d(self, x, C, S, iters=1) -> bool:
         """iters x (Forward3D, complex DataConstraint with C, Backward3D,

@@ -237,6 +237,9 @@ struct cpra_b200_ctx {
     // slices sorted by direction for the gathers over slices (angle_table.cuh)
     void* atab = nullptr;
     uint64_t atab_bytes = 0;
+    // the slice operator's per-slice orientation table (sines and cosines)
+    void* otab = nullptr;
+    uint64_t otab_bytes = 0;
     bool graphs = false;
     bool capturing = false;
     uint64_t epoch = 0;  // bumped whenever a context buffer is freed or reallocated
@@ -695,6 +698,7 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     if (c->refine_buf) cudaFree(c->refine_buf);
     if (c->best_sums) cudaFree(c->best_sums);
     if (c->atab) cudaFree(c->atab);
+    if (c->otab) cudaFree(c->otab);
     for (RunLane& lane : c->run_lanes) {
         if (lane.stream) cudaStreamSynchronize(lane.stream);
         if (lane.drv) cudaFree(lane.drv);
@@ -1365,87 +1369,204 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
     return run_maybe_graph(c, key, enqueue);
 }
 
-int cpra_b200_slice(cpra_b200_ctx* c, const void* V, const void* angles, uint64_t m, uint64_t n, uint64_t p,
-                    uint64_t l, void* slices) {
+namespace {
+
+// the orientation table of p slices in the context's buffer
+int orient_table(cpra_b200_ctx* c, const void* angles, const void* rot, uint64_t p) {
+    int r = ensure_buffer(c, &c->otab, &c->otab_bytes, orient_table_bytes(c->dbl, p), "cudaMalloc(orientation table)");
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_orient_table(c->dbl, angles, rot, c->otab, p, c->stream), "orientation table");
+    return CPRA_B200_OK;
+}
+
+// buffers of the loss and its gradients: G (work), the reductions (three
+// sums per slice), the direction table; returns it (null above its limit)
+int loss_buffers(cpra_b200_ctx* c, uint64_t m, uint64_t n, uint64_t p, void** atab) {
+    int r = ensure_work(c, p * n * m * c->csize());
+    if (r) return r;
+    r = ensure_reduction(c, 2 * p);  // 2 * CONVERGE_BLOCKS * 2p >= 3 partials per block and slice
+    if (r) return r;
+    *atab = nullptr;
+    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
+        r = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
+        if (r) return r;
+        *atab = c->atab;
+    }
+    return CPRA_B200_OK;
+}
+
+// the per-slice sums of the last loss evaluation to the host
+int loss_to_host(cpra_b200_ctx* c, uint64_t p, double* loss_host, double* ga_host, double* gr_host) {
+    CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 3 * p, cudaMemcpyDeviceToHost, c->stream),
+                    "slice_loss_grad");
+    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "slice_loss_grad");
+    double loss = 0.0;
+    for (uint64_t i = 0; i < p; ++i) {
+        loss += c->host_sums[3 * i];
+        if (ga_host) ga_host[i] = c->host_sums[3 * i + 1];
+        if (gr_host) gr_host[i] = c->host_sums[3 * i + 2];
+    }
+    if (loss_host) *loss_host = loss;
+    return CPRA_B200_OK;
+}
+
+bool volume_fft_ok(cpra_b200_ctx* c, uint64_t m, uint64_t n, uint64_t l) {
+    auto p2 = [](uint64_t v) { return v >= 2 && (v & (v - 1)) == 0 && v <= 1024; };
+    return c->m == m && c->n == n && c->l == l && p2(m) && p2(n) && p2(l);
+}
+
+// Forward3D of one real volume into the complex buffer VF
+int volume_forward(cpra_b200_ctx* c, const void* vol, void* VF, uint64_t vox) {
+    CPRA_CHECK_CUDA(launch_real_complex(c->dbl, true, const_cast<void*>(vol), VF, 1.0, vox, c->stream), "volume");
+    CPRA_CHECK_CUDA(launch_fft3d(c->dbl, VF, c->m, c->n, c->l, 1, false, 1.0, twiddles(c, c->m), twiddles(c, c->n),
+                                 twiddles(c, c->l), c->work, c->stream),
+                    "volume Forward3D");
+    return CPRA_B200_OK;
+}
+
+// grad_vol = Re(Forward3D^H gV): the adjoint of the shifted unnormalised
+// transform is the inverse transform without its 1/(m n l)
+int volume_adjoint(cpra_b200_ctx* c, void* gV, void* grad_vol, uint64_t vox) {
+    CPRA_CHECK_CUDA(launch_fft3d(c->dbl, gV, c->m, c->n, c->l, 1, true, 1.0, twiddles(c, c->m), twiddles(c, c->n),
+                                 twiddles(c, c->l), c->work, c->stream),
+                    "volume adjoint");
+    CPRA_CHECK_CUDA(launch_real_complex(c->dbl, false, grad_vol, gV, 1.0, vox, c->stream), "volume adjoint");
+    return CPRA_B200_OK;
+}
+
+}  // namespace
+
+int cpra_b200_slice_orient(cpra_b200_ctx* c, const void* V, const void* angles, const void* rot, uint64_t m, uint64_t n,
+                           uint64_t p, uint64_t l, void* slices) {
     CTX_OR_RETURN(c);
     if (!V || !angles || !slices) return fail(CPRA_B200_EARG, "slice: null pointer");
     if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "slice: zero size");
     int r = flush(c);
     if (r) return take_deferred(c);
-    CPRA_CHECK_CUDA(launch_slice(c->dbl, V, angles, slices, m, n, p, l, c->stream), "slice");
+    r = orient_table(c, angles, rot, p);
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_slice(c->dbl, V, c->otab, slices, m, n, p, l, c->stream), "slice");
     return CPRA_B200_OK;
 }
 
-int cpra_b200_slice_loss_grad(cpra_b200_ctx* c, const void* V, const void* angles, const void* A, uint64_t m,
-                              uint64_t n, uint64_t p, uint64_t l, void* grad_V, double* loss_host,
-                              double* grad_angles_host) {
+int cpra_b200_slice(cpra_b200_ctx* c, const void* V, const void* angles, uint64_t m, uint64_t n, uint64_t p,
+                    uint64_t l, void* slices) {
+    return cpra_b200_slice_orient(c, V, angles, nullptr, m, n, p, l, slices);
+}
+
+int cpra_b200_slice_loss_grad_orient(cpra_b200_ctx* c, const void* V, const void* angles, const void* rot,
+                                     const void* A, uint64_t m, uint64_t n, uint64_t p, uint64_t l, void* grad_V,
+                                     double* loss_host, double* grad_angles_host, double* grad_rot_host) {
     CTX_OR_RETURN(c);
     if (!V || !angles || !A || !grad_V) return fail(CPRA_B200_EARG, "slice_loss_grad: null pointer");
     if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "slice_loss_grad: zero size");
     if (p > 65535) return fail(CPRA_B200_EUNSUP, "slice_loss_grad: more than 65535 slices");
     int r = flush(c);
     if (r) return take_deferred(c);
-    r = ensure_work(c, p * n * m * c->csize());  // G = dL/ds
-    if (r) return r;
-    r = ensure_reduction(c, p);
-    if (r) return r;
     void* atab = nullptr;
-    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
-        r = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
-        if (r) return r;
-        atab = c->atab;
-    }
-    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, grad_V, m, n, p, l, c->partials, c->sums, atab,
-                                           c->stream),
+    r = loss_buffers(c, m, n, p, &atab);
+    if (r) return r;
+    r = orient_table(c, angles, rot, p);
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, c->otab, A, c->work, grad_V, m, n, p, l, c->partials,
+                                           c->sums, atab, c->stream),
                     "slice_loss_grad");
-    CPRA_CHECK_CUDA(cudaMemcpyAsync(c->host_sums, c->sums, sizeof(double) * 2 * p, cudaMemcpyDeviceToHost, c->stream),
-                    "slice_loss_grad");
-    CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "slice_loss_grad");
-    double loss = 0.0;
-    for (uint64_t i = 0; i < p; ++i) {
-        loss += c->host_sums[2 * i];
-        if (grad_angles_host) grad_angles_host[i] = c->host_sums[2 * i + 1];
-    }
-    if (loss_host) *loss_host = loss;
-    return CPRA_B200_OK;
+    return loss_to_host(c, p, loss_host, grad_angles_host, grad_rot_host);
 }
 
-int cpra_b200_refine(cpra_b200_ctx* c, void* V, void* angles, const void* A, uint64_t m, uint64_t n, uint64_t p,
-                     uint64_t l, int steps, double lr_volume, double lr_angle, double* loss_host) {
+int cpra_b200_slice_loss_grad(cpra_b200_ctx* c, const void* V, const void* angles, const void* A, uint64_t m,
+                              uint64_t n, uint64_t p, uint64_t l, void* grad_V, double* loss_host,
+                              double* grad_angles_host) {
+    return cpra_b200_slice_loss_grad_orient(c, V, angles, nullptr, A, m, n, p, l, grad_V, loss_host, grad_angles_host,
+                                            nullptr);
+}
+
+int cpra_b200_volume_loss_grad(cpra_b200_ctx* c, const void* vol, const void* angles, const void* rot, const void* A,
+                               uint64_t m, uint64_t n, uint64_t p, uint64_t l, void* grad_vol, double* loss_host,
+                               double* grad_angles_host, double* grad_rot_host) {
+    CTX_OR_RETURN(c);
+    if (!vol || !angles || !A || !grad_vol) return fail(CPRA_B200_EARG, "volume_loss_grad: null pointer");
+    if (m == 0 || n == 0 || p == 0 || l == 0) return fail(CPRA_B200_EARG, "volume_loss_grad: zero size");
+    if (p > 65535) return fail(CPRA_B200_EUNSUP, "volume_loss_grad: more than 65535 slices");
+    if (!volume_fft_ok(c, m, n, l))
+        return fail(CPRA_B200_EUNSUP, "volume_loss_grad: the context's (m, n, l) must be the volume's, powers of two "
+                                      "2..1024");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t vox = l * n * m;
+    r = ensure_buffer(c, &c->refine_buf, &c->refine_bytes, 2 * vox * c->csize(), "cudaMalloc(volume buffers)");
+    if (r) return r;
+    void* atab = nullptr;
+    r = loss_buffers(c, m, n, p, &atab);
+    if (r) return r;
+    r = orient_table(c, angles, rot, p);
+    if (r) return r;
+    char* buf = static_cast<char*>(c->refine_buf);
+    void* VF = buf;
+    void* gV = buf + vox * c->csize();
+    r = volume_forward(c, vol, VF, vox);
+    if (r) return r;
+    CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, VF, angles, c->otab, A, c->work, gV, m, n, p, l, c->partials,
+                                           c->sums, atab, c->stream),
+                    "volume_loss_grad");
+    r = volume_adjoint(c, gV, grad_vol, vox);
+    if (r) return r;
+    return loss_to_host(c, p, loss_host, grad_angles_host, grad_rot_host);
+}
+
+int cpra_b200_refine_orient(cpra_b200_ctx* c, void* V, int real_space, void* angles, void* rot, const void* A,
+                            uint64_t m, uint64_t n, uint64_t p, uint64_t l, int steps, double lr_volume,
+                            double lr_angle, double lr_rot, double* loss_host) {
     CTX_OR_RETURN(c);
     if (!V || !angles || !A) return fail(CPRA_B200_EARG, "refine: null pointer");
     if (m == 0 || n == 0 || p == 0 || l == 0 || steps < 0) return fail(CPRA_B200_EARG, "refine: zero size or steps < 0");
     if (p > 65535) return fail(CPRA_B200_EUNSUP, "refine: more than 65535 slices");
+    if (real_space && !volume_fft_ok(c, m, n, l))
+        return fail(CPRA_B200_EUNSUP, "refine: a real-space volume needs the context's (m, n, l) to be the volume's, "
+                                      "powers of two 2..1024");
     int r = flush(c);
     if (r) return take_deferred(c);
     if (steps == 0) return CPRA_B200_OK;
     const uint64_t vox = l * n * m;
-    const uint64_t gbytes = vox * c->csize(), mbytes = (4 * vox + 2 * p) * c->esize();
-    const uint64_t mofs = (gbytes + 255) / 256 * 256, lofs = mofs + (mbytes + 255) / 256 * 256;
+    const uint64_t nv = real_space ? vox : 2 * vox;  // reals refined
+    // gV (complex), VF (complex, real-space only), the real gradient
+    // (real-space only), the Adam moments, the per-step losses
+    const uint64_t cb = (vox * c->csize() + 255) / 256 * 256;
+    const uint64_t rb = real_space ? (vox * c->esize() + 255) / 256 * 256 : 0;
+    const uint64_t mbytes = (2 * nv + 4 * p) * c->esize();
+    const uint64_t gofs = 0, fofs = cb, rofs = fofs + (real_space ? cb : 0), mofs = rofs + rb;
+    const uint64_t lofs = mofs + (mbytes + 255) / 256 * 256;
     r = ensure_buffer(c, &c->refine_buf, &c->refine_bytes, lofs + sizeof(double) * (uint64_t)steps,
                       "cudaMalloc(refine buffers)");
     if (r) return r;
-    r = ensure_work(c, p * n * m * c->csize());  // G = dL/ds
-    if (r) return r;
-    r = ensure_reduction(c, p);
-    if (r) return r;
     void* atab = nullptr;
-    if (p <= (uint64_t)ANGLE_TABLE_MAX) {
-        r = ensure_buffer(c, &c->atab, &c->atab_bytes, angle_table_bytes(p), "cudaMalloc(angle table)");
-        if (r) return r;
-        atab = c->atab;
-    }
+    r = loss_buffers(c, m, n, p, &atab);
+    if (r) return r;
     char* buf = static_cast<char*>(c->refine_buf);
-    void* gV = buf;
+    void* gV = buf + gofs;
+    void* VF = real_space ? buf + fofs : V;
+    void* greal = real_space ? buf + rofs : nullptr;
     void* mom = buf + mofs;
     double* loss_dev = reinterpret_cast<double*>(buf + lofs);
     CPRA_CHECK_CUDA(cudaMemsetAsync(mom, 0, mbytes, c->stream), "refine");
     for (int k = 1; k <= steps; ++k) {
-        CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, V, angles, A, c->work, gV, m, n, p, l, c->partials, c->sums, atab,
-                                               c->stream),
+        // the iterates are recomputed each step: orientation table, Fourier
+        // volume, slices and residuals
+        r = orient_table(c, angles, rot, p);
+        if (r) return r;
+        if (real_space) {
+            r = volume_forward(c, V, VF, vox);
+            if (r) return r;
+        }
+        CPRA_CHECK_CUDA(launch_slice_loss_grad(c->dbl, VF, angles, c->otab, A, c->work, gV, m, n, p, l, c->partials,
+                                               c->sums, atab, c->stream),
                         "refine");
-        CPRA_CHECK_CUDA(launch_refine_step(c->dbl, V, angles, gV, mom, vox, p, c->sums, lr_volume, lr_angle, k,
-                                           loss_dev + (k - 1), c->stream),
+        if (real_space) {
+            r = volume_adjoint(c, gV, greal, vox);
+            if (r) return r;
+        }
+        CPRA_CHECK_CUDA(launch_refine_step(c->dbl, V, nv, angles, rot, real_space ? greal : gV, mom, p, c->sums,
+                                           lr_volume, lr_angle, lr_rot, k, loss_dev + (k - 1), c->stream),
                         "refine");
     }
     if (loss_host) {
@@ -1454,6 +1575,12 @@ int cpra_b200_refine(cpra_b200_ctx* c, void* V, void* angles, const void* A, uin
         CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "refine");
     }
     return CPRA_B200_OK;
+}
+
+int cpra_b200_refine(cpra_b200_ctx* c, void* V, void* angles, const void* A, uint64_t m, uint64_t n, uint64_t p,
+                     uint64_t l, int steps, double lr_volume, double lr_angle, double* loss_host) {
+    return cpra_b200_refine_orient(c, V, 0, angles, nullptr, A, m, n, p, l, steps, lr_volume, lr_angle, 0.0,
+                                   loss_host);
 }
 
 int cpra_b200_best_start(cpra_b200_ctx* c, const void* x, const void* A, uint64_t P, uint64_t batch,

@@ -144,20 +144,29 @@ int dm_large_ctas_per_sm(uint64_t M);
 uint64_t dm_large_row_ctas(uint64_t M, uint64_t batch);
 
 // ---- central slices and the amplitude-loss adjoints (kernels_adj.cu) --------
-// slices out[p] ([P][N][M]) of the [L][N][M] volume V at angles ang[p]
-cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, uint64_t m, uint64_t n, uint64_t p,
+// Orientation table of P slices: sines and cosines of the tilts ang[p] and of
+// the in-plane rotations rot[p] (rot may be null: none), orient_table_bytes.
+uint64_t orient_table_bytes(bool dbl, uint64_t p);
+cudaError_t launch_orient_table(bool dbl, const void* ang, const void* rot, void* tab, uint64_t p, cudaStream_t st);
+// slices out[p] ([P][N][M]) of the [L][N][M] volume V at the table's orientations
+cudaError_t launch_slice(bool dbl, const void* V, const void* tab, void* out, uint64_t m, uint64_t n, uint64_t p,
                          uint64_t l, cudaStream_t st);
-// G = dL/ds (scratch, [P][N][M]), gV = dL/dV, sums[2p] = loss of slice p,
-// sums[2p+1] = dL/d ang[p] (partials: >= P * CONVERGE_BLOCKS * 2 doubles)
-cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
-                                   uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
-                                   void* atab, cudaStream_t st);
-// one Adam step (step >= 1) on the volume (vox complex) and the P angles from
-// gV and the per-slice sums; moments: 4*vox + 2*P elements of the element
-// type, zero before step 1; loss <- sum_p sums[2p]
-cudaError_t launch_refine_step(bool dbl, void* V, void* ang, const void* gV, void* moments, uint64_t vox, uint64_t P,
-                               const double* sums, double lr_volume, double lr_angle, int step, double* loss,
-                               cudaStream_t st);
+// G = dL/ds (scratch, [P][N][M]), gV = dL/dV, sums[3p] = loss of slice p,
+// sums[3p+1] = dL/d ang[p], sums[3p+2] = dL/d rot[p] (partials: >= P *
+// CONVERGE_BLOCKS * 3 doubles); ang orders the slices for the gather (atab)
+cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* tab, const void* A, void* G,
+                                   void* gV, uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials,
+                                   double* sums, void* atab, cudaStream_t st);
+// one Adam step (step >= 1) on the nv reals of V, the P tilts and (rot not
+// null) the P rotations from gV and the per-slice sums; moments: 2 nv + 4 P
+// elements, zero before step 1; loss <- sum_p sums[3p]
+cudaError_t launch_refine_step(bool dbl, void* V, uint64_t nv, void* ang, void* rot, const void* gV, void* moments,
+                               uint64_t P, const double* sums, double lr_volume, double lr_angle, double lr_rot,
+                               int step, double* loss, cudaStream_t st);
+// real volume <-> complex volume: to_complex: cplx = real + 0i; else real =
+// Re(cplx) * scale (n values)
+cudaError_t launch_real_complex(bool dbl, bool to_complex, void* real, void* cplx, double scale, uint64_t n,
+                                cudaStream_t st);
 
 // ---- fused HIO + shrinkwrap iterations (kernels_hio.cu) -----------------------
 struct HioArgs {

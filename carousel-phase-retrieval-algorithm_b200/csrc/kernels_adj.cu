@@ -1,25 +1,36 @@
 // Central slices of a 3D Fourier volume and the adjoints of the amplitude loss
 // (project-defined; the reference has no slice operator, loss or gradient).
 //
-// Geometry: the merges' (CUDA_Impl_Kernel.cuh:80-90).  A volume is [L][N][M]
-// (y fastest); voxel (z, x, y) sits at the point (j, k, l) = (L/2 - z,
-// x - N/2, M/2 - y).  Slice pixel (xIn, yIn) of angle a, slices stored
-// [P][N][M] (yIn fastest), is the point (yr sin a, xr, yr cos a) with
-// xr = xIn - N/2, yr = M/2 - yIn, i.e. the voxel coordinates
-//   z = L/2 - yr sin a,  x = xIn,  y = M/2 - yr cos a.
-// The x coordinate is integral, so trilinear interpolation reduces to
-// bilinear interpolation in (z, y) on the plane x = xIn:
-//   s[p](xIn, yIn) = sum_{z,y} w(z) w(y) V[z][xIn][y],  w(u) = max(0, 1 - |u - u*|)
-// (points outside the volume contribute 0).
+// Geometry: the merges' (CUDA_Impl_Kernel.cuh:80-90) with an in-plane rotation
+// added.  A volume is [L][N][M] (y fastest); voxel (z, x, y) sits at the point
+// (j, k, l) = (L/2 - z, x - N/2, M/2 - y).  Slice p has the tilt a_p (the
+// merges' rotating angle) and the in-plane rotation r_p; its pixel
+// (xIn, yIn), slices stored [P][N][M] (yIn fastest), has the detector
+// coordinates xr = xIn - N/2, yr = M/2 - yIn, rotated in the detector plane to
+//   xq = xr cos r - yr sin r,  yq = xr sin r + yr cos r,
+// and sits at the point (yq sin a, xq, yq cos a), i.e. the voxel coordinates
+//   zf = L/2 - yq sin a,  xf = N/2 + xq,  yf = M/2 - yq cos a.
+// A slice pixel is the trilinear sample of V there,
+//   s[p](xIn, yIn) = sum_{z,x,y} w(zf - z) w(xf - x) w(yf - y) V[z][x][y],
+//   w(u) = max(0, 1 - |u|)   (voxels outside the volume read 0).
+// With r = 0, xf = xIn is integral and the sample is the merges' bilinear
+// sample on the plane x = xIn.  The plane of slice p has the normal
+// (cos a, 0, -sin a) whatever r is: r turns the pixel grid inside the plane.
 //
 // Loss L = sum_p sum_px (|s| - A)^2 with G = 2 (|s| - A) s / |s| (0 where s = 0),
 // the derivative with respect to Re s + i Im s:
 //   dL/dV (Re + i Im)  = S^T G: each voxel gathers w * G from the pixels whose
-//                        bilinear footprint covers it (at most 3 rows per slice,
-//                        found from the voxel), so the sum is deterministic;
-//   dL/da_p            = sum_px Re(conj(G) ds/da), ds/da from the derivative of
-//                        the weights (dz/da = -yr cos a, dy/da = yr sin a).
-// Coordinates and weights are computed in double; data stay in T.
+//                        trilinear footprint covers it (found from the voxel's
+//                        coordinates in each nearby slice's plane), so the sum
+//                        is deterministic;
+//   dL/da_p, dL/dr_p   = sum_px Re(conj(G) ds/da), Re(conj(G) ds/dr), from the
+//                        derivatives of the weights:
+//                        d(zf, xf, yf)/da = (-yq cos a, 0, yq sin a),
+//                        d(zf, xf, yf)/dr = (-xq sin a, -yq, -xq cos a).
+// Coordinates and weights are computed in the element type T (float for the
+// float path); the sums over pixels are in double.  Forward and adjoint
+// evaluate the same weight expression for each (pixel, voxel) pair, so the
+// gather is the transpose of the sample up to the summation order.
 #include "cpra_internal.h"
 #include "ops_ew.cuh"
 #include "angle_table.cuh"
@@ -32,70 +43,119 @@ constexpr int ADJ_THREADS = 256;
 __device__ __forceinline__ uint64_t tid_g() { return blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t str_g() { return (uint64_t)gridDim.x * blockDim.x; }
 
-// slice value at pixel (p, xIn, yIn) and, optionally, its derivative in the angle
+// sin and cos of a slice's tilt and in-plane rotation, in T
 template <typename T>
-__device__ __forceinline__ void sample(const Cx<T>* __restrict__ V, int64_t M, int64_t N, int64_t L, double sa,
-                                       double ca, int64_t xIn, int64_t yIn, double& re, double& im, double* dre,
-                                       double* dim) {
-    const double yr = (double)(M / 2 - yIn);
-    const double zf = (double)(L / 2) - yr * sa;
-    const double yf = (double)(M / 2) - yr * ca;
-    const double dz = -yr * ca, dy = yr * sa;  // dzf/da, dyf/da
-    const int64_t z0 = (int64_t)floor(zf), y0 = (int64_t)floor(yf);
-    const double fz = zf - (double)z0, fy = yf - (double)y0;
-    re = im = 0.0;
-    if (dre) *dre = *dim = 0.0;
-    for (int a = 0; a < 2; ++a) {
-        const int64_t z = z0 + a;
-        if (z < 0 || z >= L) continue;
-        const double wz = a ? fz : 1.0 - fz;
-        const double dwz = a ? dz : -dz;  // d wz / d angle
-        for (int b = 0; b < 2; ++b) {
-            const int64_t y = y0 + b;
-            if (y < 0 || y >= M) continue;
-            const double wy = b ? fy : 1.0 - fy;
-            const double dwy = b ? dy : -dy;
-            const Cx<T> v = V[(z * N + xIn) * M + y];
-            const double w = wz * wy;
-            re += w * (double)v.x;
-            im += w * (double)v.y;
-            if (dre) {
-                const double dw = dwz * wy + wz * dwy;
-                *dre += dw * (double)v.x;
-                *dim += dw * (double)v.y;
+struct Orient {
+    T sa, ca, sr, cr;
+};
+
+// one entry per slice (the sines and cosines evaluated once per call, in
+// double, then rounded to T); rot may be null (no in-plane rotation)
+template <typename T>
+__global__ void k_orient_table(const T* __restrict__ ang, const T* __restrict__ rot, Orient<T>* __restrict__ tab,
+                               int64_t P) {
+    for (uint64_t i = tid_g(); i < (uint64_t)P; i += str_g()) {
+        const double a = (double)ang[i], r = rot ? (double)rot[i] : 0.0;
+        tab[i] = Orient<T>{(T)sin(a), (T)cos(a), (T)sin(r), (T)cos(r)};
+    }
+}
+
+// voxel coordinates of pixel (xr, yr) (detector coordinates) of a slice, and
+// the rotated detector coordinates (xq, yq) the derivatives need
+template <typename T>
+__device__ __forceinline__ void pixel_point(const Orient<T>& o, T xr, T yr, T hl, T hn, T hm, T& zf, T& xf, T& yf,
+                                            T& xq, T& yq) {
+    xq = o.cr * xr - o.sr * yr;
+    yq = o.sr * xr + o.cr * yr;
+    zf = hl - yq * o.sa;
+    xf = hn + xq;
+    yf = hm - yq * o.ca;
+}
+
+__device__ __forceinline__ int64_t floor_i(float v) { return (int64_t)floorf(v); }
+__device__ __forceinline__ int64_t floor_i(double v) { return (int64_t)floor(v); }
+__device__ __forceinline__ float absT(float v) { return fabsf(v); }
+__device__ __forceinline__ double absT(double v) { return fabs(v); }
+
+// trilinear sample of V at (zf, xf, yf) and, with D, its derivatives along the
+// directions (dz1, dx1, dy1) and (dz2, dx2, dy2)
+template <typename T, bool D>
+__device__ __forceinline__ void trilinear(const Cx<T>* __restrict__ V, int64_t M, int64_t N, int64_t L, T zf, T xf,
+                                          T yf, T dz1, T dx1, T dy1, T dz2, T dx2, T dy2, double& re, double& im,
+                                          double& d1r, double& d1i, double& d2r, double& d2i) {
+    const int64_t z0 = floor_i(zf), x0 = floor_i(xf), y0 = floor_i(yf);
+    re = im = d1r = d1i = d2r = d2i = 0.0;
+    for (int cz = 0; cz < 2; ++cz) {
+        const int64_t z = z0 + cz;
+        const T uz = zf - (T)z;
+        const T wz = T(1) - absT(uz);
+        if (z < 0 || z >= L || !(wz > T(0))) continue;
+        const T sz = uz >= T(0) ? T(-1) : T(1);  // d wz / d zf
+        for (int cx = 0; cx < 2; ++cx) {
+            const int64_t x = x0 + cx;
+            const T ux = xf - (T)x;
+            const T wx = T(1) - absT(ux);
+            if (x < 0 || x >= N || !(wx > T(0))) continue;
+            const T sx = ux >= T(0) ? T(-1) : T(1);
+            for (int cy = 0; cy < 2; ++cy) {
+                const int64_t y = y0 + cy;
+                const T uy = yf - (T)y;
+                const T wy = T(1) - absT(uy);
+                if (y < 0 || y >= M || !(wy > T(0))) continue;
+                const T sy = uy >= T(0) ? T(-1) : T(1);
+                const Cx<T> v = V[(z * N + x) * M + y];
+                const double w = (double)(wz * wx * wy);
+                re += w * (double)v.x;
+                im += w * (double)v.y;
+                if (D) {
+                    const double g1 = (double)(sz * dz1 * wx * wy + wz * sx * dx1 * wy + wz * wx * sy * dy1);
+                    const double g2 = (double)(sz * dz2 * wx * wy + wz * sx * dx2 * wy + wz * wx * sy * dy2);
+                    d1r += g1 * (double)v.x;
+                    d1i += g1 * (double)v.y;
+                    d2r += g2 * (double)v.x;
+                    d2i += g2 * (double)v.y;
+                }
             }
         }
     }
 }
 
 template <typename T>
-__global__ void k_slice(const Cx<T>* __restrict__ V, const T* __restrict__ ang, Cx<T>* __restrict__ out, int64_t M,
-                        int64_t N, int64_t P, int64_t L) {
+__global__ void k_slice(const Cx<T>* __restrict__ V, const Orient<T>* __restrict__ tab, Cx<T>* __restrict__ out,
+                        int64_t M, int64_t N, int64_t P, int64_t L) {
     const uint64_t total = (uint64_t)P * N * M;
+    const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
     for (uint64_t i = tid_g(); i < total; i += str_g()) {
         const int64_t yIn = (int64_t)(i % M), xIn = (int64_t)((i / M) % N), p = (int64_t)(i / ((uint64_t)M * N));
-        const double a = (double)ang[p];
-        double re, im;
-        sample(V, M, N, L, sin(a), cos(a), xIn, yIn, re, im, (double*)nullptr, (double*)nullptr);
+        const Orient<T> o = tab[p];
+        T zf, xf, yf, xq, yq;
+        pixel_point(o, (T)(xIn - N / 2), (T)(M / 2 - yIn), hl, hn, hm, zf, xf, yf, xq, yq);
+        double re, im, a, b, c, d;
+        const T z0 = T(0);
+        trilinear<T, false>(V, M, N, L, zf, xf, yf, z0, z0, z0, z0, z0, z0, re, im, a, b, c, d);
         out[i] = Cx<T>{(T)re, (T)im};
     }
 }
 
-// G and the per-slice sums of the loss and of Re(conj(G) ds/da); grid
-// (CONVERGE_BLOCKS, P), one partial pair per block
+// G and the per-slice sums of the loss and of Re(conj(G) ds/da),
+// Re(conj(G) ds/dr); grid (CONVERGE_BLOCKS, P), one partial triple per block
 template <typename T>
-__global__ void k_slice_residual(const Cx<T>* __restrict__ V, const T* __restrict__ ang, const T* __restrict__ A,
-                                 Cx<T>* __restrict__ G, int64_t M, int64_t N, int64_t L, double* __restrict__ partials) {
-    __shared__ double sl[ADJ_THREADS], sg[ADJ_THREADS];
+__global__ void k_slice_residual(const Cx<T>* __restrict__ V, const Orient<T>* __restrict__ tab,
+                                 const T* __restrict__ A, Cx<T>* __restrict__ G, int64_t M, int64_t N, int64_t L,
+                                 double* __restrict__ partials) {
+    __shared__ double sl[ADJ_THREADS], sg[ADJ_THREADS], sh[ADJ_THREADS];
     const int64_t p = blockIdx.y;
-    const double a = (double)ang[p];
-    const double sa = sin(a), ca = cos(a);
+    const Orient<T> o = tab[p];
     const uint64_t plane = (uint64_t)N * M;
-    double accL = 0.0, accT = 0.0;
+    const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
+    double accL = 0.0, accA = 0.0, accR = 0.0;
     for (uint64_t i = blockIdx.x * (uint64_t)ADJ_THREADS + threadIdx.x; i < plane; i += (uint64_t)gridDim.x * ADJ_THREADS) {
         const int64_t yIn = (int64_t)(i % M), xIn = (int64_t)(i / M);
-        double re, im, dre, dim;
-        sample(V, M, N, L, sa, ca, xIn, yIn, re, im, &dre, &dim);
+        T zf, xf, yf, xq, yq;
+        pixel_point(o, (T)(xIn - N / 2), (T)(M / 2 - yIn), hl, hn, hm, zf, xf, yf, xq, yq);
+        double re, im, dar, dai, drr, dri;
+        trilinear<T, true>(V, M, N, L, zf, xf, yf, -yq * o.ca, T(0), yq * o.sa, -xq * o.sa, -yq, -xq * o.ca, re, im,
+                           dar, dai, drr, dri);
         const double mag = sqrt(re * re + im * im);
         const double d = mag - (double)A[p * plane + i];
         accL += d * d;
@@ -105,141 +165,112 @@ __global__ void k_slice_residual(const Cx<T>* __restrict__ V, const T* __restric
             gi = 2.0 * d * im / mag;
         }
         G[p * plane + i] = Cx<T>{(T)gr, (T)gi};
-        accT += gr * dre + gi * dim;
+        accA += gr * dar + gi * dai;
+        accR += gr * drr + gi * dri;
     }
     sl[threadIdx.x] = accL;
-    sg[threadIdx.x] = accT;
+    sg[threadIdx.x] = accA;
+    sh[threadIdx.x] = accR;
     __syncthreads();
     for (int h = ADJ_THREADS / 2; h > 0; h >>= 1) {
         if (threadIdx.x < h) {
             sl[threadIdx.x] += sl[threadIdx.x + h];
             sg[threadIdx.x] += sg[threadIdx.x + h];
+            sh[threadIdx.x] += sh[threadIdx.x + h];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        partials[(p * gridDim.x + blockIdx.x) * 2 + 0] = sl[0];
-        partials[(p * gridDim.x + blockIdx.x) * 2 + 1] = sg[0];
+        double* q = partials + (p * gridDim.x + blockIdx.x) * 3;
+        q[0] = sl[0];
+        q[1] = sg[0];
+        q[2] = sh[0];
     }
 }
 
-// gradient with respect to V: each voxel gathers w * G over the slices.  The
-// slices' sines, cosines and the reciprocals that bound each slice's rows are
-// staged per block in shared memory, ADJ_ANGLES at a time, so the voxel loop
-// evaluates no transcendental and no division.  The row window is computed in
-// float and widened by 0.01 of a row: it only bounds the loop (rows are
-// integers; its float rounding is below 1e-3 of a row at these coordinates),
-// and the double weights decide which rows contribute, exactly as before.
-constexpr int ADJ_ANGLES = 512;
-struct AngleRow {
-    double sa, ca;   // sin, cos
-    float isa, ica;  // 1/sin (0 when |sin| <= 1e-12), 1/cos (likewise)
-};
+// sums[3p + c] = the CONVERGE_BLOCKS partials of slice p, in block order
+__global__ void k_sum3_final(const double* __restrict__ partials, double* __restrict__ sums, int64_t P) {
+    for (uint64_t i = tid_g(); i < (uint64_t)P * 3; i += str_g()) {
+        const uint64_t p = i / 3, c = i % 3;
+        double acc = 0.0;
+        for (int b = 0; b < CONVERGE_BLOCKS; ++b) acc += partials[(p * CONVERGE_BLOCKS + b) * 3 + c];
+        sums[i] = acc;
+    }
+}
 
+// the adjoint's contribution of slice p to the voxel at point (j, k, l), voxel
+// indices (z, x, y): the pixels whose trilinear footprint covers the voxel.
+// In the slice's plane the voxel has the coordinates u = k (along the tilt
+// axis) and v = j sin a + l cos a, and the distance d = j cos a - l sin a.  A
+// pixel covers it only if |d| < sqrt 2 and its rotated coordinates satisfy
+// |xq - u| < 1, |yq - v| < sqrt 2; turned back by -r that rectangle bounds the
+// candidate (xr, yr), whose weight is then computed as in the forward sample.
+constexpr double ADJ_SQRT2 = 1.4142135623730951;
 template <typename T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __restrict__ G, const T* __restrict__ ang,
+__device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const Orient<T>& o, int64_t M, int64_t N,
+                                             T hl, T hn, T hm, T j, T k, T l, int64_t z, int64_t x, int64_t y,
+                                             double& re, double& im) {
+    const T d = j * o.ca - l * o.sa;
+    if (!(absT(d) < T(ADJ_SQRT2 + 1e-3))) return;
+    const T u = k, v = j * o.sa + l * o.ca;
+    const T xc = o.cr * u + o.sr * v, yc = o.cr * v - o.sr * u;
+    const T ar = absT(o.cr), as = absT(o.sr);
+    const T hx = ar + as * T(ADJ_SQRT2) + T(1e-3), hy = as + ar * T(ADJ_SQRT2) + T(1e-3);
+    const int64_t xr0 = floor_i(xc - hx) + 1, xr1 = floor_i(xc + hx);
+    const int64_t yr0 = floor_i(yc - hy) + 1, yr1 = floor_i(yc + hy);
+    for (int64_t xr = xr0; xr <= xr1; ++xr) {
+        const int64_t xIn = xr + N / 2;
+        if (xIn < 0 || xIn >= N) continue;
+        for (int64_t yr = yr0; yr <= yr1; ++yr) {
+            const int64_t yIn = M / 2 - yr;
+            if (yIn < 0 || yIn >= M) continue;
+            T zf, xf, yf, xq, yq;
+            pixel_point(o, (T)xr, (T)yr, hl, hn, hm, zf, xf, yf, xq, yq);
+            const T wz = T(1) - absT(zf - (T)z), wx = T(1) - absT(xf - (T)x), wy = T(1) - absT(yf - (T)y);
+            if (!(wz > T(0)) || !(wx > T(0)) || !(wy > T(0))) continue;
+            const Cx<T> g = Gp[xIn * M + yIn];
+            const double w = (double)(wz * wx * wy);
+            re += w * (double)g.x;
+            im += w * (double)g.y;
+        }
+    }
+}
+
+// gradient with respect to V, every slice visited (more slices than the
+// direction table holds)
+template <typename T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __restrict__ G,
+                                                               const Orient<T>* __restrict__ tab,
                                                                Cx<T>* __restrict__ gV, int64_t M, int64_t N,
                                                                int64_t P, int64_t L) {
-    __shared__ AngleRow tab[ADJ_ANGLES];
     const uint64_t total = (uint64_t)L * N * M;
-    // every thread of the block runs the same number of outer iterations
-    const uint64_t iters = (total + str_g() - 1) / str_g();
-    for (uint64_t it = 0, i = tid_g(); it < iters; ++it, i += str_g()) {
-        const bool live = i < total;
-        const int64_t y = live ? (int64_t)(i % M) : 0, x = live ? (int64_t)((i / M) % N) : 0;
-        const int64_t z = live ? (int64_t)(i / ((uint64_t)M * N)) : 0;
-        const float czf = (float)(L / 2 - z), cyf = (float)(M / 2 - y);
+    const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
+    for (uint64_t i = tid_g(); i < total; i += str_g()) {
+        const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
+        const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
         double re = 0.0, im = 0.0;
-        for (int64_t p0 = 0; p0 < P; p0 += ADJ_ANGLES) {
-            const int64_t np = (P - p0 < ADJ_ANGLES) ? P - p0 : ADJ_ANGLES;
-            __syncthreads();
-            for (int64_t k = threadIdx.x; k < np; k += ADJ_THREADS) {
-                const double a = (double)ang[p0 + k];
-                const double sa = sin(a), ca = cos(a);
-                tab[k] = AngleRow{sa, ca, fabs(sa) > 1e-12 ? (float)(1.0 / sa) : 0.0f,
-                                  fabs(ca) > 1e-12 ? (float)(1.0 / ca) : 0.0f};
-            }
-            __syncthreads();
-            if (!live) continue;
-            for (int64_t k = 0; k < np; ++k) {
-                const AngleRow w = tab[k];
-                // rows whose point (zf, yf) = (L/2 - yr sa, M/2 - yr ca) lies within 1 of (z, y) in both axes
-                float lo = -3.0e38f, hi = 3.0e38f;
-                if (w.isa != 0.0f) {
-                    const float r0 = (czf - 1.0f) * w.isa, r1 = (czf + 1.0f) * w.isa;
-                    lo = fmaxf(lo, fminf(r0, r1));
-                    hi = fminf(hi, fmaxf(r0, r1));
-                } else if (fabsf(czf) >= 1.0f) {
-                    continue;
-                }
-                if (w.ica != 0.0f) {
-                    const float r0 = (cyf - 1.0f) * w.ica, r1 = (cyf + 1.0f) * w.ica;
-                    lo = fmaxf(lo, fminf(r0, r1));
-                    hi = fminf(hi, fmaxf(r0, r1));
-                } else if (fabsf(cyf) >= 1.0f) {
-                    continue;
-                }
-                if (lo > hi + 0.02f) continue;
-                lo = fmaxf(lo, (float)(-M));  // rows outside the slice never contribute
-                hi = fminf(hi, (float)M);
-                const int64_t p = p0 + k;
-                for (int64_t yr = (int64_t)ceilf(lo - 0.01f); (float)yr <= hi + 0.01f; ++yr) {
-                    const int64_t yIn = M / 2 - yr;
-                    if (yIn < 0 || yIn >= M) continue;
-                    const double wz = 1.0 - fabs((double)(L / 2) - (double)yr * w.sa - (double)z);
-                    const double wy = 1.0 - fabs((double)(M / 2) - (double)yr * w.ca - (double)y);
-                    if (!(wz > 0.0) || !(wy > 0.0)) continue;
-                    const Cx<T> g = G[(p * N + x) * M + yIn];
-                    const double wt = wz * wy;
-                    re += wt * (double)g.x;
-                    im += wt * (double)g.y;
-                }
-            }
-        }
-        if (live) gV[i] = Cx<T>{(T)re, (T)im};
+        for (int64_t p = 0; p < P; ++p)
+            gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
+        gV[i] = Cx<T>{(T)re, (T)im};
     }
 }
 
-// the same gather visiting only the slices that can reach the voxel
-// (angle_table.cuh), in direction order; rows and weights as above, in double
+// the same gather visiting only the slices whose plane passes near the voxel
+// (angle_table.cuh: ordered by tilt, which alone fixes the plane), in
+// direction order
 template <typename T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __restrict__ G, const AngleTable tab,
+__global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __restrict__ G, const AngleTable at,
+                                                                 const Orient<T>* __restrict__ tab,
                                                                  Cx<T>* __restrict__ gV, int64_t M, int64_t N,
                                                                  int64_t L) {
     const uint64_t total = (uint64_t)L * N * M;
+    const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
     for (uint64_t i = tid_g(); i < total; i += str_g()) {
         const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
-        const double cz = (double)(L / 2) - (double)z, cy = (double)(M / 2) - (double)y;
+        const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
         double re = 0.0, im = 0.0;
-        for_slices_near(tab, cz, cy, [&](int64_t p, double sa, double ca) {
-            double lo = -1e300, hi = 1e300;
-            if (fabs(sa) > 1e-12) {
-                const double r0 = (cz - 1.0) / sa, r1 = (cz + 1.0) / sa;
-                lo = fmax(lo, fmin(r0, r1));
-                hi = fmin(hi, fmax(r0, r1));
-            } else if (fabs(cz) >= 1.0) {
-                return;
-            }
-            if (fabs(ca) > 1e-12) {
-                const double r0 = (cy - 1.0) / ca, r1 = (cy + 1.0) / ca;
-                lo = fmax(lo, fmin(r0, r1));
-                hi = fmin(hi, fmax(r0, r1));
-            } else if (fabs(cy) >= 1.0) {
-                return;
-            }
-            lo = fmax(lo, (double)(-M));
-            hi = fmin(hi, (double)M);
-            for (int64_t yr = (int64_t)ceil(lo - 1e-9); (double)yr <= hi + 1e-9; ++yr) {
-                const int64_t yIn = M / 2 - yr;
-                if (yIn < 0 || yIn >= M) continue;
-                const double wz = 1.0 - fabs((double)(L / 2) - (double)yr * sa - (double)z);
-                const double wy = 1.0 - fabs((double)(M / 2) - (double)yr * ca - (double)y);
-                if (!(wz > 0.0) || !(wy > 0.0)) continue;
-                const Cx<T> g = G[(p * N + x) * M + yIn];
-                const double wt = wz * wy;
-                re += wt * (double)g.x;
-                im += wt * (double)g.y;
-            }
+        for_slices_near(at, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double, double) {
+            gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
         });
         gV[i] = Cx<T>{(T)re, (T)im};
     }
@@ -292,28 +323,34 @@ __global__ void k_adam_volume(T* __restrict__ V, const T* __restrict__ g, T* __r
     for (uint64_t i = nv * K + tid_g(); i < n; i += str_g()) adam_apply(V[i], g[i], m[i], v[i], lr, b1, b2, eps, c1, c2);
 }
 
-// angles from the per-slice sums (sums[2p + 1] = dL/d ang[p]); loss[step] =
-// sum_p sums[2p] in index order (one thread: P is small)
+// tilts and rotations from the per-slice sums (sums[3p + 1] = dL/da_p,
+// sums[3p + 2] = dL/dr_p); rot may be null (not refined).  loss = sum_p
+// sums[3p] in index order (one thread: P is small)
 template <typename T>
-__global__ void k_adam_angles(T* __restrict__ ang, const double* __restrict__ sums, T* __restrict__ m,
-                              T* __restrict__ v, uint64_t P, T lr, T b1, T b2, T eps, T c1, T c2,
+__global__ void k_adam_angles(T* __restrict__ ang, T* __restrict__ rot, const double* __restrict__ sums,
+                              T* __restrict__ mom, uint64_t P, T lr_a, T lr_r, T b1, T b2, T eps, T c1, T c2,
                               double* __restrict__ loss) {
-    for (uint64_t i = tid_g(); i < P; i += str_g())
-        adam_apply(ang[i], (T)sums[2 * i + 1], m[i], v[i], lr, b1, b2, eps, c1, c2);
+    for (uint64_t i = tid_g(); i < P; i += str_g()) {
+        adam_apply(ang[i], (T)sums[3 * i + 1], mom[i], mom[P + i], lr_a, b1, b2, eps, c1, c2);
+        if (rot) adam_apply(rot[i], (T)sums[3 * i + 2], mom[2 * P + i], mom[3 * P + i], lr_r, b1, b2, eps, c1, c2);
+    }
     if (tid_g() == 0) {
         double acc = 0.0;
-        for (uint64_t p = 0; p < P; ++p) acc += sums[2 * p];
+        for (uint64_t p = 0; p < P; ++p) acc += sums[3 * p];
         *loss = acc;
     }
 }
 
+// volume parameters: `nv` reals (2 * voxels for a complex Fourier volume, the
+// voxels of a real volume); moments: 2 nv for them, then 4 P for the angles
 template <typename T>
-cudaError_t refine_step_t(void* V, void* ang, const void* gV, void* mom, uint64_t vox, uint64_t P,
-                          const double* sums, double lr_v, double lr_a, int step, double* loss, cudaStream_t st) {
+cudaError_t refine_step_t(void* V, uint64_t nv, void* ang, void* rot, const void* gV, void* mom, uint64_t P,
+                          const double* sums, double lr_v, double lr_a, double lr_r, int step, double* loss,
+                          cudaStream_t st) {
     const T b1 = T(0.9), b2 = T(0.999), eps = T(1e-8);
     const T c1 = T(1) - pow(b1, (T)step), c2 = T(1) - pow(b2, (T)step);
     T* mv = static_cast<T*>(mom);
-    const uint64_t n = 2 * vox;
+    const uint64_t n = nv;
     auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     if (a16(V) && a16(gV) && a16(mv) && a16(mv + n))
         k_adam_volume<T, true><<<ew_grid(n / Vec16<T>::N + 1, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
@@ -321,72 +358,117 @@ cudaError_t refine_step_t(void* V, void* ang, const void* gV, void* mom, uint64_
     else
         k_adam_volume<T, false><<<ew_grid(n, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
             static_cast<T*>(V), static_cast<const T*>(gV), mv, mv + n, n, (T)lr_v, b1, b2, eps, c1, c2);
-    k_adam_angles<T><<<1, 128, 0, st>>>(static_cast<T*>(ang), sums, mv + 2 * n, mv + 2 * n + P, P, (T)lr_a, b1, b2,
-                                        eps, c1, c2, loss);
+    k_adam_angles<T><<<1, 128, 0, st>>>(static_cast<T*>(ang), static_cast<T*>(rot), sums, mv + 2 * n, P, (T)lr_a,
+                                        (T)lr_r, b1, b2, eps, c1, c2, loss);
     count_launches(2);
+    return cudaGetLastError();
+}
+
+// a real volume as complex values (imaginary parts 0), and back: the real
+// parts times `scale`
+template <typename T>
+__global__ void k_real_to_complex(const T* __restrict__ r, Cx<T>* __restrict__ c, uint64_t n) {
+    for (uint64_t i = tid_g(); i < n; i += str_g()) c[i] = Cx<T>{r[i], T(0)};
+}
+template <typename T>
+__global__ void k_complex_real_part(const Cx<T>* __restrict__ c, T* __restrict__ r, T scale, uint64_t n) {
+    for (uint64_t i = tid_g(); i < n; i += str_g()) r[i] = c[i].x * scale;
+}
+
+template <typename T>
+cudaError_t slice_loss_grad_t(const void* V, const void* ang, const void* tab, const void* A, void* G, void* gV,
+                              uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
+                              void* atab, cudaStream_t st) {
+    dim3 grid(CONVERGE_BLOCKS, (unsigned)p);
+    k_slice_residual<T><<<grid, ADJ_THREADS, 0, st>>>((const Cx<T>*)V, (const Orient<T>*)tab, (const T*)A,
+                                                       (Cx<T>*)G, m, n, l, partials);
+    k_sum3_final<<<ew_grid(3 * p, ADJ_THREADS), ADJ_THREADS, 0, st>>>(partials, sums, (int64_t)p);
+    count_launches(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const uint64_t vox = l * n * m;
+    const unsigned g = ew_grid(vox, ADJ_THREADS);
+    if (atab && p <= (uint64_t)ANGLE_TABLE_MAX) {
+        e = launch_sort_angles<T>((const T*)ang, (int64_t)p, atab, st);
+        if (e != cudaSuccess) return e;
+        const AngleTable t = angle_table_view(atab, (int64_t)p);
+        k_slice_adjoint_w<T><<<g, ADJ_THREADS, 0, st>>>((const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n,
+                                                         l);
+        count_launches(2);
+        return cudaGetLastError();
+    }
+    k_slice_adjoint<T><<<g, ADJ_THREADS, 0, st>>>((const Cx<T>*)G, (const Orient<T>*)tab, (Cx<T>*)gV, m, n, p, l);
+    count_launches();
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_refine_step(bool dbl, void* V, void* ang, const void* gV, void* moments, uint64_t vox, uint64_t P,
-                               const double* sums, double lr_volume, double lr_angle, int step, double* loss,
-                               cudaStream_t st) {
-    return dbl ? refine_step_t<double>(V, ang, gV, moments, vox, P, sums, lr_volume, lr_angle, step, loss, st)
-               : refine_step_t<float>(V, ang, gV, moments, vox, P, sums, lr_volume, lr_angle, step, loss, st);
+uint64_t orient_table_bytes(bool dbl, uint64_t p) { return p * (dbl ? sizeof(Orient<double>) : sizeof(Orient<float>)); }
+
+cudaError_t launch_orient_table(bool dbl, const void* ang, const void* rot, void* tab, uint64_t p, cudaStream_t st) {
+    if (p == 0) return cudaSuccess;
+    const unsigned g = ew_grid(p, ADJ_THREADS);
+    if (dbl)
+        k_orient_table<double><<<g, ADJ_THREADS, 0, st>>>((const double*)ang, (const double*)rot,
+                                                          (Orient<double>*)tab, (int64_t)p);
+    else
+        k_orient_table<float><<<g, ADJ_THREADS, 0, st>>>((const float*)ang, (const float*)rot, (Orient<float>*)tab,
+                                                         (int64_t)p);
+    count_launches();
+    return cudaGetLastError();
 }
 
-cudaError_t launch_slice(bool dbl, const void* V, const void* ang, void* out, uint64_t m, uint64_t n, uint64_t p,
+cudaError_t launch_refine_step(bool dbl, void* V, uint64_t nv, void* ang, void* rot, const void* gV, void* moments,
+                               uint64_t P, const double* sums, double lr_volume, double lr_angle, double lr_rot,
+                               int step, double* loss, cudaStream_t st) {
+    return dbl ? refine_step_t<double>(V, nv, ang, rot, gV, moments, P, sums, lr_volume, lr_angle, lr_rot, step, loss,
+                                       st)
+               : refine_step_t<float>(V, nv, ang, rot, gV, moments, P, sums, lr_volume, lr_angle, lr_rot, step, loss,
+                                      st);
+}
+
+cudaError_t launch_slice(bool dbl, const void* V, const void* tab, void* out, uint64_t m, uint64_t n, uint64_t p,
                          uint64_t l, cudaStream_t st) {
     const uint64_t total = p * n * m;
     if (total == 0) return cudaSuccess;
     const unsigned g = ew_grid(total, ADJ_THREADS);
     if (dbl)
-        k_slice<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)V, (const double*)ang, (Cx<double>*)out, m, n,
-                                                   p, l);
+        k_slice<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)V, (const Orient<double>*)tab,
+                                                   (Cx<double>*)out, m, n, p, l);
     else
-        k_slice<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)V, (const float*)ang, (Cx<float>*)out, m, n, p, l);
+        k_slice<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)V, (const Orient<float>*)tab, (Cx<float>*)out, m,
+                                                  n, p, l);
     count_launches();
     return cudaGetLastError();
 }
 
-cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* A, void* G, void* gV,
-                                   uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials, double* sums,
-                                   void* atab, cudaStream_t st) {
+cudaError_t launch_slice_loss_grad(bool dbl, const void* V, const void* ang, const void* tab, const void* A, void* G,
+                                   void* gV, uint64_t m, uint64_t n, uint64_t p, uint64_t l, double* partials,
+                                   double* sums, void* atab, cudaStream_t st) {
     if (p == 0) return cudaSuccess;
     if (p > 65535) return cudaErrorInvalidValue;
-    dim3 grid(CONVERGE_BLOCKS, (unsigned)p);
-    if (dbl)
-        k_slice_residual<double><<<grid, ADJ_THREADS, 0, st>>>((const Cx<double>*)V, (const double*)ang,
-                                                               (const double*)A, (Cx<double>*)G, m, n, l, partials);
-    else
-        k_slice_residual<float><<<grid, ADJ_THREADS, 0, st>>>((const Cx<float>*)V, (const float*)ang,
-                                                              (const float*)A, (Cx<float>*)G, m, n, l, partials);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    e = launch_norm_final(partials, sums, p, st);
-    if (e != cudaSuccess) return e;
-    const uint64_t vox = l * n * m;
-    const unsigned g = ew_grid(vox, ADJ_THREADS);
-    if (atab && p <= (uint64_t)ANGLE_TABLE_MAX) {
-        e = dbl ? launch_sort_angles<double>((const double*)ang, (int64_t)p, atab, st)
-                : launch_sort_angles<float>((const float*)ang, (int64_t)p, atab, st);
-        if (e != cudaSuccess) return e;
-        const AngleTable t = angle_table_view(atab, (int64_t)p);
+    return dbl ? slice_loss_grad_t<double>(V, ang, tab, A, G, gV, m, n, p, l, partials, sums, atab, st)
+               : slice_loss_grad_t<float>(V, ang, tab, A, G, gV, m, n, p, l, partials, sums, atab, st);
+}
+
+cudaError_t launch_real_complex(bool dbl, bool to_complex, void* real, void* cplx, double scale, uint64_t n,
+                                cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const unsigned g = ew_grid(n, ADJ_THREADS);
+    if (to_complex) {
         if (dbl)
-            k_slice_adjoint_w<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)G, t, (Cx<double>*)gV, m, n, l);
+            k_real_to_complex<double><<<g, ADJ_THREADS, 0, st>>>((const double*)real, (Cx<double>*)cplx, n);
         else
-            k_slice_adjoint_w<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)G, t, (Cx<float>*)gV, m, n, l);
-        count_launches(3);
-        return cudaGetLastError();
+            k_real_to_complex<float><<<g, ADJ_THREADS, 0, st>>>((const float*)real, (Cx<float>*)cplx, n);
+    } else {
+        if (dbl)
+            k_complex_real_part<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)cplx, (double*)real, scale, n);
+        else
+            k_complex_real_part<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)cplx, (float*)real,
+                                                                  (float)scale, n);
     }
-    if (dbl)
-        k_slice_adjoint<double><<<g, ADJ_THREADS, 0, st>>>((const Cx<double>*)G, (const double*)ang, (Cx<double>*)gV,
-                                                           m, n, p, l);
-    else
-        k_slice_adjoint<float><<<g, ADJ_THREADS, 0, st>>>((const Cx<float>*)G, (const float*)ang, (Cx<float>*)gV, m,
-                                                          n, p, l);
-    count_launches(2);
+    count_launches();
     return cudaGetLastError();
 }
 

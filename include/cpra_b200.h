@@ -355,6 +355,41 @@ int cpra_b200_slice_loss_grad(cpra_b200_ctx* ctx, const void* V, const void* ang
 int cpra_b200_refine(cpra_b200_ctx* ctx, void* V, void* angles, const void* A, uint64_t m, uint64_t n, uint64_t p,
                      uint64_t l, int steps, double lr_volume, double lr_angle, double* loss_host);
 
+/* Extension (project-defined): the slice operator with two orientation degrees
+ * of freedom per slice: the tilt angles[p] as above and an in-plane rotation
+ * rot[p] (radians, element type; may be null: none) of the detector grid.
+ * Pixel (xIn, yIn) has xr = xIn - n/2, yr = m/2 - yIn, rotated to
+ * xq = xr cos r - yr sin r, yq = xr sin r + yr cos r, and samples V
+ * trilinearly at z = l/2 - yq sin a, x = n/2 + xq, y = m/2 - yq cos a (with
+ * rot null this is cpra_b200_slice).  Coordinates and weights are computed in
+ * the element type. */
+int cpra_b200_slice_orient(cpra_b200_ctx* ctx, const void* V, const void* angles, const void* rot, uint64_t m,
+                           uint64_t n, uint64_t p, uint64_t l, void* slices);
+/* Extension (project-defined): cpra_b200_slice_loss_grad for the two-parameter
+ * orientations; grad_rot_host[p] (host, double, may be null) receives
+ * dL/drot_p.  Synchronous. */
+int cpra_b200_slice_loss_grad_orient(cpra_b200_ctx* ctx, const void* V, const void* angles, const void* rot,
+                                     const void* A, uint64_t m, uint64_t n, uint64_t p, uint64_t l, void* grad_V,
+                                     double* loss_host, double* grad_angles_host, double* grad_rot_host);
+/* Extension (project-defined): the amplitude loss of a real-space volume,
+ * L = sum (|slice(Forward3D(vol), a_p, r_p)| - A_p)^2, and its gradients
+ * through the hand-written adjoints of the modulus loss, the slice operator
+ * and the transform: grad_vol (device, [l][n][m] element type) receives
+ * dL/dvol = Re(Forward3D^H dL/dV), Forward3D^H being the inverse transform
+ * without its 1/(m n l).  The context must have been created with this volume's
+ * (m, n, l), powers of two 2..1024.  Synchronous. */
+int cpra_b200_volume_loss_grad(cpra_b200_ctx* ctx, const void* vol, const void* angles, const void* rot,
+                               const void* A, uint64_t m, uint64_t n, uint64_t p, uint64_t l, void* grad_vol,
+                               double* loss_host, double* grad_angles_host, double* grad_rot_host);
+/* Extension (project-defined): cpra_b200_refine for the two-parameter
+ * orientations (rot may be null: not refined) and, with real_space != 0, a
+ * real-space volume V ([l][n][m] element type) refined through
+ * cpra_b200_volume_loss_grad's chain (the context then needs the volume's
+ * (m, n, l)); with real_space == 0, V is the complex Fourier volume. */
+int cpra_b200_refine_orient(cpra_b200_ctx* ctx, void* V, int real_space, void* angles, void* rot, const void* A,
+                            uint64_t m, uint64_t n, uint64_t p, uint64_t l, int steps, double lr_volume,
+                            double lr_angle, double lr_rot, double* loss_host);
+
 /* Extension: the best of the random starts, the step the reference's
  * benchmark describes and omits (src/benchmark_mkl.cpp:127-138).  x is
  * [P][batch][m][n] (the driver's layout), A is [P][m][n].  The score of start

@@ -549,6 +549,103 @@ def hio_shrinkwrap(x0, A, S0, L, batch, iters, beta, sw_every=0, sigma_start=3.0
     return np.concatenate(xs), np.concatenate(ss), np.concatenate(es)
 
 
+def _orient_weights(M, N, L, a, r=0.0):
+    """Trilinear sampling of one slice with tilt a and in-plane rotation r
+    (the slice operator's geometry, project-defined; r = 0 is the merges'
+    bilinear sample on the plane x = xIn): for every slice pixel, [N][M] with
+    yIn fastest, the (z, x, y) of its up to eight voxels, their weights and the
+    weights' derivatives in a and r (float64).  xr = xIn - N/2, yr = M/2 - yIn,
+    xq = xr cos r - yr sin r, yq = xr sin r + yr cos r; the point is
+    z = L/2 - yq sin a, x = N/2 + xq, y = M/2 - yq cos a."""
+    xIn, yIn = np.meshgrid(np.arange(N), np.arange(M), indexing="ij")
+    xr, yr = (xIn - N // 2).astype(np.float64), (M // 2 - yIn).astype(np.float64)
+    sa, ca, sr, cr = np.sin(a), np.cos(a), np.sin(r), np.cos(r)
+    xq, yq = cr * xr - sr * yr, sr * xr + cr * yr
+    pts = (L // 2 - yq * sa, N // 2 + xq, M // 2 - yq * ca)
+    d_a = (-yq * ca, np.zeros_like(yq), yq * sa)
+    d_r = (-xq * sa, -yq, -xq * ca)
+    lo = [np.floor(q).astype(np.int64) for q in pts]
+    out = []
+    for cz in (0, 1):
+        for cx in (0, 1):
+            for cy in (0, 1):
+                idx, w, ga, gr = [], [], [], []
+                for q, l0, c, da, dr in zip(pts, lo, (cz, cx, cy), d_a, d_r):
+                    v = l0 + c
+                    u = q - v
+                    idx.append(v)
+                    w.append(np.maximum(0.0, 1.0 - np.abs(u)))
+                    sg = np.where(u >= 0, -1.0, 1.0)
+                    ga.append(sg * da)
+                    gr.append(sg * dr)
+                z, x, y = idx
+                ok = (z >= 0) & (z < L) & (x >= 0) & (x < N) & (y >= 0) & (y < M) & (w[0] > 0) & (w[1] > 0) & (w[2] > 0)
+                wt = w[0] * w[1] * w[2]
+                dwa = ga[0] * w[1] * w[2] + w[0] * ga[1] * w[2] + w[0] * w[1] * ga[2]
+                dwr = gr[0] * w[1] * w[2] + w[0] * gr[1] * w[2] + w[0] * w[1] * gr[2]
+                out.append((np.where(ok, z, 0), np.where(ok, x, 0), np.where(ok, y, 0), ok, np.where(ok, wt, 0.0),
+                            np.where(ok, dwa, 0.0), np.where(ok, dwr, 0.0)))
+    return out
+
+
+def slice_volume_orient(V, angles, rot, M, N, P, L):
+    """Central slices ([P][N][M] complex128) of the [L][N][M] Fourier volume V
+    at tilts `angles` and in-plane rotations `rot` (None: zero), float64."""
+    V = np.asarray(V).astype(np.complex128).reshape(L, N, M)
+    out = np.zeros((P, N, M), np.complex128)
+    for p in range(P):
+        r = 0.0 if rot is None else float(rot[p])
+        for z, x, y, ok, w, _, _ in _orient_weights(M, N, L, float(angles[p]), r):
+            out[p] += w * V[z, x, y]
+    return out
+
+
+def slice_loss_grad_orient(V, angles, rot, A, M, N, P, L):
+    """Loss sum (|slice| - A)^2 and its gradients in float64: (loss,
+    dL/dRe V + i dL/dIm V as [L][N][M], dL/da [P], dL/dr [P])."""
+    V = np.asarray(V).astype(np.complex128).reshape(L, N, M)
+    A = np.asarray(A, np.float64).reshape(P, N, M)
+    gV = np.zeros_like(V)
+    ga, gr = np.zeros(P), np.zeros(P)
+    loss = 0.0
+    for p in range(P):
+        ws = _orient_weights(M, N, L, float(angles[p]), 0.0 if rot is None else float(rot[p]))
+        s = np.zeros((N, M), np.complex128)
+        dsa = np.zeros((N, M), np.complex128)
+        dsr = np.zeros((N, M), np.complex128)
+        for z, x, y, ok, w, dwa, dwr in ws:
+            vals = V[z, x, y]
+            s += w * vals
+            dsa += dwa * vals
+            dsr += dwr * vals
+        mag = np.abs(s)
+        d = mag - A[p]
+        loss += float((d * d).sum())
+        G = np.where(mag > 0, 2 * d * s / np.where(mag > 0, mag, 1), 0)
+        ga[p] = float(np.real(np.conj(G) * dsa).sum())
+        gr[p] = float(np.real(np.conj(G) * dsr).sum())
+        for z, x, y, ok, w, _, _ in ws:
+            np.add.at(gV, (z[ok], x[ok], y[ok]), (w * G)[ok])
+    return loss, gV, ga, gr
+
+
+def volume_loss_grad(vol, angles, rot, A, M, N, P, L):
+    """The loss of a real-space volume through the shifted 3D transform
+    (Forward3D, MKL_Impl.inl:154-178 with fftshifts; cube volumes) and the
+    slice operator, float64: (loss, dL/dvol [L][N][M] real, dL/da, dL/dr).
+    dL/dvol = Re(Forward3D^H dL/dV), the adjoint transform being the inverse
+    transform without its normalisation."""
+    assert M == N == L
+    vol = np.asarray(vol, np.float64).reshape(L, N, M)
+    impl = OracleImpl(np.float64, M, N, L, 1)
+    VF = vol.astype(np.complex128).ravel().copy()
+    impl.Forward3D(VF)
+    loss, gV, ga, gr = slice_loss_grad_orient(VF, angles, rot, A, M, N, P, L)
+    g = gV.ravel().copy()
+    impl.Backward3D(g)
+    return loss, np.real(g).reshape(L, N, M) * float(M * N * L), ga, gr
+
+
 def _slice_weights(M, N, L, a):
     """Bilinear sampling of one slice (the merges' geometry): for every slice
     pixel (xIn, yIn) the (z, y) of its up to four voxels on the plane x = xIn,
