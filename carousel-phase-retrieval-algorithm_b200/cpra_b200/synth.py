@@ -10,8 +10,11 @@ benchmark configurations (no dataset is involved; all inputs are generated).
   sphere, 0 outside).
 * ``patterns_2d(...)``: independent 2D objects (Gaussian blobs in a disc,
   phase in [-0.3, 0.3]) with their noisy moduli and supports.
+* ``carousel_gpu(...)``: the large carousel on the GPU, its moduli taken with
+  the slice operator itself (tilt and in-plane rotation per pattern), so that
+  the data match the model of the orientation refinement.
 
-Host-side data preparation only (numpy); nothing here is on the GPU path.
+Data preparation only: nothing here is on the benchmarked path.
 """
 from __future__ import annotations
 
@@ -128,14 +131,20 @@ def random_phase_start(A, seed=0):
 
 def carousel_gpu(torch, n=256, P=180, step_deg=1.0, jitter_deg=0.3, ellipsoids=64, axes=(4, 16), radius=None,
                  photons=1e8, seed=3, device="cuda"):
-    """The carousel synthesis of ``carousel`` at sizes where numpy is too slow
-    (256^3 and up), on the GPU with torch: a real volume of random ellipsoids
-    inside a sphere, parallel projections at P angles (step_deg apart, each
-    jittered by N(0, jitter_deg)) about the same axis, Poisson-noised far-field
-    moduli and disc supports.  Data preparation only; trilinear resampling by
-    torch's grid_sample.  Returns dict(A, S [P][n][n] float32, angles_true,
-    angles_nominal [P] float32 radians, volume [n][n][n] float32), all on
-    `device`."""
+    """The carousel synthesis at sizes where numpy is too slow (256^3 and up),
+    on the GPU, with the slice operator's own geometry so that the data match
+    the model the refinement fits: a real volume of random ellipsoids inside a
+    sphere, its Fourier volume (Forward3D), central slices at P tilts step_deg
+    apart, each tilt and each in-plane rotation jittered by N(0, jitter_deg)
+    (cpra_b200_slice_orient: the merges' geometry with the detector grid turned
+    in its plane), intensities |slice|^2 scaled to `photons` per pattern on
+    average, Poisson noise, and disc supports.  Returns dict(A [P][n][n]
+    float32 in the 2D stage's pattern layout (row: the tilted coordinate,
+    column: the tilt axis), A_slices [P][n][n] in the slice layout (the
+    transpose), S, angles_true, rot_true, angles_nominal [P] float32 radians,
+    volume [n][n][n] float32 in the data's units, i.e. the real-space volume
+    whose slices the noise-free A are), all on `device`."""
+    import cpra_b200
     g = torch.Generator(device=device).manual_seed(seed)
     radius = radius if radius is not None else 0.3125 * n
     ax = torch.arange(n, device=device, dtype=torch.float32) - n / 2
@@ -155,24 +164,24 @@ def carousel_gpu(torch, n=256, P=180, step_deg=1.0, jitter_deg=0.3, ellipsoids=6
     del z, y, x
     nominal = torch.deg2rad(torch.arange(P, device=device, dtype=torch.float64) * step_deg)
     true = nominal + torch.deg2rad(jitter_deg * torch.randn(P, device=device, generator=g, dtype=torch.float64))
-    # projection at angle a about the y axis: detector row u, integration w,
-    # x = cos(a) u + sin(a) w, z = -sin(a) u + cos(a) w (grid coordinates in [-1, 1])
-    lin = (torch.arange(n, device=device, dtype=torch.float32) + 0.5) / n * 2 - 1
-    w_, u_, y_ = torch.meshgrid(lin, lin, lin, indexing="ij")
-    src = vol[None, None]
-    proj = torch.empty((P, n, n), device=device)
-    for p in range(P):
-        ca, sa = float(torch.cos(true[p])), float(torch.sin(true[p]))
-        grid = torch.stack([ca * u_ + sa * w_, y_, -sa * u_ + ca * w_], -1)[None]
-        proj[p] = torch.nn.functional.grid_sample(src, grid, mode="bilinear", padding_mode="zeros",
-                                                  align_corners=False)[0, 0].sum(0)
-    del w_, u_, y_
-    F = torch.fft.fftshift(torch.fft.fft2(torch.fft.ifftshift(proj.double(), dim=(-2, -1))), dim=(-2, -1))
-    I = F.abs() ** 2
-    I = I * (photons / I.sum(dim=(-2, -1), keepdim=True))
-    A = torch.sqrt(torch.poisson(I, generator=g)).float()
+    rot = torch.deg2rad(jitter_deg * torch.randn(P, device=device, generator=g, dtype=torch.float64))
+    impl = cpra_b200.B200Impl(n, n, n, 1)
+    VF = vol.reshape(-1).to(torch.complex64)
+    impl.Forward3D(VF)
+    sl = torch.empty(P * n * n, dtype=torch.complex64, device=device)
+    impl.slice_orient(VF, true.float().contiguous(), rot.float().contiguous(), n, n, P, n, sl)
+    impl.Sync()
+    impl.close()
+    del VF
+    I = sl.abs().double().reshape(P, n, n) ** 2
+    del sl
+    scale = photons * P / float(I.sum())
+    I = I * scale
+    A_sl = torch.sqrt(torch.poisson(I, generator=g)).float()
+    del I
     yy, xx = torch.meshgrid(ax, ax, indexing="ij")
     disc = ((yy * yy + xx * xx) <= (radius + 2) ** 2).float()
     S = disc.expand(P, n, n).contiguous()
-    return {"A": A.contiguous(), "S": S, "angles_true": true.float(), "angles_nominal": nominal.float(),
-            "volume": vol}
+    return {"A": A_sl.transpose(1, 2).contiguous(), "A_slices": A_sl.contiguous(), "S": S,
+            "angles_true": true.float(), "rot_true": rot.float(), "angles_nominal": nominal.float(),
+            "volume": vol * float(scale) ** 0.5}
