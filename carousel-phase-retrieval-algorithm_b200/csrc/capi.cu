@@ -248,6 +248,8 @@ struct cpra_b200_ctx {
     uint64_t hio_chunk = 0;
     // CPRA_B200_OPT_TMEM: the 128 x 128 fused kernels keep their iterates in tensor memory
     bool tmem = true;
+    // CPRA_B200_OPT_FUSED3D: the 3D loops as fused axis passes (off: the operator kernels)
+    bool fused3d = false;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -518,7 +520,7 @@ int take_deferred(cpra_b200_ctx* c) {
 bool fusable_shape(const cpra_b200_ctx* c) { return c->fusion && dm_fusable(c); }
 // the 3D iteration fuses for power-of-two volumes (axis passes)
 bool fusable_shape3d(const cpra_b200_ctx* c) {
-    return c->fusion && c->l > 1 && constraint3d_fused_supported(c->m, c->n, c->l);
+    return c->fusion && c->fused3d && c->l > 1 && constraint3d_fused_supported(c->m, c->n, c->l);
 }
 
 // Does `op` extend the pending prefix (of length k) of the pattern?
@@ -770,6 +772,7 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
             break;
         case CPRA_B200_OPT_AUTOTUNE: c->autotune = value != 0; break;
         case CPRA_B200_OPT_TMEM: c->tmem = value != 0; break;
+        case CPRA_B200_OPT_FUSED3D: c->fused3d = value != 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -859,14 +862,15 @@ int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void*
     const uint64_t vol = c->m * c->n * c->l, num = vol * c->batch;
     // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
     const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
-    if (constraint3d_fused_supported(c->m, c->n, c->l)) {
+    if (c->fused3d && constraint3d_fused_supported(c->m, c->n, c->l)) {
         CPRA_CHECK_CUDA(launch_constraint3d(c->dbl, x, C, S, c->m, c->n, c->l, c->batch, iters, c->space_mode, scale,
                                             twiddles(c, c->m), twiddles(c, c->n), twiddles(c, c->l), c->work,
                                             c->stream),
                         "constraint3d");
         return CPRA_B200_OK;
     }
-    // other sizes: the four operators in turn
+    // the four operators in turn (by default: faster on B200 than the fused
+    // passes at 64^3 to 256^3, same bits)
     r = ensure_work(c, num * c->csize());
     if (r) return r;
     for (int it = 0; it < iters; ++it) {
@@ -1717,6 +1721,7 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
         case CPRA_B200_OPT_IO_CHUNK: *value = (int64_t)c->io_chunk; break;
         case CPRA_B200_OPT_AUTOTUNE: *value = c->autotune ? 1 : 0; break;
         case CPRA_B200_OPT_TMEM: *value = c->tmem ? 1 : 0; break;
+        case CPRA_B200_OPT_FUSED3D: *value = c->fused3d ? 1 : 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;

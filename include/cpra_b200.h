@@ -77,6 +77,10 @@ extern "C" {
                                     runs only once it is cached.  No tuning during a stream capture or for
                                     epi < 2; if the copy cannot be allocated the key keeps the automatic
                                     choice.  0 (default): the automatic choice.  Same results either way. */
+#define CPRA_B200_OPT_FUSED3D 12   /* 1: cpra_b200_constraint3d and the recognised 3D difference-map iteration
+                                    run as fused axis passes (5 and 10 passes per iteration); 0 (default):
+                                    as the operator kernels, measured faster on B200 (64^3 to 256^3).  Same
+                                    results either way. */
 #define CPRA_B200_OPT_TMEM 11      /* 1 (default): the fused 128 x 128 kernels keep their per-thread iterates
                                     in the SM's tensor memory for the whole launch (x and t2 of the
                                     difference map); 0: through L2 once per iteration.  Same results either

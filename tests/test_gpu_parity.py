@@ -993,9 +993,12 @@ def test_constraint3d_equals_operator_calls(tb, T, M, N, L, B, mode):
     S = (rng.uniform(size=vol) > 0.4).astype(T)
     dtype = "float32" if T == np.float32 else "float64"
     outs = []
-    for fused in (False, True):
+    # the operator calls; constraint3d on its default path (the operator
+    # kernels); constraint3d as fused axis passes (CPRA_B200_OPT_FUSED3D)
+    for fused, fused3d in ((False, 0), (True, 0), (True, 1)):
         impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
         assert impl.set_option(cb.OPT_SPACE_MODE, mode)
+        assert impl.set_option(cb.OPT_FUSED3D, fused3d)
         x = dev(torch, x0)
         Cd, Sd = dev(torch, C), dev(torch, S)
         for _ in range(2):
@@ -1009,6 +1012,7 @@ def test_constraint3d_equals_operator_calls(tb, T, M, N, L, B, mode):
         assert impl.Sync()
         outs.append(host(x))
     np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
     if mode == 0:
         o = O.OracleImpl(T, M, N, L, B)
         xo = x0.copy()
@@ -1090,8 +1094,9 @@ def test_conv_run_equals_driver(tb, T, M, N, L, B, iters, with_err, final):
     err_r = np.zeros(B, T) if with_err else None
     conv_driver_per_call(ref, torch, xr, A, S, M, N, L, B, iters, 0.9, err_r, final)
     run = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
-    for graph in (0, 1, 1):
+    for graph, fused3d in ((0, 0), (1, 0), (1, 0), (0, 1), (1, 1), (1, 1)):
         assert run.set_option(cb.OPT_GRAPH, graph)
+        assert run.set_option(cb.OPT_FUSED3D, fused3d)
         x = dev(torch, x0)
         err = np.zeros(B, T) if with_err else None
         assert run.conv_run(x, A, S, iters, 0.9, final_step=final, err=err) and run.Sync()
@@ -1124,8 +1129,9 @@ def test_conv_run_equals_driver(tb, T, M, N, L, B, iters, with_err, final):
                                              (np.float64, 16, 16, 16, 1, 2), (np.float32, 12, 12, 12, 1, 2)])
 def test_dm3d_recorder_equals_per_call(tb, T, M, N, L, B, iters):
     """The 12-call iteration with the 3D transforms, issued one call at a time,
-    runs as ten fused axis passes per iteration (power-of-two sizes) and
-    writes the same bits as with fusion off; other sizes run per call."""
+    runs as ten fused axis passes per iteration (power-of-two sizes, with
+    CPRA_B200_OPT_FUSED3D) and writes the same bits as with fusion off; other
+    sizes run per call."""
     torch, cb = tb
     rng = np.random.default_rng(M * N * L + B)
     vol = M * N * L
@@ -1139,6 +1145,7 @@ def test_dm3d_recorder_equals_per_call(tb, T, M, N, L, B, iters):
     for fusion in (0, 1):
         impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, M, N, L, B, dtype=dtype)
         impl.set_option(cb.OPT_FUSION, fusion)
+        impl.set_option(cb.OPT_FUSED3D, fusion)
         x, t1, t2 = (dev(torch, x0) for _ in range(3))
         A, S = dev(torch, amps), dev(torch, sup)
         for _ in range(iters):
