@@ -58,7 +58,7 @@ _lib = None
 class HioBucket(C.Structure):
     """cpra_b200_hio_bucket (include/cpra_b200.h)."""
     _fields_ = [("side", C.c_uint64), ("count", C.c_uint64), ("x", C.c_void_p), ("A", C.c_void_p),
-                ("S", C.c_void_p), ("estimate", C.c_void_p)]
+                ("S", C.c_void_p), ("estimate", C.c_void_p), ("sigma_start", C.c_double), ("sigma_end", C.c_double)]
 
 
 _SIGS = {
@@ -401,11 +401,13 @@ class B200Impl:
         """HIO + shrinkwrap over patterns of uneven sizes in one call
         (project-defined): ``buckets`` is a list of dicts with keys side,
         count, x, A, S and optionally estimate (device buffers, per-pattern
-        contiguous); each bucket runs on its own stream."""
+        contiguous) and sigma_start, sigma_end (the bucket's own blur
+        schedule); each bucket runs on its own stream."""
         arr = (HioBucket * len(buckets))()
         for i, b in enumerate(buckets):
             arr[i] = HioBucket(int(b["side"]), int(b["count"]), _addr(b["x"]), _addr(b["A"]), _addr(b["S"]),
-                               _addr(b.get("estimate")))
+                               _addr(b.get("estimate")), float(b.get("sigma_start", 0.0)),
+                               float(b.get("sigma_end", 0.0)))
         return _check(lib().cpra_b200_hio_batched(self._h, C.cast(arr, C.c_void_p), len(buckets), int(iters),
                                                   float(beta), int(sw_every), float(sigma_start), float(sigma_end),
                                                   float(threshold), 1 if positivity else 0), "hio_batched")

@@ -1314,7 +1314,18 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
         if (!b.x || !b.A || !b.S || b.count == 0) return fail(CPRA_B200_EARG, "hio_batched: bucket without data");
         if (!hio_side_supported(c->dbl, b.side))
             return fail(CPRA_B200_EUNSUP, "hio_batched: sides must be 32, 64, 128, 256 or 512 (float context)");
+        if ((b.sigma_start > 0.0) != (b.sigma_end > 0.0))
+            return fail(CPRA_B200_EARG, "hio_batched: a bucket's sigma_start and sigma_end are both set or neither");
     }
+    // each bucket's parameters: its own blur schedule when it has one
+    auto bucket_params = [&](const cpra_b200_hio_bucket& b) {
+        HioParams hb = h;
+        if (b.sigma_start > 0.0) {
+            hb.sigma_start = b.sigma_start;
+            hb.sigma_end = b.sigma_end;
+        }
+        return hb;
+    };
     r = flush(c);
     if (r) return take_deferred(c);
     if (iters == 0) {
@@ -1347,7 +1358,8 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
         if (r) return r;
         if (h.updates() > 0) {
             const void* unused;
-            r = blur_tables(c, b.side, h.updates(), sigma_start, sigma_end, &unused);
+            const HioParams hb = bucket_params(b);
+            r = blur_tables(c, b.side, hb.updates(), hb.sigma_start, hb.sigma_end, &unused);
             if (r) return r;
         }
     }
@@ -1359,8 +1371,8 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
             const uint64_t plane = b.side * b.side;
             const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
             CPRA_CHECK_CUDA(cudaStreamWaitEvent(lane.stream, c->fork_event, 0), "hio_batched");
-            int rr = hio_enqueue(c, HioJob{b.side, b.count, b.x, b.A, plane, b.S, plane, b.estimate}, h, chunk,
-                                 lane.scratch, lane.stream);
+            int rr = hio_enqueue(c, HioJob{b.side, b.count, b.x, b.A, plane, b.S, plane, b.estimate},
+                                 bucket_params(b), chunk, lane.scratch, lane.stream);
             if (rr) return rr;
             CPRA_CHECK_CUDA(cudaEventRecord(lane.done, lane.stream), "hio_batched");
             CPRA_CHECK_CUDA(cudaStreamWaitEvent(c->stream, lane.done, 0), "hio_batched");

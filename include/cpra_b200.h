@@ -306,6 +306,8 @@ typedef struct cpra_b200_hio_bucket {
     const void* A;
     void* S;
     void* estimate;
+    double sigma_start; /* this bucket's shrinkwrap blur schedule (pixels); <= 0: the call's */
+    double sigma_end;
 } cpra_b200_hio_bucket;
 #define CPRA_B200_MAX_BUCKETS 64
 

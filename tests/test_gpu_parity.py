@@ -849,29 +849,37 @@ def test_hio_large_full_run_rfactor(tb):
 
 
 # ---- uneven sizes in one call --------------------------------------------------------------
-def test_hio_batched_matches_per_size_calls(tb):
+@pytest.mark.parametrize("own_sigma", [False, True])
+def test_hio_batched_matches_per_size_calls(tb, own_sigma):
     """Each bucket of the uneven-size call gives the same bits as a
     single-size call with the same patterns (the buckets only share the
-    device, not data)."""
+    device, not data); with own_sigma each bucket has its own blur schedule
+    (3 -> 1.5 px times side / 128) and the CUDA backend's DataConstraint."""
     torch, cb = tb
     sizes = [(64, 3), (128, 2), (256, 2), (512, 3)]
     iters, sw = 12, 5
     data = {L: _hio_inputs(L, B, seed=L) for L, B in sizes}
+    sig = {L: ((3.0 * L / 128, 1.5 * L / 128) if own_sigma else (3.0, 1.5)) for L, _ in sizes}
     buckets, keep = [], []
     for L, B in sizes:
         A, S0, x0 = data[L]
         b = {"side": L, "count": B, "x": dev(torch, x0.ravel()), "A": dev(torch, A.ravel()),
              "S": dev(torch, S0.ravel())}
+        if own_sigma:
+            b["sigma_start"], b["sigma_end"] = sig[L]
         b["estimate"] = torch.empty_like(b["x"])
         buckets.append(b)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
+    assert impl.set_option(cb.OPT_DATA_MODE, 1 if own_sigma else 0)
     assert impl.hio_batched(buckets, iters, beta=0.9, sw_every=sw) and impl.Sync()
     for (L, B), b in zip(sizes, buckets):
         A, S0, x0 = data[L]
         one = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert one.set_option(cb.OPT_DATA_MODE, 1 if own_sigma else 0)
         x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
         est = torch.empty_like(x)
-        assert one.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=sw, estimate=est)
+        assert one.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=sw,
+                                  sigma_start=sig[L][0], sigma_end=sig[L][1], estimate=est)
         assert one.Sync()
         np.testing.assert_array_equal(host(b["x"]), host(x))
         np.testing.assert_array_equal(host(b["S"]), host(S))
