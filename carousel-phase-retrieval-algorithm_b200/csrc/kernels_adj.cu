@@ -27,8 +27,9 @@
 //                        derivatives of the weights:
 //                        d(zf, xf, yf)/da = (-yq cos a, 0, yq sin a),
 //                        d(zf, xf, yf)/dr = (-xq sin a, -yq, -xq cos a).
-// Coordinates and weights are computed in the element type T (float for the
-// float path); the sums over pixels are in double.  Forward and adjoint
+// Coordinates, weights and the per-pixel and per-voxel sums are computed in the
+// element type T (float for the float path); the loss and angle-gradient sums
+// over a slice's pixels are in double.  Forward and adjoint
 // evaluate the same weight expression for each (pixel, voxel) pair, so the
 // gather is the transpose of the sample up to the summation order.
 #include "cpra_internal.h"
@@ -81,10 +82,10 @@ __device__ __forceinline__ double absT(double v) { return fabs(v); }
 // directions (dz1, dx1, dy1) and (dz2, dx2, dy2)
 template <typename T, bool D>
 __device__ __forceinline__ void trilinear(const Cx<T>* __restrict__ V, int64_t M, int64_t N, int64_t L, T zf, T xf,
-                                          T yf, T dz1, T dx1, T dy1, T dz2, T dx2, T dy2, double& re, double& im,
-                                          double& d1r, double& d1i, double& d2r, double& d2i) {
+                                          T yf, T dz1, T dx1, T dy1, T dz2, T dx2, T dy2, T& re, T& im, T& d1r,
+                                          T& d1i, T& d2r, T& d2i) {
     const int64_t z0 = floor_i(zf), x0 = floor_i(xf), y0 = floor_i(yf);
-    re = im = d1r = d1i = d2r = d2i = 0.0;
+    re = im = d1r = d1i = d2r = d2i = T(0);
     for (int cz = 0; cz < 2; ++cz) {
         const int64_t z = z0 + cz;
         const T uz = zf - (T)z;
@@ -104,16 +105,16 @@ __device__ __forceinline__ void trilinear(const Cx<T>* __restrict__ V, int64_t M
                 if (y < 0 || y >= M || !(wy > T(0))) continue;
                 const T sy = uy >= T(0) ? T(-1) : T(1);
                 const Cx<T> v = V[(z * N + x) * M + y];
-                const double w = (double)(wz * wx * wy);
-                re += w * (double)v.x;
-                im += w * (double)v.y;
+                const T w = wz * wx * wy;
+                re += w * v.x;
+                im += w * v.y;
                 if (D) {
-                    const double g1 = (double)(sz * dz1 * wx * wy + wz * sx * dx1 * wy + wz * wx * sy * dy1);
-                    const double g2 = (double)(sz * dz2 * wx * wy + wz * sx * dx2 * wy + wz * wx * sy * dy2);
-                    d1r += g1 * (double)v.x;
-                    d1i += g1 * (double)v.y;
-                    d2r += g2 * (double)v.x;
-                    d2i += g2 * (double)v.y;
+                    const T g1 = sz * dz1 * wx * wy + wz * sx * dx1 * wy + wz * wx * sy * dy1;
+                    const T g2 = sz * dz2 * wx * wy + wz * sx * dx2 * wy + wz * wx * sy * dy2;
+                    d1r += g1 * v.x;
+                    d1i += g1 * v.y;
+                    d2r += g2 * v.x;
+                    d2i += g2 * v.y;
                 }
             }
         }
@@ -130,10 +131,10 @@ __global__ void k_slice(const Cx<T>* __restrict__ V, const Orient<T>* __restrict
         const Orient<T> o = tab[p];
         T zf, xf, yf, xq, yq;
         pixel_point(o, (T)(xIn - N / 2), (T)(M / 2 - yIn), hl, hn, hm, zf, xf, yf, xq, yq);
-        double re, im, a, b, c, d;
+        T re, im, a, b, c, d;
         const T z0 = T(0);
         trilinear<T, false>(V, M, N, L, zf, xf, yf, z0, z0, z0, z0, z0, z0, re, im, a, b, c, d);
-        out[i] = Cx<T>{(T)re, (T)im};
+        out[i] = Cx<T>{re, im};
     }
 }
 
@@ -153,9 +154,11 @@ __global__ void k_slice_residual(const Cx<T>* __restrict__ V, const Orient<T>* _
         const int64_t yIn = (int64_t)(i % M), xIn = (int64_t)(i / M);
         T zf, xf, yf, xq, yq;
         pixel_point(o, (T)(xIn - N / 2), (T)(M / 2 - yIn), hl, hn, hm, zf, xf, yf, xq, yq);
-        double re, im, dar, dai, drr, dri;
-        trilinear<T, true>(V, M, N, L, zf, xf, yf, -yq * o.ca, T(0), yq * o.sa, -xq * o.sa, -yq, -xq * o.ca, re, im,
-                           dar, dai, drr, dri);
+        T ret, imt, dart, dait, drrt, drit;
+        trilinear<T, true>(V, M, N, L, zf, xf, yf, -yq * o.ca, T(0), yq * o.sa, -xq * o.sa, -yq, -xq * o.ca, ret, imt,
+                           dart, dait, drrt, drit);
+        // the per-pixel terms of the loss and angle sums in double (they are summed over the plane)
+        const double re = ret, im = imt, dar = dart, dai = dait, drr = drrt, dri = drit;
         const double mag = sqrt(re * re + im * im);
         const double d = mag - (double)A[p * plane + i];
         accL += d * d;
@@ -208,8 +211,8 @@ __global__ void k_sum3_final(const double* __restrict__ partials, double* __rest
 constexpr double ADJ_SQRT2 = 1.4142135623730951;
 template <typename T>
 __device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const Orient<T>& o, int64_t M, int64_t N,
-                                             T hl, T hn, T hm, T j, T k, T l, int64_t z, int64_t x, int64_t y,
-                                             double& re, double& im) {
+                                             T hl, T hn, T hm, T j, T k, T l, int64_t z, int64_t x, int64_t y, T& re,
+                                             T& im) {
     const T d = j * o.ca - l * o.sa;
     if (!(absT(d) < T(ADJ_SQRT2 + 1e-3))) return;
     const T u = k, v = j * o.sa + l * o.ca;
@@ -229,9 +232,9 @@ __device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const
             const T wz = T(1) - absT(zf - (T)z), wx = T(1) - absT(xf - (T)x), wy = T(1) - absT(yf - (T)y);
             if (!(wz > T(0)) || !(wx > T(0)) || !(wy > T(0))) continue;
             const Cx<T> g = Gp[xIn * M + yIn];
-            const double w = (double)(wz * wx * wy);
-            re += w * (double)g.x;
-            im += w * (double)g.y;
+            const T w = wz * wx * wy;
+            re += w * g.x;
+            im += w * g.y;
         }
     }
 }
@@ -248,10 +251,10 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __re
     for (uint64_t i = tid_g(); i < total; i += str_g()) {
         const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
         const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
-        double re = 0.0, im = 0.0;
+        T re = T(0), im = T(0);
         for (int64_t p = 0; p < P; ++p)
             gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
-        gV[i] = Cx<T>{(T)re, (T)im};
+        gV[i] = Cx<T>{re, im};
     }
 }
 
@@ -268,11 +271,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __
     for (uint64_t i = tid_g(); i < total; i += str_g()) {
         const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
         const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
-        double re = 0.0, im = 0.0;
+        T re = T(0), im = T(0);
         for_slices_near(at, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double, double) {
             gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
         });
-        gV[i] = Cx<T>{(T)re, (T)im};
+        gV[i] = Cx<T>{re, im};
     }
 }
 

@@ -299,20 +299,51 @@ __global__ void k_real2d_to_3d(const T* __restrict__ src, T* __restrict__ dst, c
 // Voxel (z, x, y) is the point (j, k, l) = (L/2 - z, x - N/2, M/2 - y); for
 // slice p at angle a its in-plane coordinates are (yr, xr) = (j sin a + l cos
 // a, k) and its distance to the plane is d = j cos a - l sin a.  Slices with
-// |d| < 1 contribute (1 - |d|) times the slice bilinearly sampled at
+// |d| < 1 contribute (1 - |d|) times the slice linearly sampled at
 // (yIn, xIn) = (M/2 - yr, N/2 + k); the voxel is the weight-normalised sum, or
 // 0 (left unconstrained by the complex DataConstraint) when nothing reaches it.
-// The slices' sines and cosines are staged per block in shared memory,
-// MERGE_ANGLES at a time; a float pre-test |j cos a - l sin a| < 1 + 1e-3
-// (its rounding is below 1e-4 at these coordinates) skips the slices that
-// cannot reach the voxel before the double test, which decides as before.
+// Coordinates, weights and sums are in the element type T, as the
+// reference's merge kernel computes (CUDA_Impl_Kernel.cuh:68-108); the
+// sines and cosines are evaluated once per slice in double and rounded to T.
+template <typename T>
+__device__ __forceinline__ void merge_slice(const Cx<T>* __restrict__ src, int64_t p, int64_t M, int64_t N,
+                                            int64_t x, T j, T l, T sa, T ca, T& accx, T& accy, T& wsum) {
+    const T d = j * ca - l * sa;
+    const T wd = T(1) - (d < T(0) ? -d : d);
+    if (!(wd > T(0))) return;
+    const T yIn = (T)(M / 2) - (j * sa + l * ca);
+    const T y0f = floor(yIn);
+    const int64_t y0 = (int64_t)y0f;
+    const T fy = yIn - y0f;
+    T sx = T(0), sy = T(0), sw = T(0);
+    for (int dy = 0; dy < 2; ++dy) {
+        const int64_t yy = y0 + dy;
+        const T wy = dy ? fy : T(1) - fy;
+        if (yy < 0 || yy >= M || wy == T(0)) continue;
+        const Cx<T> v = src[p * M * N + x * M + yy];
+        sx += wy * v.x;
+        sy += wy * v.y;
+        sw += wy;
+    }
+    if (sw == T(0)) return;
+    accx += wd * sx;
+    accy += wd * sy;
+    wsum += wd * sw;
+}
+
+template <typename T>
+struct SinCos2 {
+    T s, c;
+};
+
+// every slice visited: the slices' sines and cosines staged per block in
+// shared memory, MERGE_ANGLES at a time
 constexpr int MERGE_ANGLES = 512;
 template <typename T>
 __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst,
                                                                 const T* __restrict__ ang, int64_t M, int64_t N,
                                                                 int64_t P, int64_t L) {
-    __shared__ double2 sc[MERGE_ANGLES];
-    __shared__ float2 scf[MERGE_ANGLES];
+    __shared__ SinCos2<T> sc[MERGE_ANGLES];
     const uint64_t total = (uint64_t)M * N * L;
     const uint64_t iters = (total + gstride() - 1) / gstride();  // the same for every thread of the block
     for (uint64_t it = 0, idx = gtid(); it < iters; ++it, idx += gstride()) {
@@ -320,50 +351,20 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d(const Cx<T>* __r
         const int64_t y = live ? (int64_t)(idx % M) : 0;
         const int64_t x = live ? (int64_t)((idx / M) % N) : 0;
         const int64_t z = live ? (int64_t)(idx / ((uint64_t)M * N)) : 0;
-        const double j = (double)(L / 2 - z), l = (double)(M / 2 - y);
-        const float jf = (float)j, lf = (float)l;
-        double accx = 0.0, accy = 0.0, wsum = 0.0;
+        const T j = (T)(L / 2 - z), l = (T)(M / 2 - y);
+        T accx = T(0), accy = T(0), wsum = T(0);
         for (int64_t p0 = 0; p0 < P; p0 += MERGE_ANGLES) {
             const int64_t np = (P - p0 < MERGE_ANGLES) ? P - p0 : MERGE_ANGLES;
             __syncthreads();
             for (int64_t k = threadIdx.x; k < np; k += blockDim.x) {
                 const double a = (double)ang[p0 + k];
-                const double sa = sin(a), ca = cos(a);
-                sc[k] = make_double2(sa, ca);
-                scf[k] = make_float2((float)sa, (float)ca);
+                sc[k] = SinCos2<T>{(T)sin(a), (T)cos(a)};
             }
             __syncthreads();
             if (!live) continue;
-            for (int64_t k = 0; k < np; ++k) {
-                const float2 f = scf[k];
-                if (fabsf(jf * f.y - lf * f.x) >= 1.001f) continue;
-                const double2 w = sc[k];
-                const double sa = w.x, ca = w.y;
-                const int64_t p = p0 + k;
-                const double d = j * ca - l * sa;
-                const double wd = 1.0 - fabs(d);
-                if (!(wd > 0.0)) continue;
-                const double yIn = (double)(M / 2) - (j * sa + l * ca);
-                const double y0f = floor(yIn);
-                const int64_t y0 = (int64_t)y0f;
-                const double fy = yIn - y0f;
-                double sx = 0.0, sy = 0.0, sw = 0.0;
-                for (int dy = 0; dy < 2; ++dy) {
-                    const int64_t yy = y0 + dy;
-                    const double wy = dy ? fy : 1.0 - fy;
-                    if (yy < 0 || yy >= M || wy == 0.0) continue;
-                    const Cx<T> v = src[p * M * N + x * M + yy];
-                    sx += wy * (double)v.x;
-                    sy += wy * (double)v.y;
-                    sw += wy;
-                }
-                if (sw == 0.0) continue;
-                accx += wd * sx;
-                accy += wd * sy;
-                wsum += wd * sw;
-            }
+            for (int64_t k = 0; k < np; ++k) merge_slice(src, p0 + k, M, N, x, j, l, sc[k].s, sc[k].c, accx, accy, wsum);
         }
-        if (live) dst[idx] = (wsum > 0.0) ? Cx<T>{(T)(accx / wsum), (T)(accy / wsum)} : Cx<T>{T(0), T(0)};
+        if (live) dst[idx] = (wsum > T(0)) ? Cx<T>{accx / wsum, accy / wsum} : Cx<T>{T(0), T(0)};
     }
 }
 
@@ -378,32 +379,12 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d_w(const Cx<T>* _
         const int64_t y = (int64_t)(idx % M);
         const int64_t x = (int64_t)((idx / M) % N);
         const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
-        const double j = (double)(L / 2 - z), l = (double)(M / 2 - y);
-        double accx = 0.0, accy = 0.0, wsum = 0.0;
-        for_slices_near(tab, j, l, [&](int64_t p, double sa, double ca) {
-            const double d = j * ca - l * sa;
-            const double wd = 1.0 - fabs(d);
-            if (!(wd > 0.0)) return;
-            const double yIn = (double)(M / 2) - (j * sa + l * ca);
-            const double y0f = floor(yIn);
-            const int64_t y0 = (int64_t)y0f;
-            const double fy = yIn - y0f;
-            double sx = 0.0, sy = 0.0, sw = 0.0;
-            for (int dy = 0; dy < 2; ++dy) {
-                const int64_t yy = y0 + dy;
-                const double wy = dy ? fy : 1.0 - fy;
-                if (yy < 0 || yy >= M || wy == 0.0) continue;
-                const Cx<T> v = src[p * M * N + x * M + yy];
-                sx += wy * (double)v.x;
-                sy += wy * (double)v.y;
-                sw += wy;
-            }
-            if (sw == 0.0) return;
-            accx += wd * sx;
-            accy += wd * sy;
-            wsum += wd * sw;
+        const T j = (T)(L / 2 - z), l = (T)(M / 2 - y);
+        T accx = T(0), accy = T(0), wsum = T(0);
+        for_slices_near(tab, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double sa, double ca) {
+            merge_slice(src, p, M, N, x, j, l, (T)sa, (T)ca, accx, accy, wsum);
         });
-        dst[idx] = (wsum > 0.0) ? Cx<T>{(T)(accx / wsum), (T)(accy / wsum)} : Cx<T>{T(0), T(0)};
+        dst[idx] = (wsum > T(0)) ? Cx<T>{accx / wsum, accy / wsum} : Cx<T>{T(0), T(0)};
     }
 }
 

@@ -663,12 +663,15 @@ def test_rfactor_vs_oracle(tb, L, B, shared):
     np.testing.assert_array_equal(host(xd), x)   # input untouched
 
 
-def test_complex_merge_vs_oracle(tb):
-    """Project-defined trilinear gather merge (Complex2DTo3DInterpolation)."""
+@pytest.mark.parametrize("M,P,tol", [(24, 10, 1e-5), (64, 40, 1e-4)])
+def test_complex_merge_vs_oracle(tb, M, P, tol):
+    """Project-defined trilinear gather merge (Complex2DTo3DInterpolation)
+    against the float64 oracle.  Coordinates and weights are float: their
+    rounding (about M/2 * 2^-23 absolute) bounds the relative L2 error at
+    1e-5 for 24^3 and 1e-4 for 64^3."""
     torch, cb = tb
     rng = np.random.default_rng(21)
-    M = N = L = 24
-    P = 10
+    N = L = M
     src = (rng.standard_normal(P * M * N) + 1j * rng.standard_normal(P * M * N)).astype(np.complex64)
     ang = np.deg2rad(np.linspace(0, 170, P) + 0.37).astype(np.float32)
     want = O.complex2d_to_3d(np.float32, src, ang, M, N, P, L)
@@ -676,7 +679,7 @@ def test_complex_merge_vs_oracle(tb):
     dst = torch.zeros(M * N * L, dtype=torch.complex64, device="cuda")
     assert impl.Complex2DTo3DInterpolation(dev(torch, src), dst, dev(torch, ang), M, N, P, L) and impl.Sync()
     got = host(dst)
-    assert O.rel_l2(got, want) < 1e-6
+    assert O.rel_l2(got, want) < tol
     assert (np.abs(want) > 0).mean() > 0.3
 
 
