@@ -116,29 +116,32 @@ __device__ __forceinline__ int64_t angle_lower_bound(const double* key, int64_t 
 }
 
 // f(p, sin a_p, cos a_p) for the slices that can reach the voxel at (cz, cy)
-// (cz = L/2 - z, cy = M/2 - y), in ascending direction order
+// (cz = L/2 - z, cy = M/2 - y), in ascending direction order.  The window
+// only prunes (the caller's weights decide), so it is computed in float and
+// widened by 1e-4 rad, far above the float rounding of its bounds.
 template <class Fn>
 __device__ __forceinline__ void for_slices_near(const AngleTable& t, double cz, double cy, Fn f) {
-    const double rho = sqrt(cz * cz + cy * cy);
+    const float czf = (float)cz, cyf = (float)cy;
+    const float rho = sqrtf(czf * czf + cyf * cyf);
     auto range = [&](double a, double b) {
         for (int64_t k = angle_lower_bound(t.key, t.P, a); k < t.P && t.key[k] <= b; ++k) {
             const double2 w = t.sc[k];
             f((int64_t)t.idx[k], w.x, w.y);
         }
     };
-    if (!(rho > 1.5)) {
+    if (!(rho > 1.51f)) {
         range(-1.0, 4.0);
         return;
     }
-    const double delta0 = asin(1.5 / rho);
-    if (delta0 >= 0.5 * ANGLE_PI - 1e-6) {  // the two windows would meet
+    const double delta0 = (double)asinf(1.5f / rho);
+    if (delta0 >= 0.5 * ANGLE_PI - 1e-3) {  // the two windows would meet
         range(-1.0, 4.0);
         return;
     }
-    double phi = atan2(cz, cy);
+    double phi = (double)atan2f(czf, cyf);
     if (phi < 0.0) phi += ANGLE_PI;
     if (phi >= ANGLE_PI) phi -= ANGLE_PI;
-    const double delta = delta0 + 1e-9;
+    const double delta = delta0 + 1e-4;
     const double lo = phi - delta, hi = phi + delta;
     if (lo < 0.0) {
         range(-1.0, hi);
