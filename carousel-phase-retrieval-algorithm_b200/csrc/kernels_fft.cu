@@ -224,6 +224,10 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
     auto gindex = [&](int n) -> uint64_t {
         return contig ? (o0 + line) * (uint64_t)L + n : (o0 * L + n) * Bi + i0 + line;
     };
+    // the constraint's index gi % aux_plane; the arrays of one volume never
+    // wrap, and the 64-bit remainder per element is then skipped
+    const bool aux_wraps = Bo * (uint64_t)L * Bi > op.aux_plane;
+    auto aux_index = [&](uint64_t gi) -> uint64_t { return aux_wraps ? gi % op.aux_plane : gi; };
     Cx<T>* lb = buf + slot(line, 0);  // this line's slots, stride ss
     Cx<T> v[R];
 #pragma unroll
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         if constexpr (!PLAIN) {
             if (op.kind == AXIS_T2_PROLOGUE && line_ok) {
                 const uint64_t gi = gindex(n);
-                const T sv = static_cast<const T*>(op.aux)[gi % op.aux_plane];
+                const T sv = static_cast<const T*>(op.aux)[aux_index(gi)];
                 v[k] = merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], space_apply(v[k], sv, op.space_mode),
                                    (T)op.a, (T)op.b);
             }
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
                 Cx<T> w = o[i];
                 if (shift) w = csign(w, f + out_neg);
                 if (line_ok) {
-                    const uint64_t ai = gindex(f) % op.aux_plane;
+                    const uint64_t ai = aux_index(gindex(f));
                     w = (op.kind == AXIS_DC_ROUNDTRIP)
                             ? data_apply_complex(w, static_cast<const Cx<T>*>(op.aux)[ai])
                             : data_apply(w, static_cast<const T*>(op.aux)[ai], op.data_mode);
@@ -276,11 +280,11 @@ __global__ void __launch_bounds__(AXIS_THREADS) k_axis_fft(Cx<T>* __restrict__ d
         if constexpr (!PLAIN) {
             if (line_ok) {
                 if (op.kind == AXIS_SPACE) {
-                    w = space_apply(w, static_cast<const T*>(op.aux)[gindex(f) % op.aux_plane], op.space_mode);
+                    w = space_apply(w, static_cast<const T*>(op.aux)[aux_index(gindex(f))], op.space_mode);
                 } else if (op.kind == AXIS_T1_EPILOGUE) {
                     const uint64_t gi = gindex(f);
                     w = space_apply(merge_apply(static_cast<const Cx<T>*>(op.x_in)[gi], w, (T)op.a, (T)op.b),
-                                    static_cast<const T*>(op.aux)[gi % op.aux_plane], op.space_mode);
+                                    static_cast<const T*>(op.aux)[aux_index(gi)], op.space_mode);
                 } else if (op.kind == AXIS_X_EPILOGUE) {
                     const uint64_t gi = gindex(f);
                     Cx<T>* X = static_cast<Cx<T>*>(op.x_in);
