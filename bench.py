@@ -48,9 +48,10 @@ def parse():
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the per-op and 3D side measurements")
-    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d", "plain2d"], default="carousel",
+    ap.add_argument("--case", choices=["carousel", "uneven", "carousel3d", "fft3d", "plain2d", "ops2d", "ops3d"],
+                    default="carousel",
                     help="uneven / carousel3d / fft3d / plain2d: only that side measurement (one JSON line, for "
-                         "profiling runs)")
+                         "profiling runs); ops2d / ops3d: one launch of each kernel family (for ncu captures)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
     # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
@@ -339,6 +340,11 @@ def main():
         return
     if a.case == "plain2d":
         out = plain2d(torch, cpra_b200, torch.device("cuda", local), reps=max(1, a.steps))
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
+    if a.case in ("ops2d", "ops3d"):
+        out = kernel_families(torch, cpra_b200, torch.device("cuda", local), a.case)
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -900,6 +906,82 @@ def plain2d(torch, cpra_b200, dev, B=16, n=128, iters=200, sw_every=20, reps=3):
 
 UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns): 512 patterns, 18,612,224 pixels
 HIO_BYTES_PER_PIXEL = 24  # read+write x (complex64) + read A, S (float32) per HIO pattern-iteration
+
+
+def kernel_families(torch, cpra_b200, dev, case):
+    """One launch of each kernel family on inputs larger than L2, for ncu
+    captures (no timing here).  ops2d: the per-operator 2D kernels on 2000
+    planes of 128^2 (262 MB per complex array): Forward2D, Backward2D,
+    SpaceConstraint, DataConstraint (real and complex), MergeAddData,
+    Normalization, FFTShift2D, ConvergeError.  ops3d at 256^3 with 180 slices:
+    the trilinear merge, the slice operator's loss, gradients and adjoint, the
+    slice operator, one real-space refinement step (transform, slice, adjoints,
+    transform adjoint, Adam), Forward3D, the benchmark's 3D step on the
+    operator kernels and as fused passes, one fused 3D difference-map
+    iteration; and the real merge (Real2DTo3DInterpolation) at 128^3 from 90
+    slices."""
+    g = torch.Generator(device=dev).manual_seed(1)
+    n0 = cpra_b200.kernels_launched()
+    if case == "ops2d":
+        n, B = 128, 2000
+        num = B * n * n
+        impl = cpra_b200.B200Impl(n, n, 1, B)
+        impl.set_option(cpra_b200.OPT_FUSION, 0)
+        x = torch.rand(num, dtype=torch.complex64, device=dev, generator=g)
+        y = torch.rand(num, dtype=torch.complex64, device=dev, generator=g)
+        A = torch.rand(n * n, device=dev, generator=g) * 10
+        S = (torch.rand(n * n, device=dev, generator=g) > 0.5).float()
+        C = torch.rand(n * n, dtype=torch.complex64, device=dev, generator=g)
+        impl.Forward2D(x)
+        impl.Backward2D(x)
+        impl.SpaceConstraint(x, S, num, B)
+        impl.DataConstraint(x, A, num, B)
+        impl.DataConstraintComplex(x, C, num, B)
+        impl.MergeAddData(y, x, 0.5, 0.5, num)
+        impl.Normalization(x, 3.0, num)
+        impl.FFTShift2D(x, n, n, B)
+        impl.ConvergeError(x, y, np.zeros(B, np.float32), n, n, 1, B)
+        impl.Sync()
+        impl.close()
+    else:
+        n, P = 256, 180
+        vox = n ** 3
+        impl3 = cpra_b200.B200Impl(n, n, n, 1)
+        impl3.set_option(cpra_b200.OPT_FUSION, 0)
+        ang = torch.deg2rad(torch.arange(P, device=dev, dtype=torch.float32))
+        rot = torch.zeros(P, device=dev)
+        src = torch.rand(P * n * n, dtype=torch.complex64, device=dev, generator=g)
+        V = torch.zeros(vox, dtype=torch.complex64, device=dev)
+        impl3.Complex2DTo3DInterpolation(src, V, ang, n, n, P, n)
+        A = torch.rand(P * n * n, device=dev, generator=g) * 5
+        gV = torch.zeros_like(V)
+        impl3.slice_loss_grad_orient(V, ang, rot, A, n, n, P, n, gV)
+        out = torch.empty(P * n * n, dtype=torch.complex64, device=dev)
+        impl3.slice_orient(V, ang, rot, n, n, P, n, out)
+        vol = torch.rand(vox, device=dev, generator=g)
+        impl3.refine_orient(vol, ang, rot, A, n, n, P, n, 1, real_space=True, lr_volume=1e-3, lr_angle=1e-4,
+                            lr_rot=1e-4)
+        x = torch.rand(vox, dtype=torch.complex64, device=dev, generator=g)
+        S3 = (torch.rand(vox, device=dev, generator=g) > 0.5).float()
+        impl3.Forward3D(x)
+        impl3.constraint3d(x, V, S3, 1)
+        impl3.set_option(cpra_b200.OPT_FUSED3D, 1)
+        impl3.set_option(cpra_b200.OPT_FUSION, 1)
+        impl3.constraint3d(x, V, S3, 1)
+        A3 = torch.rand(vox, device=dev, generator=g) * 10
+        impl3.conv_run(x, A3, S3, 1, 0.9, final_step=False)
+        impl3.Sync()
+        impl3.close()
+        m = 128
+        impl1 = cpra_b200.B200Impl(m, m, m, 1)
+        rs = torch.rand(90 * m * m, device=dev, generator=g)
+        rv = torch.zeros(m ** 3, device=dev)
+        impl1.Real2DTo3DInterpolation(rs, rv, torch.deg2rad(torch.arange(90, device=dev, dtype=torch.float32) * 2),
+                                      m, m, 90, m)
+        impl1.Sync()
+        impl1.close()
+    return {"case": case, "gpu_launches": int(cpra_b200.kernels_launched() - n0),
+            "note": "one launch of each kernel family, for ncu captures; not a timing"}
 
 
 def fft3d_ops(torch, cpra_b200, dev, n=128, reps=5):

@@ -851,27 +851,89 @@ static int run_fft3d(cpra_b200_ctx* c, void* x, bool inverse) {
     return submit(c, Op{inverse ? OpKind::Bwd3D : OpKind::Fwd3D, x, nullptr, 0, 0, 0, 0});
 }
 
-int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void* S, int iters) {
-    CTX_OR_RETURN(c);
-    if (!x || !C || !S) return fail(CPRA_B200_EARG, "constraint3d: null pointer");
-    if (iters < 0) return fail(CPRA_B200_EARG, "constraint3d: iters must be >= 0");
-    if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
-        return fail(CPRA_B200_EUNSUP, "constraint3d: each size must be 1 or even and at most 4096");
-    int r = flush(c);
-    if (r) return take_deferred(c);
+namespace {
+
+// CPRA_B200_OPT_AUTOTUNE for choices that leave the results unchanged: the
+// cached choice of `key`, or, for a new key, a measurement: each candidate
+// runs once untimed and once timed, prepare() restoring the trial inputs
+// before each run and run(k) enqueuing candidate k; the fastest is cached.
+int tuned_choice(cpra_b200_ctx* c, const std::string& key, const std::vector<uint64_t>& cand,
+                 const std::function<int()>& prepare, const std::function<int(uint64_t)>& run, uint64_t* out) {
+    for (const auto& e : c->tune_cache)
+        if (e.first == key) {
+            *out = (uint64_t)e.second;
+            return CPRA_B200_OK;
+        }
+    struct Events {
+        cudaEvent_t e[2] = {nullptr, nullptr};
+        ~Events() {
+            for (cudaEvent_t v : e)
+                if (v) cudaEventDestroy(v);
+        }
+    } ev;
+    CPRA_CHECK_CUDA(cudaEventCreate(&ev.e[0]), "cudaEventCreate");
+    CPRA_CHECK_CUDA(cudaEventCreate(&ev.e[1]), "cudaEventCreate");
+    std::vector<float> ms(cand.size(), 0.0f);
+    for (int pass = 0; pass < 2; ++pass) {
+        for (size_t k = 0; k < cand.size(); ++k) {
+            int r = prepare();
+            if (r) return r;
+            CPRA_CHECK_CUDA(cudaEventRecord(ev.e[0], c->stream), "autotune");
+            r = run(cand[k]);
+            if (r) return r;
+            CPRA_CHECK_CUDA(cudaEventRecord(ev.e[1], c->stream), "autotune");
+            CPRA_CHECK_CUDA(cudaEventSynchronize(ev.e[1]), "autotune");
+            CPRA_CHECK_CUDA(cudaEventElapsedTime(&ms[k], ev.e[0], ev.e[1]), "autotune");
+        }
+    }
+    size_t best = 0;
+    for (size_t k = 1; k < cand.size(); ++k)
+        if (ms[k] < ms[best]) best = k;
+    c->tune_cache.emplace_back(key, (int)cand[best]);
+    *out = cand[best];
+    return CPRA_B200_OK;
+}
+
+// a stream capture is under way on the context's stream (ours or the caller's)
+bool stream_capturing(cpra_b200_ctx* c) {
+    if (c->capturing) return true;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(c->stream, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone;
+}
+
+// a device buffer for the duration of a measurement (freed on scope exit)
+struct TrialBuffer {
+    cpra_b200_ctx* c;
+    void* p = nullptr;
+    explicit TrialBuffer(cpra_b200_ctx* ctx) : c(ctx) {}
+    bool alloc(uint64_t bytes) {
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();  // out of memory is not sticky
+            p = nullptr;
+            return false;
+        }
+        return true;
+    }
+    ~TrialBuffer() {
+        if (p) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(p);
+        }
+    }
+};
+
+// `iters` repetitions of the benchmark's 3D step, as fused axis passes or as
+// the four operator kernels (the same bits)
+int constraint3d_path(cpra_b200_ctx* c, void* x, const void* C, const void* S, int iters, bool fused, double scale) {
     const uint64_t vol = c->m * c->n * c->l, num = vol * c->batch;
-    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
-    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
-    if (c->fused3d && constraint3d_fused_supported(c->m, c->n, c->l)) {
+    if (fused) {
         CPRA_CHECK_CUDA(launch_constraint3d(c->dbl, x, C, S, c->m, c->n, c->l, c->batch, iters, c->space_mode, scale,
                                             twiddles(c, c->m), twiddles(c, c->n), twiddles(c, c->l), c->work,
                                             c->stream),
                         "constraint3d");
         return CPRA_B200_OK;
     }
-    // the four operators in turn (by default: faster on B200 than the fused
-    // passes at 64^3 to 256^3, same bits)
-    r = ensure_work(c, num * c->csize());
+    int r = ensure_work(c, num * c->csize());
     if (r) return r;
     for (int it = 0; it < iters; ++it) {
         CPRA_CHECK_CUDA(launch_fft3d(c->dbl, x, c->m, c->n, c->l, c->batch, false, scale, twiddles(c, c->m),
@@ -884,6 +946,45 @@ int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void*
         CPRA_CHECK_CUDA(launch_space_constraint(c->dbl, x, S, num, vol, c->space_mode, c->stream), "constraint3d");
     }
     return CPRA_B200_OK;
+}
+
+}  // namespace
+
+int cpra_b200_constraint3d(cpra_b200_ctx* c, void* x, const void* C, const void* S, int iters) {
+    CTX_OR_RETURN(c);
+    if (!x || !C || !S) return fail(CPRA_B200_EARG, "constraint3d: null pointer");
+    if (iters < 0) return fail(CPRA_B200_EARG, "constraint3d: iters must be >= 0");
+    if (!fft_length_supported(c->m) || !fft_length_supported(c->n) || !fft_length_supported(c->l))
+        return fail(CPRA_B200_EUNSUP, "constraint3d: each size must be 1 or even and at most 4096");
+    int r = flush(c);
+    if (r) return take_deferred(c);
+    const uint64_t vol = c->m * c->n * c->l, num = vol * c->batch;
+    // DFTI_BACKWARD_SCALE = (T)1.0 / (m*n*l) (include/MKL_Impl.hpp:62)
+    const double scale = c->dbl ? 1.0 / (double)vol : (double)(1.0f / (float)vol);
+    const bool can_fuse = constraint3d_fused_supported(c->m, c->n, c->l);
+    bool fused = c->fused3d && can_fuse;
+    // CPRA_B200_OPT_AUTOTUNE: the faster of the two paths, measured once per
+    // shape on a copy of x (one iteration each)
+    if (c->autotune && can_fuse && iters > 0 && !stream_capturing(c)) {
+        TrialBuffer trial(c);
+        if (trial.alloc(num * c->csize())) {
+            const std::string key = "constraint3d:" + std::to_string(c->m) + "," + std::to_string(c->n) + "," +
+                                    std::to_string(c->l) + "," + std::to_string(c->batch) + "," +
+                                    std::to_string(c->dbl) + "," + std::to_string(c->space_mode);
+            uint64_t choice = fused ? 1 : 0;
+            r = tuned_choice(
+                c, key, {0, 1},
+                [&]() -> int {
+                    CPRA_CHECK_CUDA(cudaMemcpyAsync(trial.p, x, num * c->csize(), cudaMemcpyDeviceToDevice, c->stream),
+                                    "autotune");
+                    return CPRA_B200_OK;
+                },
+                [&](uint64_t k) { return constraint3d_path(c, trial.p, C, S, 1, k != 0, scale); }, &choice);
+            if (r) return r;
+            fused = choice != 0;
+        }
+    }
+    return constraint3d_path(c, x, C, S, iters, fused, scale);
 }
 
 int cpra_b200_forward3d(cpra_b200_ctx* c, void* x) {
@@ -1294,7 +1395,46 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
     r = flush(c);
     if (r) return take_deferred(c);
     if (iters == 0 && !estimate) return CPRA_B200_OK;
-    const uint64_t chunk = (c->hio_chunk == 0) ? batch : std::min(c->hio_chunk, batch);
+    uint64_t chunk = (c->hio_chunk == 0) ? batch : std::min(c->hio_chunk, batch);
+    // CPRA_B200_OPT_AUTOTUNE (chunk 0 only): the line passes' chunk measured
+    // once per (side, batch) among the whole batch, a half and a quarter, on
+    // copies of x and S, min(iters, 20) iterations each (the chunk changes
+    // the schedule only)
+    if (c->autotune && c->hio_chunk == 0 && !hio_fused_supported(c->dbl, c->m, c->n) && batch > 1 && iters > 0 &&
+        !stream_capturing(c)) {
+        const uint64_t plane = c->plane();
+        const uint64_t xb = batch * plane * c->csize();
+        // S too: the passes write the support back (packed at the start, unpacked at the end)
+        const uint64_t sb = (s_stride ? batch * s_stride : plane) * c->esize();
+        TrialBuffer trial(c);
+        r = ensure_work(c, hio_scratch_bytes(c->dbl, c->m, batch));
+        if (r) return r;
+        if (trial.alloc(xb + sb + 256)) {
+            void* tx = trial.p;
+            void* tS = static_cast<char*>(trial.p) + (xb + 255) / 256 * 256;
+            std::vector<uint64_t> cand;
+            for (uint64_t k : {batch, (batch + 1) / 2, (batch + 3) / 4})
+                if (std::find(cand.begin(), cand.end(), k) == cand.end()) cand.push_back(k);
+            HioParams ht = h;
+            ht.iters = std::min(iters, 20);
+            const std::string key = "hio_chunk:" + std::to_string(c->m) + "," + std::to_string(batch) + "," +
+                                    std::to_string(ht.iters) + "," + std::to_string(sw_every) + "," +
+                                    std::to_string(c->data_mode);
+            r = tuned_choice(
+                c, key, cand,
+                [&]() -> int {
+                    CPRA_CHECK_CUDA(cudaMemcpyAsync(tx, x, xb, cudaMemcpyDeviceToDevice, c->stream), "autotune");
+                    CPRA_CHECK_CUDA(cudaMemcpyAsync(tS, S, sb, cudaMemcpyDeviceToDevice, c->stream), "autotune");
+                    return CPRA_B200_OK;
+                },
+                [&](uint64_t k) {
+                    return hio_enqueue(c, HioJob{c->m, batch, tx, A, a_stride, tS, s_stride, nullptr}, ht, k, c->work,
+                                       c->stream);
+                },
+                &chunk);
+            if (r) return r;
+        }
+    }
     r = ensure_work(c, hio_scratch_bytes(c->dbl, c->m, chunk));
     if (r) return r;
     return hio_enqueue(c, HioJob{c->m, batch, x, A, a_stride, S, s_stride, estimate}, h, chunk, c->work, c->stream);

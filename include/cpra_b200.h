@@ -76,7 +76,14 @@ extern "C" {
                                     fastest in the context's cache; later runs of that key use it, host-buffer
                                     runs only once it is cached.  No tuning during a stream capture or for
                                     epi < 2; if the copy cannot be allocated the key keeps the automatic
-                                    choice.  0 (default): the automatic choice.  Same results either way. */
+                                    choice.  0 (default): the automatic choice.  Same results either way.
+                                    The same option also measures, once per shape and on copies of the
+                                    inputs: for cpra_b200_constraint3d, fused axis passes against the
+                                    operator kernels (one iteration each; CPRA_B200_OPT_FUSED3D is then
+                                    ignored there); for cpra_b200_hio_shrinkwrap at 256 and 512 with
+                                    CPRA_B200_OPT_HIO_CHUNK 0, the line passes' chunk among the whole batch,
+                                    a half and a quarter (min(iters, 20) iterations each).  No measurement
+                                    during a stream capture or when the copy cannot be allocated. */
 #define CPRA_B200_OPT_FUSED3D 12   /* 1: cpra_b200_constraint3d and the recognised 3D difference-map iteration
                                     run as fused axis passes (5 and 10 passes per iteration); 0 (default):
                                     as the operator kernels, measured faster on B200 (64^3 to 256^3).  Same

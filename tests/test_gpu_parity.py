@@ -1177,3 +1177,45 @@ def test_dm3d_recorder_equals_per_call(tb, T, M, N, L, B, iters):
     tol = (FP32_DM_TOL if T == np.float32 else 1e-12) * iters
     for got, want in zip(outs[1], (xo, t1o, t2o)):
         assert O.rel_l2(got, want) < tol
+
+
+# ---- the autotuner's other choices: the path of the 3D step and the HIO chunk ------------------
+def test_autotune_constraint3d_and_hio_chunk_bitwise(tb):
+    """With CPRA_B200_OPT_AUTOTUNE the 3D step measures its two paths and the
+    256^2 HIO passes their chunk (on copies of the inputs, once per shape);
+    whatever each picks, the results equal those of every candidate, on the
+    measuring call and on the cached one."""
+    torch, cb = tb
+    rng = np.random.default_rng(77)
+    n = 32
+    vol = n ** 3
+    x0 = (rng.standard_normal(vol) + 1j * rng.standard_normal(vol)).astype(np.complex64)
+    C = (rng.standard_normal(vol) + 1j * rng.standard_normal(vol)).astype(np.complex64)
+    C[rng.uniform(size=vol) < 0.3] = 0
+    S = (rng.uniform(size=vol) > 0.4).astype(np.float32)
+    outs = []
+    for tune, fused3d in ((0, 0), (0, 1), (1, 0), (1, 1)):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, n, n, n, 1)
+        assert impl.set_option(cb.OPT_AUTOTUNE, tune) and impl.set_option(cb.OPT_FUSED3D, fused3d)
+        for _ in range(2):   # the first tuned call measures, the second uses the cache
+            x = dev(torch, x0)
+            assert impl.constraint3d(x, dev(torch, C), dev(torch, S), 3) and impl.Sync()
+            outs.append(host(x))
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o, outs[0])
+
+    L, B, iters, sw = 256, 4, 12, 5
+    A, S0, x0 = _hio_inputs(L, B, seed=5)
+    res = []
+    for tune, chunk in ((0, 4), (0, 2), (0, 1), (1, 0)):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert impl.set_option(cb.OPT_AUTOTUNE, tune) and impl.set_option(cb.OPT_HIO_CHUNK, chunk)
+        for _ in range(2 if tune else 1):
+            x, Sd = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+            est = torch.empty_like(x)
+            assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), Sd, B, iters, beta=0.9, sw_every=sw, estimate=est)
+            assert impl.Sync()
+            res.append((host(x), host(Sd), host(est)))
+    for r in res[1:]:
+        for a, b in zip(r, res[0]):
+            np.testing.assert_array_equal(a, b)
