@@ -466,10 +466,11 @@ def main():
         avg_s = kms / klaunches / 1e3
         alg_bytes = DM_BYTES_PER_PIXEL * MN * kpi / klaunches
         achieved = alg_bytes / avg_s / 1e9
-        tr = read_traffic(f"k_dm_{M}")
+        tr = read_traffic(f"k_dm_{M}")  # profiles/ncu_traffic.txt (the 128x128 kernel's capture)
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (tr * kpi / klaunches) if tr is not None else None,
-                "kernel": f"k_dm<{M}> (fused difference-map iterations)",
+                "kernel": (f"k_dm_tm (fused difference-map iterations, {M}x{M}, iterates in tensor memory)"
+                           if M == 128 else f"k_dm<{M}> (fused difference-map iterations)"),
                 "avg_launch_ms": kms / klaunches, "launches": klaunches,
                 "algorithmic_bytes_per_launch": alg_bytes, "peak_kind": f"{peak_kind} hbm_gbs",
                 "share_of_step": kms / ms}
