@@ -61,6 +61,15 @@ __host__ __device__ __forceinline__ constexpr double tw32_cos<double>(int k) { r
 template <>
 __host__ __device__ __forceinline__ constexpr double tw32_sin<double>(int k) { return tw32_sin_d(k); }
 
+// The block index as a fresh read of %ctaid.x, not folded with earlier reads:
+// lets a kernel recompute an address late instead of keeping it in a register
+// through a long loop.
+__device__ __forceinline__ unsigned cta_index() {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(v));
+    return v;
+}
+
 // Number of SMs of the current device, cached per device by the host code.
 int sm_count();
 

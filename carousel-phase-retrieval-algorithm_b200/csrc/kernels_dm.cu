@@ -266,13 +266,6 @@ __global__ void __launch_bounds__(DmP<L>::NT, (L == 64) ? 2 : 1) k_dm(const DmDe
     }
 }
 
-// The block index as a fresh read of %ctaid.x (not folded with earlier reads).
-__device__ __forceinline__ unsigned cta_index() {
-    unsigned v;
-    asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(v));
-    return v;
-}
-
 // The 128 x 128 kernel with its iterates resident in tensor memory.
 //
 // Every thread reads and writes x, t1 and t2 only at its own row's split

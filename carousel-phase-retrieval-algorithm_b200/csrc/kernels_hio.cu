@@ -25,6 +25,7 @@
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
+#include "tmem.cuh"
 
 namespace cpra_b200 {
 
@@ -57,6 +58,16 @@ struct HioPlan {
 };
 
 // column forward transform, a per-frequency operation, column inverse transform
+template <class P, class Op>
+__device__ __forceinline__ void spectral_columns_t(Cx<float>* buf, const Cx<float>* tw, int c, int q, Op op) {
+    Cx<float> o[P::J][P::TPL];
+    P::template col_from_buf<false>(o, buf, tw, c, q);
+#pragma unroll
+    for (int j = 0; j < P::J; ++j)
+#pragma unroll
+        for (int s = 0; s < P::TPL; ++s) o[j][s] = op(o[j][s], P::split_pos(q, j, s), c);
+    P::template col_to_buf<true>(o, buf, tw, c, q);
+}
 template <int L, class Op>
 __device__ __forceinline__ void spectral_columns(Cx<float>* buf, const Cx<float>* tw, int c, int q, Op op) {
     using P = Plane<float, L>;
@@ -218,6 +229,191 @@ __global__ void __launch_bounds__(4 * L, (L == 64) ? 3 : 1) k_hio(const HioDev p
         }
 }
 
+// The 128 x 128 kernel with x in tensor memory and 8 threads per line.
+//
+// A thread reads and writes x only at its own row's 16 split positions, and
+// the support only at the same pixels, so both are thread-private: x lives in
+// the SM's tensor memory for the whole launch (warp w's threads own lane
+// 32*(w % 4) + lane id, columns (w / 4)*32 .. +31, element (j, s) at
+// 2*(8j + s)), the support of the thread's 16 pixels in one register of bits.
+// Registers then hold only the 16 transform values, the CTA runs 1024 threads
+// (32 warps per SM), and global memory is touched when the launch starts (x,
+// A, S) and after the last iteration (x, S, the estimate).  The shrinkwrap
+// blur reads x back from tensor memory.  The transforms split each line over
+// 8 threads as the float 128 x 128 plane kernels do (plane_tpl); the
+// iteration is k_hio's.
+template <int DMODE, bool POS>
+__global__ void __launch_bounds__(1024, 1) k_hio_tm(const HioDev p) {
+    constexpr int L = 128;
+    using P = Plane<float, L, plane_tpl<float, L>()>;
+    constexpr int J = P::J, TPL = P::TPL, AP = L + 4, WARPS = P::NT / 32;
+    static_assert(TPL == 8 && J == 2 && P::NT == 1024, "two 8-value groups per thread, 32 warps");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t tm_base;
+    Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem_raw);
+    float* As = reinterpret_cast<float*>(smem_raw + P::buf_bytes());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + P::buf_bytes() + sizeof(float) * L * AP);
+    float* gt = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(tw) + P::tw_bytes());
+    float* red = gt + L;
+    const int t = threadIdx.x, row = P::row_of(t), col = P::col_of(t), q = P::rank_of(t), warp = t >> 5;
+    if (warp == 0) tm_alloc(&tm_base, 256);
+    P::F::fill_twiddles(tw, p.tw, t, P::NT);
+    Cx<float>* __restrict__ X = p.x + (size_t)blockIdx.x * L * L;
+    const float* __restrict__ A = p.A + blockIdx.x * p.a_stride;
+    float* __restrict__ S = p.S + blockIdx.x * p.s_stride;
+    for (int i = t; i < L * L; i += P::NT) As[(i / L) * AP + (i % L)] = A[i];
+    auto at = [&](int j, int s) { return row * L + P::split_pos(q, j, s); };
+    const bool neg = ((row + q) & 1) != 0;
+    auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
+    // the support of this thread's pixels: bit 8j + s
+    uint32_t in_bits = 0;
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) in_bits |= (S[at(j, s)] > 0.5f ? 1u : 0u) << (TPL * j + s);
+    auto inside = [&](int j, int s) { return (in_bits >> (TPL * j + s)) & 1u; };
+    tm_fence_before_sync();
+    __syncthreads();
+    tm_fence_after_sync();
+    const uint32_t xa = tm_lane_addr(tm_base, warp, (warp >> 2) * 32);
+    Cx<float> o[J][TPL];
+    // x into tensor memory (group g = 2j + h: elements s in [4h, 4h + 4))
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            Cx<float> xs[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                xs[u] = X[at(j, 4 * h + u)];
+                o[j][4 * h + u] = xs[u];
+            }
+            tm_st4(xa + 8 * (2 * j + h), xs);
+        }
+    int update = 0;
+    for (int it = 0; it < p.iters; ++it) {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(o[j][s]);
+        P::template rows_split_to_buf<false>(o, buf, tw, row, q);
+        __syncthreads();
+        spectral_columns_t<P>(buf, tw, col, q, [&](Cx<float> z, int f, int c) {
+            return data_apply(z, As[f * AP + c], DMODE);
+        });
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, row, q);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                Cx<float> xr[4];
+                tm_ld4(xa + 8 * (2 * j + h), xr);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int s = 4 * h + u;
+                    const Cx<float> y = sgn(cscale(o[j][s], p.scale));
+                    const bool keep = inside(j, s) && (!POS || y.x >= 0.0f);
+                    xr[u] = keep ? y : merge_apply(y, xr[u], -p.beta, 1.0f);
+                    o[j][s] = xr[u];
+                }
+                tm_st4(xa + 8 * (2 * j + h), xr);
+            }
+        const bool update_next = p.sw_every > 0 && p.blur && (it + 1) % p.sw_every == 0;
+        if (!update_next) continue;
+
+        // ---- shrinkwrap: v = |x| blurred, support = { v > thresh * max v } ----
+        if (t < L) gt[t] = p.blur[(size_t)update * L + t];
+        ++update;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const Cx<float> z = o[j][s];
+                o[j][s] = sgn(Cx<float>{sqrtf(fmaf(z.x, z.x, z.y * z.y)), 0.0f});
+            }
+        P::template rows_split_to_buf<false>(o, buf, tw, row, q);
+        __syncthreads();
+        spectral_columns_t<P>(buf, tw, col, q, [&](Cx<float> z, int f, int c) { return cscale(z, gt[f] * gt[c]); });
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, row, q);
+        float vmax = -INFINITY;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                o[j][s].x = sgn(cscale(o[j][s], p.scale)).x;
+                vmax = fmaxf(vmax, o[j][s].x);
+            }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+        if ((t & 31) == 0) red[t >> 5] = vmax;
+        __syncthreads();
+        float m = red[0];
+        for (int w = 1; w < WARPS; ++w) m = fmaxf(m, red[w]);
+        const float thr = p.thresh * m;
+        in_bits = 0;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) in_bits |= (o[j][s].x > thr ? 1u : 0u) << (TPL * j + s);
+        __syncthreads();  // red[] is reused by the next update
+        // the blur overwrote o: x again from tensor memory
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                Cx<float> xr[4];
+                tm_ld4(xa + 8 * (2 * j + h), xr);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) o[j][4 * h + u] = xr[u];
+            }
+    }
+    // x and the support out (the addresses again from the block index, so
+    // that no pointer stays in a register through the iterations)
+    const unsigned b = cta_index();
+    Cx<float>* __restrict__ Xo = p.x + (size_t)b * L * L;
+    float* __restrict__ So = p.S + b * p.s_stride;
+#pragma unroll
+    for (int j = 0; j < J; ++j)
+#pragma unroll
+        for (int s = 0; s < TPL; ++s) {
+            Xo[at(j, s)] = o[j][s];
+            So[at(j, s)] = inside(j, s) ? 1.0f : 0.0f;
+        }
+    if (p.est) {
+        // the estimate: the modulus projection of the final x, restricted to the support
+        Cx<float>* __restrict__ E = p.est + (size_t)b * L * L;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(o[j][s]);
+        P::template rows_split_to_buf<false>(o, buf, tw, row, q);
+        __syncthreads();
+        spectral_columns_t<P>(buf, tw, col, q, [&](Cx<float> z, int f, int c) {
+            return data_apply(z, As[f * AP + c], DMODE);
+        });
+        __syncthreads();
+        P::template row_from_buf<true>(o, buf, tw, row, q);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s)
+                E[at(j, s)] = inside(j, s) ? sgn(cscale(o[j][s], p.scale)) : Cx<float>{0.0f, 0.0f};
+    }
+    tm_wait_st();
+    tm_fence_before_sync();
+    __syncthreads();
+    tm_fence_after_sync();
+    if (warp == 0) tm_free(tm_base, 256);
+}
+
+size_t hio_tm_smem_bytes() {
+    using P = Plane<float, 128, plane_tpl<float, 128>()>;
+    return P::buf_bytes() + sizeof(float) * 128 * (128 + 4) + P::tw_bytes() + sizeof(float) * 128 +
+           sizeof(float) * (P::NT / 32);
+}
+
 template <int L>
 cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
     HioDev d;
@@ -236,8 +432,20 @@ cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
     d.sw_every = a.sw_every;
     d.positivity = a.positivity;
     d.data_mode = a.data_mode;
-    const size_t smem = HioPlan<L>::smem_bytes();
     const bool always = (a.data_mode == DATA_ALWAYS);
+    if constexpr (L == 128) {
+        if (a.tmem) {
+            const size_t smem = hio_tm_smem_bytes();
+            auto k = a.positivity ? (always ? k_hio_tm<DATA_ALWAYS, true> : k_hio_tm<DATA_SKIP_ZERO, true>)
+                                  : (always ? k_hio_tm<DATA_ALWAYS, false> : k_hio_tm<DATA_SKIP_ZERO, false>);
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            k<<<(unsigned)a.batch, 1024, smem, st>>>(d);
+            count_launches();
+            return cudaGetLastError();
+        }
+    }
+    const size_t smem = HioPlan<L>::smem_bytes();
     auto k = a.positivity ? (always ? k_hio<L, DATA_ALWAYS, true> : k_hio<L, DATA_SKIP_ZERO, true>)
                           : (always ? k_hio<L, DATA_ALWAYS, false> : k_hio<L, DATA_SKIP_ZERO, false>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
