@@ -692,12 +692,17 @@ def _hio_inputs(L, B, seed):
     return d["A"], S0, x0
 
 
-@pytest.mark.parametrize("L,B,iters,pos", [(64, 3, 1, False), (64, 3, 5, False), (128, 2, 3, True),
-                                            (256, 2, 3, False), (512, 1, 2, True)])
-def test_hio_iterations_vs_oracle(tb, L, B, iters, pos):
+@pytest.mark.parametrize("L,B,iters,pos,tmem", [(64, 3, 1, False, 1), (64, 3, 5, False, 1), (128, 2, 3, True, 1),
+                                                 (128, 2, 5, False, 0), (128, 3, 5, False, 1),
+                                                 (256, 2, 3, False, 1), (512, 1, 2, True, 1)])
+def test_hio_iterations_vs_oracle(tb, L, B, iters, pos, tmem):
+    """HIO iterations (no support update) against the oracle, 1e-5 relative L2
+    per iteration; at 128^2 both the tensor-memory kernel (tmem 1) and the
+    L2 kernel (tmem 0)."""
     torch, cb = tb
     A, S0, x0 = _hio_inputs(L, B, seed=L + iters)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_TMEM, tmem)
     x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
     assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=0, positivity=pos)
     assert impl.Sync()
@@ -706,8 +711,8 @@ def test_hio_iterations_vs_oracle(tb, L, B, iters, pos):
     np.testing.assert_array_equal(host(S), So.astype(np.float32))   # no update: support unchanged
 
 
-@pytest.mark.parametrize("L", [32, 64, 128])
-def test_hio_fused_split_calls_bitwise(tb, L):
+@pytest.mark.parametrize("L,tmem", [(32, 1), (64, 1), (128, 1), (128, 0)])
+def test_hio_fused_split_calls_bitwise(tb, L, tmem):
     """The fused HIO kernel carries x in registers from one iteration to the
     next and writes half of it to memory only after its last iteration: 7
     iterations in one call equal 3 + 4 iterations in two calls (which restart
@@ -716,6 +721,7 @@ def test_hio_fused_split_calls_bitwise(tb, L):
     B = 3
     A, S0, x0 = _hio_inputs(L, B, seed=L + 11)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_TMEM, tmem)
     Ad = dev(torch, A.ravel())
     for pos in (False, True):
         x1, S1 = dev(torch, x0.ravel()), dev(torch, S0.ravel())
