@@ -754,12 +754,14 @@ def test_hio_shrinkwrap_full_run_rfactor(tb):
     """The plain 2D configuration: 16 patterns of 128x128, HIO beta 0.9, 200
     iterations, shrinkwrap every 20 (sigma 3 -> 1.5, threshold 0.1), random
     phase starts.  The reconstruction (support times modulus projection of the
-    final iterate) has a mean R-factor within 1% (relative) of the float64
-    oracle's.  HIO from random starts is chaotic: the float64 oracle and the
-    same oracle rounded to complex64 each iteration already differ per pattern
-    by up to ~8%, and single patterns of an FP32 run drift further (up to ~18%
-    seen), so per pattern only the median difference (< 3%) and the worst
-    case (< 25%) are bounded."""
+    final iterate) has a mean R-factor within 2% (relative) of the float64
+    oracle's.  HIO from random starts is chaotic: the float64 oracle itself,
+    started from the same starts perturbed by 1e-7 (relative, below float
+    rounding), moves its 16-pattern mean R-factor by 0.1% to 1.6% (six
+    perturbations), its per-pattern median difference by 1.1% to 2.5% and its
+    worst pattern by 7% to 12%; single patterns of an FP32 run drift further
+    (up to ~18% seen).  So the mean is bounded at 2%, the per-pattern median
+    difference at 4% and the worst pattern at 25%."""
     torch, cb = tb
     L, B = 128, 16
     A, S0, x0 = _hio_inputs(L, B, seed=0)
@@ -773,8 +775,8 @@ def test_hio_shrinkwrap_full_run_rfactor(tb):
                                   threshold=0.1)
     ro = O.rfactor(eo, A, L, L, B, a_stride=L * L)
     rel = np.abs(r - ro) / ro
-    assert abs(r.mean() - ro.mean()) / ro.mean() < 0.01, (r, ro)
-    assert np.median(rel) < 0.03 and np.max(rel) < 0.25, (r, ro)
+    assert abs(r.mean() - ro.mean()) / ro.mean() < 0.02, (r, ro)
+    assert np.median(rel) < 0.04 and np.max(rel) < 0.25, (r, ro)
     # the estimate is the modulus projection inside the final support, zero outside
     e = host(est).reshape(B, -1)
     assert np.all(e[host(S).reshape(B, -1) < 0.5] == 0)
@@ -851,8 +853,8 @@ def test_hio_large_full_run_rfactor(tb):
                                   threshold=0.1)
     ro = O.rfactor(eo, A, L, L, B, a_stride=L * L)
     rel = np.abs(r - ro) / ro
-    assert abs(r.mean() - ro.mean()) / ro.mean() < 0.01, (r, ro)
-    assert np.median(rel) < 0.03 and np.max(rel) < 0.25, (r, ro)
+    assert abs(r.mean() - ro.mean()) / ro.mean() < 0.02, (r, ro)
+    assert np.median(rel) < 0.04 and np.max(rel) < 0.25, (r, ro)
     e = host(est).reshape(B, -1)
     assert np.all(e[host(S).reshape(B, -1) < 0.5] == 0)
 
