@@ -250,6 +250,16 @@ struct cpra_b200_ctx {
     bool tmem = true;
     // CPRA_B200_OPT_FUSED3D: the 3D loops as fused axis passes (off: the operator kernels)
     bool fused3d = false;
+    // CPRA_B200_OPT_HIO_CLUSTER: CTAs per pattern of the cluster HIO kernel (0 off, 1 automatic)
+    int hio_cluster = 1;
+    int hio_cluster_trial = -1;  // >= 0: the size under measurement by the tuner
+    std::vector<std::pair<int, int>> cluster_active;  // (side * 100 + size, resident clusters)
+    int sm_count = 0;
+    // device word a cluster kernel sets when a wait for a peer CTA's data ran
+    // out; once such a kernel was launched (directly or in a captured graph),
+    // every Sync reads it (and clears it when set)
+    int* dev_err = nullptr;
+    bool err_pending = false;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -664,6 +674,12 @@ int cpra_b200_create(cpra_b200_ctx** out, int dtype, uint64_t m, uint64_t n, uin
         delete c;
         return cuda_fail(e, "cudaStreamCreate");
     }
+    e = cudaMalloc(reinterpret_cast<void**>(&c->dev_err), sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->dev_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        cpra_b200_destroy(c);
+        return cuda_fail(e, "cudaMalloc(error word)");
+    }
     for (uint64_t L : {m, n, l}) {
         if (L <= 4096) {
             int r = ensure_twiddles(c, L);
@@ -683,6 +699,7 @@ int cpra_b200_destroy(cpra_b200_ctx* c) {
     int rc = flush(c);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& kv : c->tw) cudaFree(kv.second);
+    if (c->dev_err) cudaFree(c->dev_err);
     if (c->work) cudaFree(c->work);
     if (c->partials) cudaFree(c->partials);
     if (c->sums) cudaFree(c->sums);
@@ -773,6 +790,11 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
         case CPRA_B200_OPT_AUTOTUNE: c->autotune = value != 0; break;
         case CPRA_B200_OPT_TMEM: c->tmem = value != 0; break;
         case CPRA_B200_OPT_FUSED3D: c->fused3d = value != 0; break;
+        case CPRA_B200_OPT_HIO_CLUSTER:
+            if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 16)
+                return fail(CPRA_B200_EARG, "hio cluster must be 0, 1, 2, 4, 8 or 16");
+            c->hio_cluster = (int)value;
+            break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1132,6 +1154,15 @@ int cpra_b200_sync(cpra_b200_ctx* c) {
     int r = flush(c);
     if (r) return take_deferred(c);
     CPRA_CHECK_CUDA(cudaStreamSynchronize(c->stream), "Sync");
+    if (c->err_pending) {
+        int h = 0;
+        CPRA_CHECK_CUDA(cudaMemcpy(&h, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost), "Sync");
+        if (h) {
+            CPRA_CHECK_CUDA(cudaMemset(c->dev_err, 0, sizeof(int)), "Sync");
+            return fail(CPRA_B200_ECUDA,
+                        "hio cluster kernel: a CTA's wait for its peers' data ran out; the results are invalid");
+        }
+    }
     return CPRA_B200_OK;
 }
 
@@ -1274,6 +1305,43 @@ uint64_t hio_scratch_bytes(bool dbl, uint64_t L, uint64_t chunk) {
     return chunk * L * L * 8 + chunk * L * L * 4 + chunk * L * L / 8 + chunk * 4;
 }
 
+// clusters of `cluster` CTAs of the side-L kernel resident at once (cached)
+int cluster_resident(cpra_b200_ctx* c, uint64_t L, int cluster) {
+    const int key = (int)L * 100 + cluster;
+    for (const auto& e : c->cluster_active)
+        if (e.first == key) return e.second;
+    const int n = hio_cluster_max_active(L, cluster);
+    c->cluster_active.emplace_back(key, n);
+    return n;
+}
+
+// CTAs per pattern of the cluster kernel for a job of `batch` patterns of
+// side L, or 0 for the one-CTA kernels (32-128) and the line passes (256, 512).
+// Automatic: the cluster kernel only where the batch cannot fill the device
+// otherwise, the largest cluster whose CTAs take one SM each and all fit at
+// once (128: 8, 4 or 2; 256: 8); at 128 only with the tensor-memory kernel
+// as the alternative, whose bits it shares.  A batch that fills the SMs with
+// one CTA per pattern (128) or runs as line passes (256) is faster without.
+int hio_cluster_for(cpra_b200_ctx* c, uint64_t L, uint64_t batch) {
+    if (c->dbl || batch == 0) return 0;
+    if (c->hio_cluster_trial >= 0) return c->hio_cluster_trial;
+    if (c->hio_cluster == 0) return 0;
+    if (c->hio_cluster > 1) return hio_cluster_supported(c->dbl, L, c->hio_cluster) ? c->hio_cluster : 0;
+    if (L == 128 && !c->tmem) return 0;
+    if (c->sm_count == 0 && cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess)
+        return 0;
+    for (int cl : {8, 4, 2}) {
+        if (!hio_cluster_supported(c->dbl, L, cl)) continue;
+        if (batch * (uint64_t)cl <= (uint64_t)c->sm_count && batch <= (uint64_t)cluster_resident(c, L, cl)) return cl;
+    }
+    return 0;
+}
+
+// scratch of a job: none for the fused and cluster kernels
+uint64_t hio_job_scratch(cpra_b200_ctx* c, uint64_t L, uint64_t batch, uint64_t chunk) {
+    return hio_cluster_for(c, L, batch) ? 0 : hio_scratch_bytes(c->dbl, L, chunk);
+}
+
 // enqueue one job on `st` (arguments already checked); `scratch` holds
 // hio_scratch_bytes(L, chunk)
 int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t chunk, void* scratch,
@@ -1302,6 +1370,12 @@ int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t 
     a.threshold = h.threshold;
     int r = ensure_twiddles(c, j.L);
     if (r) return r;
+    if (const int cl = hio_cluster_for(c, j.L, j.batch)) {
+        a.err = c->dev_err;
+        c->err_pending = true;
+        CPRA_CHECK_CUDA(launch_hio_cluster(a, cl, twiddles(c, j.L), st), "hio_shrinkwrap");
+        return CPRA_B200_OK;
+    }
     if (hio_fused_supported(c->dbl, j.L, j.L)) {
         CPRA_CHECK_CUDA(launch_hio_iterations(c->dbl, a, twiddles(c, j.L), st), "hio_shrinkwrap");
         return CPRA_B200_OK;
@@ -1400,8 +1474,46 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
     // once per (side, batch) among the whole batch, a half and a quarter, on
     // copies of x and S, min(iters, 20) iterations each (the chunk changes
     // the schedule only)
-    if (c->autotune && c->hio_chunk == 0 && !hio_fused_supported(c->dbl, c->m, c->n) && batch > 1 && iters > 0 &&
-        !stream_capturing(c)) {
+    // CPRA_B200_OPT_AUTOTUNE with the automatic cluster choice at 128 (the
+    // tensor-memory kernel): one CTA per pattern against clusters of 2, 4 and
+    // 8, measured once per (batch, iterations) on copies of x and S,
+    // min(iters, 20) iterations each (all four write the same bits)
+    int tuned_cluster = -1;
+    if (c->autotune && c->hio_cluster == 1 && !c->dbl && c->m == 128 && c->tmem && iters > 0 && !stream_capturing(c)) {
+        const uint64_t plane = c->plane();
+        const uint64_t xb = batch * plane * c->csize();
+        const uint64_t sb = (s_stride ? batch * s_stride : plane) * c->esize();
+        TrialBuffer trial(c);
+        if (trial.alloc(xb + sb + 256)) {
+            void* tx = trial.p;
+            void* tS = static_cast<char*>(trial.p) + (xb + 255) / 256 * 256;
+            HioParams ht = h;
+            ht.iters = std::min(iters, 20);
+            const std::string key = "hio_cluster:" + std::to_string(c->m) + "," + std::to_string(batch) + "," +
+                                    std::to_string(ht.iters) + "," + std::to_string(sw_every) + "," +
+                                    std::to_string(c->data_mode) + "," + std::to_string(positivity);
+            uint64_t pick = 0;
+            r = tuned_choice(
+                c, key, {0, 2, 4, 8},
+                [&]() -> int {
+                    CPRA_CHECK_CUDA(cudaMemcpyAsync(tx, x, xb, cudaMemcpyDeviceToDevice, c->stream), "autotune");
+                    CPRA_CHECK_CUDA(cudaMemcpyAsync(tS, S, sb, cudaMemcpyDeviceToDevice, c->stream), "autotune");
+                    return CPRA_B200_OK;
+                },
+                [&](uint64_t k) {
+                    c->hio_cluster_trial = (int)k;
+                    const int rr = hio_enqueue(c, HioJob{c->m, batch, tx, A, a_stride, tS, s_stride, nullptr}, ht, 0,
+                                               nullptr, c->stream);
+                    c->hio_cluster_trial = -1;
+                    return rr;
+                },
+                &pick);
+            if (r) return r;
+            tuned_cluster = (int)pick;
+        }
+    }
+    if (c->autotune && c->hio_chunk == 0 && !hio_fused_supported(c->dbl, c->m, c->n) &&
+        !hio_cluster_for(c, c->m, batch) && batch > 1 && iters > 0 && !stream_capturing(c)) {
         const uint64_t plane = c->plane();
         const uint64_t xb = batch * plane * c->csize();
         // S too: the passes write the support back (packed at the start, unpacked at the end)
@@ -1435,9 +1547,12 @@ int cpra_b200_hio_shrinkwrap(cpra_b200_ctx* c, void* x, const void* A, uint64_t 
             if (r) return r;
         }
     }
-    r = ensure_work(c, hio_scratch_bytes(c->dbl, c->m, chunk));
+    r = ensure_work(c, hio_job_scratch(c, c->m, batch, chunk));
     if (r) return r;
-    return hio_enqueue(c, HioJob{c->m, batch, x, A, a_stride, S, s_stride, estimate}, h, chunk, c->work, c->stream);
+    c->hio_cluster_trial = tuned_cluster;
+    r = hio_enqueue(c, HioJob{c->m, batch, x, A, a_stride, S, s_stride, estimate}, h, chunk, c->work, c->stream);
+    c->hio_cluster_trial = -1;
+    return r;
 }
 
 int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets, int n_buckets, int iters,
@@ -1491,7 +1606,7 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
         const cpra_b200_hio_bucket& b = buckets[order[k]];
         BucketLane& lane = c->bucket_streams[k];
         const uint64_t chunk = (c->hio_chunk == 0) ? b.count : std::min(c->hio_chunk, b.count);
-        r = ensure_buffer(c, &lane.scratch, &lane.scratch_bytes, hio_scratch_bytes(c->dbl, b.side, chunk),
+        r = ensure_buffer(c, &lane.scratch, &lane.scratch_bytes, hio_job_scratch(c, b.side, b.count, chunk),
                           "cudaMalloc(hio_batched scratch)");
         if (r) return r;
         r = ensure_twiddles(c, b.side);
@@ -1520,7 +1635,7 @@ int cpra_b200_hio_batched(cpra_b200_ctx* c, const cpra_b200_hio_bucket* buckets,
         return CPRA_B200_OK;
     };
     std::string key = graph_key("hio_batched", n_buckets, iters, beta, sw_every, sigma_start, sigma_end, threshold,
-                                positivity, c->hio_chunk, c->data_mode);
+                                positivity, c->hio_chunk, c->data_mode, c->tmem, c->hio_cluster);
     for (int i = 0; i < n_buckets; ++i) key.append(reinterpret_cast<const char*>(&buckets[i]), sizeof(buckets[i]));
     return run_maybe_graph(c, key, enqueue);
 }
@@ -1874,6 +1989,7 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
         case CPRA_B200_OPT_AUTOTUNE: *value = c->autotune ? 1 : 0; break;
         case CPRA_B200_OPT_TMEM: *value = c->tmem ? 1 : 0; break;
         case CPRA_B200_OPT_FUSED3D: *value = c->fused3d ? 1 : 0; break;
+        case CPRA_B200_OPT_HIO_CLUSTER: *value = c->hio_cluster; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -2249,7 +2365,8 @@ static int cpra_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     r = (ready || done) ? enqueue()
                         : run_maybe_graph(c,
                                           graph_key("cpra_run", x, A, S, P, batch, epi, iters, pre_iter, b,
-                                                    final_step, want_err, c->space_mode, c->data_mode, c->fusion, W),
+                                                    final_step, want_err, c->space_mode, c->data_mode, c->fusion, W,
+                                                    c->tmem),
                                           enqueue);
     if (r) return r;
     if (after_enqueue && (r = after_enqueue())) return r;
@@ -2431,7 +2548,7 @@ static int conv_run_impl(cpra_b200_ctx* c, void* x, const void* A, const void* S
     };
     r = run_maybe_graph(c,
                         graph_key("conv_run", x, A, S, iters, b, final_step, want_err, c->space_mode, c->data_mode,
-                                  c->fusion),
+                                  c->fusion, c->fused3d),
                         enqueue);
     if (r) return r;
     if (want_err) {

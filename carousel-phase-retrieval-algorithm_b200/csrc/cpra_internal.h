@@ -181,9 +181,20 @@ struct HioArgs {
     int iters, sw_every, positivity, data_mode;
     double beta, threshold;
     int tmem = 1;  // 128 x 128: the half of x that k_hio sends through L2 stays in tensor memory
+    int* err = nullptr;  // cluster kernel: device word set to 1 when a wait for a peer's data ran out
 };
 bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st);
+
+// ---- the same iteration with each pattern over a thread-block cluster (kernels_hio.cu) ----
+// Float square planes: 128 with 2, 4 or 8 CTAs per pattern, 256 with 8 or 16.
+// Same bits as the one-CTA kernel of the same line split (k_hio_tm at 128)
+// for every cluster size.  No scratch.
+bool hio_cluster_supported(bool dbl, uint64_t L, int cluster);
+size_t hio_cluster_smem_bytes(uint64_t L, int cluster);
+// clusters of that size resident at once on the current device (0: none)
+int hio_cluster_max_active(uint64_t L, int cluster);
+cudaError_t launch_hio_cluster(const HioArgs& a, int cluster, const void* tw, cudaStream_t st);
 
 // ---- the same HIO iteration as line passes through L2 (kernels_large.cu) ----
 // Float square planes of 256 or 512; patterns run in chunks of `chunk`, each

@@ -25,6 +25,7 @@
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
+#include "cluster.cuh"
 #include "tmem.cuh"
 
 namespace cpra_b200 {
@@ -40,6 +41,7 @@ struct HioDev {
     uint64_t s_stride;
     const Cx<float>* tw;
     const float* blur;  // [updates][L]: g at the frequency of each (D-shifted) row/column index
+    int* err;           // cluster kernel: set to 1 when a wait for a peer's data ran out
     float scale, beta, thresh;
     int iters, sw_every, positivity, data_mode;
 };
@@ -414,8 +416,340 @@ size_t hio_tm_smem_bytes() {
            sizeof(float) * (P::NT / 32);
 }
 
-template <int L>
-cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
+// ---- one pattern over a thread-block cluster of CL CTAs ----------------------------------
+//
+// CTA rank r of a pattern's cluster owns rows r*RPC .. r*RPC + RPC - 1 in the
+// row phases and the same range of columns in the column phase (RPC = L/CL).
+// A line is TPL threads (8 at 128, 16 at 256) with R = L/TPL values each.
+// Per transform of the plane:
+//   row phase     each row, from registers, through its row DFT into the
+//                 row buffer (scratch and result: the row's own slots); the
+//                 row's RPC-element block of each CTA's columns goes to that
+//                 CTA's column buffer in one bulk copy
+//   column phase  (once every CTA's blocks have arrived) each owned column
+//                 through the column DFT, the per-frequency operation (the
+//                 modulus projection or the shrinkwrap blur), the inverse
+//                 column DFT, back into the column buffer; the block of each
+//                 CTA's rows goes to that CTA's row buffer, one bulk copy per
+//                 row
+//   row phase     (once every block has arrived) each row through the
+//                 inverse row DFT into registers, then the HIO update of x.
+// Arrivals are counted in bytes on one mbarrier per buffer, armed for the
+// next phase as soon as the current one completes (no data of the next phase
+// can be sent before this CTA sends its own part of the current one).  A
+// phase whose bytes have not arrived within a second sets the launch's
+// error word; the CTA then stops waiting and sending, runs to the end and
+// waits once more, bounded, for what is still in flight.  An iteration thus
+// moves the plane twice between the SMs' shared memories by the copy
+// engines and never through L2; global memory is read when the launch starts
+// and written after the last iteration.  The shrinkwrap maximum is
+// exchanged with remote stores and a cluster barrier (one value per CTA).
+// The line transforms, their scratch layout and every per-element step are
+// those of the one-CTA kernels of the same split (k_hio_tm at 128), in the
+// same order, so the results are the same bits for any cluster size.
+//
+// Shared memory: the two mbarriers; the row buffer [RPC][LS] (LS = L + 2;
+// the rows of a half-warp 4 apart at TPL 8, so its slots fall on distinct
+// bank pairs); the column buffer [L][CP], row-major over the owned columns
+// (CP = RPC + 2: a half-warp's two columns and 8 ranks on distinct bank
+// pairs at TPL 8; rows 16-byte aligned for the copies); A of the owned
+// columns, column-major (pitch ACP); twiddles; a blur table row; maxima.
+template <int L, int CL>
+struct ClGeom {
+    static constexpr int TPL = (L <= 128) ? 8 : 16;
+    using F = LineFFT<float, L, TPL>;
+    static constexpr int R = L / TPL, J = F::J;
+    static constexpr int RPC = L / CL;  // rows (and columns) per CTA
+    static constexpr int NT = RPC * TPL;
+    static constexpr int LS = L + 2;
+    static constexpr int CP = RPC + 2;
+    static constexpr int ACP = (TPL == 8) ? L + 8 : L + 16;
+    static constexpr int WARPS = NT / 32;
+    static constexpr uint32_t BLOCK_BYTES = RPC * sizeof(Cx<float>);         // one copy
+    static constexpr uint32_t PHASE_BYTES = (uint32_t)RPC * L * sizeof(Cx<float>);  // a buffer's arrivals
+    static_assert(R == 16 && !F::HALF, "16 values per thread");
+    static_assert(TPL == 16 || NT % 128 == 0, "TPL 8: rows in groups of 16 per 128 threads");
+    static_assert(NT <= 1024 && NT >= L && CL <= TPL, "copy issuers: L threads, CL ranks per row");
+    static_assert(BLOCK_BYTES % 16 == 0 && (LS * sizeof(Cx<float>)) % 16 == 0 && (CP * sizeof(Cx<float>)) % 16 == 0,
+                  "16-byte copies");
+    static constexpr size_t rbuf_off() { return 16; }
+    static constexpr size_t cbuf_off() { return rbuf_off() + sizeof(Cx<float>) * (size_t)RPC * LS; }
+    static constexpr size_t a_off() { return cbuf_off() + sizeof(Cx<float>) * (size_t)L * CP; }
+    static constexpr size_t tw_off() { return a_off() + sizeof(float) * (size_t)RPC * ACP; }
+    static constexpr size_t smem_bytes() {
+        return tw_off() + sizeof(Cx<float>) * F::TW_ENTRIES + sizeof(float) * (L + WARPS + CL);
+    }
+    // the row of thread t in the row phases
+    __device__ __forceinline__ static int row_of(int t) {
+        if constexpr (TPL == 8)
+            return ((t >> 7) << 4) + ((t >> 5) & 3) + 4 * ((t >> 3) & 3);
+        else
+            return t / TPL;
+    }
+};
+
+// a second: far above any phase of a healthy launch
+constexpr uint64_t CLUSTER_WAIT_NS = 1000000000ull;
+
+template <int L, int CL, int DMODE, bool POS>
+__global__ void __launch_bounds__(ClGeom<L, CL>::NT, 1) k_hio_cl(const HioDev p) {
+    using G = ClGeom<L, CL>;
+    using F = typename G::F;
+    constexpr int J = G::J, TPL = G::TPL, R = G::R, RPC = G::RPC, LS = G::LS, CP = G::CP, ACP = G::ACP,
+                  NT = G::NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<float>* rbuf = reinterpret_cast<Cx<float>*>(smem_raw + G::rbuf_off());
+    Cx<float>* cbuf = reinterpret_cast<Cx<float>*>(smem_raw + G::cbuf_off());
+    float* Ac = reinterpret_cast<float*>(smem_raw + G::a_off());
+    Cx<float>* tw = reinterpret_cast<Cx<float>*>(smem_raw + G::tw_off());
+    float* gt = reinterpret_cast<float*>(tw + F::TW_ENTRIES);
+    float* red = gt + L;           // [WARPS] this CTA's warp maxima
+    float* cmax = red + G::WARPS;  // [CL] every CTA's maximum
+    const int t = threadIdx.x, q = t % TPL, warp = t >> 5;
+    const int row = G::row_of(t);  // this CTA's row in the row phases
+    const int cl = t / TPL;        // this CTA's column in the column phase
+    const int rank = (int)cluster_ctarank();
+    const int grow = rank * RPC + row, gcol = rank * RPC + cl;
+    const uint32_t base = smem_addr_u32(smem_raw);
+    const uint32_t mb_r = base, mb_c = base + 8;  // arrivals into the row / the column buffer
+    const uint32_t rb = base + (uint32_t)G::rbuf_off(), cb = base + (uint32_t)G::cbuf_off();
+    const uint32_t cm = smem_addr_u32(cmax);
+    // phases of each buffer in this launch (uniform over the cluster)
+    const int n_phases =
+        p.iters + ((p.sw_every > 0 && p.blur) ? p.iters / p.sw_every : 0) + (p.est ? 1 : 0);
+    if (t == 0) {
+        mbar_init(mb_r, 1);
+        mbar_init(mb_c, 1);
+        fence_mbar_init();
+        mbar_arrive_expect(mb_r, G::PHASE_BYTES);
+        mbar_arrive_expect(mb_c, G::PHASE_BYTES);
+    }
+    F::fill_twiddles(tw, p.tw, t, NT);
+    auto pos = [&](int j, int s) { return q + TPL * j + R * s; };
+    Cx<float> x[J][TPL];
+    uint32_t in_bits = 0;  // bit TPL j + s: the support at (grow, pos(j, s))
+    {
+        const size_t pat = blockIdx.x / CL;
+        const float* __restrict__ A = p.A + pat * p.a_stride;
+        for (int i = t; i < L * RPC; i += NT) {
+            const int f = i / RPC, c = i % RPC;
+            Ac[c * ACP + f] = A[(size_t)f * L + rank * RPC + c];
+        }
+        const Cx<float>* __restrict__ X = p.x + pat * L * L + (size_t)grow * L;
+        const float* __restrict__ S = p.S + pat * p.s_stride + (size_t)grow * L;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                x[j][s] = X[pos(j, s)];
+                in_bits |= (S[pos(j, s)] > 0.5f ? 1u : 0u) << (TPL * j + s);
+            }
+    }
+    auto inside = [&](int j, int s) { return (in_bits >> (TPL * j + s)) & 1u; };
+    const bool neg = ((grow + q) & 1) != 0;
+    auto sgn = [&](Cx<float> z) { return neg ? Cx<float>{-z.x, -z.y} : z; };
+
+    bool ok = true;  // false once a wait ran out: no more waits or copies
+    uint32_t par_r = 0, par_c = 0;
+    int done_r = 0, done_c = 0;
+    auto wait_phase = [&](uint32_t mb, uint32_t& par, int& done) {
+        if (ok && !mbar_wait(mb, par, CLUSTER_WAIT_NS)) {
+            ok = false;
+            if (p.err) atomicExch(p.err, 1);
+        }
+        // the next phase of this buffer: no byte of it can have been sent yet
+        if (t == 0 && ok && done + 1 < n_phases) mbar_arrive_expect(mb, G::PHASE_BYTES);
+        par ^= 1u;
+        ++done;
+    };
+    // forward row DFT of o into this row's slots; each CTA's block of columns to it
+    auto rows_forward = [&](Cx<float>(&o)[J][TPL]) {
+        Cx<float>* rw = rbuf + row * LS;
+        Cx<float> v[R];
+        F::template split_to_natural<false>(o, v, rw, 1, tw, q);
+#pragma unroll
+        for (int i = 0; i < R; ++i) rw[q + TPL * brev<R>(i)] = v[i];
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (q < CL && ok)
+            bulk_copy_to_cta(cluster_map(cb + 8u * (uint32_t)(grow * CP), (uint32_t)q),
+                             rb + 8u * (uint32_t)(row * LS + q * RPC), G::BLOCK_BYTES, cluster_map(mb_c, (uint32_t)q));
+    };
+    // column DFT, op per frequency, inverse column DFT of the arrived rows;
+    // each CTA's block of rows to it
+    auto columns = [&](auto op) {
+        wait_phase(mb_c, par_c, done_c);
+        Cx<float>* col = cbuf + cl;
+        Cx<float> v[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) v[k] = col[(q + TPL * k) * CP];
+        Cx<float> o[J][TPL];
+        F::template natural_to_split<false>(v, o, col, CP, tw, q);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = op(o[j][s], pos(j, s));
+        F::template split_to_natural<true>(o, v, col, CP, tw, q);
+#pragma unroll
+        for (int i = 0; i < R; ++i) col[(q + TPL * brev<R>(i)) * CP] = v[i];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (t < L && ok) {
+            const int s = t / RPC, rl = t % RPC;  // global row t: local row rl of CTA s
+            bulk_copy_to_cta(cluster_map(rb + 8u * (uint32_t)(rl * LS + rank * RPC), (uint32_t)s),
+                             cb + 8u * (uint32_t)(t * CP), G::BLOCK_BYTES, cluster_map(mb_r, (uint32_t)s));
+        }
+    };
+    // inverse row DFT of the arrived row into o
+    auto rows_inverse = [&](Cx<float>(&o)[J][TPL]) {
+        wait_phase(mb_r, par_r, done_r);
+        Cx<float>* rw = rbuf + row * LS;
+        Cx<float> v[R];
+#pragma unroll
+        for (int k = 0; k < R; ++k) v[k] = rw[q + TPL * k];
+        F::template natural_to_split<true>(v, o, rw, 1, tw, q);
+    };
+    auto modulus = [&](Cx<float> z, int f) { return data_apply(z, Ac[cl * ACP + f], DMODE); };
+    __syncthreads();
+    cluster_sync();  // every CTA running, its barriers initialised, before the first copy
+
+    int update = 0;
+    for (int it = 0; it < p.iters; ++it) {
+        Cx<float> o[J][TPL];
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(x[j][s]);
+        rows_forward(o);
+        columns(modulus);
+        rows_inverse(o);
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const Cx<float> y = sgn(cscale(o[j][s], p.scale));
+                const bool keep = inside(j, s) && (!POS || y.x >= 0.0f);
+                x[j][s] = keep ? y : merge_apply(y, x[j][s], -p.beta, 1.0f);
+            }
+        const bool update_next = p.sw_every > 0 && p.blur && (it + 1) % p.sw_every == 0;
+        if (!update_next) continue;
+
+        // ---- shrinkwrap: v = |x| blurred, support = { v > thresh * max v } ----
+        for (int i = t; i < L; i += NT) gt[i] = p.blur[(size_t)update * L + i];
+        ++update;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                const Cx<float> z = x[j][s];
+                o[j][s] = sgn(Cx<float>{sqrtf(fmaf(z.x, z.x, z.y * z.y)), 0.0f});
+            }
+        rows_forward(o);
+        // gt is read by the column phase after its wait, which follows the
+        // __syncwarp and copies above; the block barrier makes it visible
+        __syncthreads();
+        columns([&](Cx<float> z, int f) { return cscale(z, gt[f] * gt[gcol]); });
+        rows_inverse(o);
+        float vmax = -INFINITY;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                o[j][s].x = sgn(cscale(o[j][s], p.scale)).x;
+                vmax = fmaxf(vmax, o[j][s].x);
+            }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, off));
+        if ((t & 31) == 0) red[warp] = vmax;
+        __syncthreads();
+        if (t < CL) {
+            float m = red[0];
+            for (int w = 1; w < G::WARPS; ++w) m = fmaxf(m, red[w]);
+            cluster_store(cluster_map(cm + 4u * (uint32_t)rank, (uint32_t)t), m);
+        }
+        cluster_sync();
+        float m = cmax[0];
+#pragma unroll
+        for (int r = 1; r < CL; ++r) m = fmaxf(m, cmax[r]);
+        const float thr = p.thresh * m;
+        in_bits = 0;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) in_bits |= (o[j][s].x > thr ? 1u : 0u) << (TPL * j + s);
+    }
+    {
+        // x and the support out (addresses from the block index again)
+        const size_t pat = cta_index() / CL;
+        Cx<float>* __restrict__ Xo = p.x + pat * L * L + (size_t)grow * L;
+        float* __restrict__ So = p.S + pat * p.s_stride + (size_t)grow * L;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) {
+                Xo[pos(j, s)] = x[j][s];
+                So[pos(j, s)] = inside(j, s) ? 1.0f : 0.0f;
+            }
+    }
+    if (p.est) {
+        // the estimate: the modulus projection of the final x, restricted to the support
+        Cx<float> o[J][TPL];
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s) o[j][s] = sgn(x[j][s]);
+        rows_forward(o);
+        columns(modulus);
+        rows_inverse(o);
+        Cx<float>* __restrict__ E = p.est + (cta_index() / CL) * L * L + (size_t)grow * L;
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+#pragma unroll
+            for (int s = 0; s < TPL; ++s)
+                E[pos(j, s)] = inside(j, s) ? sgn(cscale(o[j][s], p.scale)) : Cx<float>{0.0f, 0.0f};
+    }
+    if (!ok) {
+        // a wait ran out: give copies still in flight a bounded moment to land
+        const uint64_t t0 = globaltimer_ns();
+        while (globaltimer_ns() - t0 < 1000000ull) {
+        }
+    }
+    // Every byte sent to this CTA has arrived (its last waits).  Once every
+    // CTA is here no copy of the launch is in flight, and no CTA's shared
+    // memory is read or written by another any more.
+    cluster_sync();
+}
+template <int L, int CL>
+cudaError_t hio_cluster_launch_cl(const HioDev& d, const HioArgs& a, cudaStream_t st) {
+    using G = ClGeom<L, CL>;
+    const bool always = (a.data_mode == DATA_ALWAYS);
+    auto k = a.positivity ? (always ? k_hio_cl<L, CL, DATA_ALWAYS, true> : k_hio_cl<L, CL, DATA_SKIP_ZERO, true>)
+                          : (always ? k_hio_cl<L, CL, DATA_ALWAYS, false> : k_hio_cl<L, CL, DATA_SKIP_ZERO, false>);
+    const size_t smem = G::smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if constexpr (CL > 8) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(a.batch * CL));
+    cfg.blockDim = dim3(G::NT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k, d);
+    count_launches();
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+HioDev hio_dev(const HioArgs& a, const void* tw) {
     HioDev d;
     d.x = (Cx<float>*)a.x;
     d.est = (Cx<float>*)a.estimate;
@@ -425,6 +759,7 @@ cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
     d.s_stride = a.s_stride;
     d.tw = (const Cx<float>*)tw;
     d.blur = (const float*)a.blur;
+    d.err = a.err;
     d.scale = 1.0f / (float)(a.M * a.N);
     d.beta = (float)a.beta;
     d.thresh = (float)a.threshold;
@@ -432,6 +767,12 @@ cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
     d.sw_every = a.sw_every;
     d.positivity = a.positivity;
     d.data_mode = a.data_mode;
+    return d;
+}
+
+template <int L>
+cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
+    const HioDev d = hio_dev(a, tw);
     const bool always = (a.data_mode == DATA_ALWAYS);
     if constexpr (L == 128) {
         if (a.tmem) {
@@ -458,6 +799,77 @@ cudaError_t hio_launch(const HioArgs& a, const void* tw, cudaStream_t st) {
 }  // namespace
 
 bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N) { return dm_fused_supported(dbl, M, N); }
+
+bool hio_cluster_supported(bool dbl, uint64_t L, int cluster) {
+    if (dbl) return false;
+    if (L == 128) return cluster == 2 || cluster == 4 || cluster == 8;
+    if (L == 256) return cluster == 8 || cluster == 16;
+    return false;
+}
+
+size_t hio_cluster_smem_bytes(uint64_t L, int cluster) {
+    if (L == 128) return cluster == 2 ? ClGeom<128, 2>::smem_bytes()
+                         : cluster == 4 ? ClGeom<128, 4>::smem_bytes()
+                                        : ClGeom<128, 8>::smem_bytes();
+    return cluster == 8 ? ClGeom<256, 8>::smem_bytes() : ClGeom<256, 16>::smem_bytes();
+}
+
+namespace {
+template <int L, int CL>
+int hio_cluster_max_active_cl() {
+    using G = ClGeom<L, CL>;
+    auto k = k_hio_cl<L, CL, DATA_SKIP_ZERO, false>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem_bytes()) != cudaSuccess)
+        return 0;
+    if constexpr (CL > 8) {
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL);
+    cfg.blockDim = dim3(G::NT);
+    cfg.dynamicSmemBytes = G::smem_bytes();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+}  // namespace
+
+int hio_cluster_max_active(uint64_t L, int cluster) {
+    if (!hio_cluster_supported(false, L, cluster)) return 0;
+    if (L == 128) return cluster == 2 ? hio_cluster_max_active_cl<128, 2>()
+                         : cluster == 4 ? hio_cluster_max_active_cl<128, 4>()
+                                        : hio_cluster_max_active_cl<128, 8>();
+    return cluster == 8 ? hio_cluster_max_active_cl<256, 8>() : hio_cluster_max_active_cl<256, 16>();
+}
+
+cudaError_t launch_hio_cluster(const HioArgs& a, int cluster, const void* tw, cudaStream_t st) {
+    if (a.M != a.N || !hio_cluster_supported(false, a.M, cluster)) return cudaErrorInvalidValue;
+    if (a.batch == 0 || (a.iters <= 0 && !a.estimate)) return cudaSuccess;
+    const HioDev d = hio_dev(a, tw);
+    if (a.M == 128) {
+        switch (cluster) {
+            case 2: return hio_cluster_launch_cl<128, 2>(d, a, st);
+            case 4: return hio_cluster_launch_cl<128, 4>(d, a, st);
+            case 8: return hio_cluster_launch_cl<128, 8>(d, a, st);
+        }
+    } else {
+        switch (cluster) {
+            case 8: return hio_cluster_launch_cl<256, 8>(d, a, st);
+            case 16: return hio_cluster_launch_cl<256, 16>(d, a, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st) {
     if (!hio_fused_supported(dbl, a.M, a.N)) return cudaErrorInvalidValue;

@@ -90,8 +90,26 @@ extern "C" {
                                     results either way. */
 #define CPRA_B200_OPT_TMEM 11      /* 1 (default): the fused 128 x 128 kernels keep their per-thread iterates
                                     in the SM's tensor memory for the whole launch (x and t2 of the
-                                    difference map); 0: through L2 once per iteration.  Same results either
-                                    way. */
+                                    difference map, x of HIO); 0: through L2 once per iteration.  The
+                                    difference map gives the same results either way; HIO with 1 splits
+                                    each line over 8 threads (4 with 0), as the 128 x 128 operator
+                                    transforms do, and agrees with 0 to rounding, not bit for bit. */
+#define CPRA_B200_OPT_HIO_CLUSTER 13 /* cpra_b200_hio_shrinkwrap and cpra_b200_hio_batched: each pattern of
+                                    side 128 or 256 spread over a thread-block cluster of this many CTAs
+                                    (128: 2, 4 or 8; 256: 8 or 16), the plane exchanged between the CTAs'
+                                    shared memories over the cluster network instead of through L2; other
+                                    sides and unsupported sizes keep their kernels.  0: one CTA per pattern
+                                    at 128, line passes at 256.  1 (default): automatic, the cluster kernel
+                                    only for a batch too small to fill the device otherwise, the largest
+                                    cluster (128: 8, 4 or 2; 256: 8) whose CTAs take one SM each and all
+                                    fit at once, and at 128 only with CPRA_B200_OPT_TMEM 1; with
+                                    CPRA_B200_OPT_AUTOTUNE, 128 x 128 calls measure one CTA per pattern
+                                    against clusters of 2, 4 and 8 once per (batch, iterations) on copies
+                                    of x and S.  At 128 the results are those of the tensor-memory kernel
+                                    bit for bit; at 256 the same for 8 and 16, and within rounding of the
+                                    line passes.  A cluster CTA that waits more than a second for its
+                                    peers' data marks the launch failed: the next cpra_b200_sync returns
+                                    CPRA_B200_ECUDA. */
 
 typedef struct cpra_b200_ctx cpra_b200_ctx;
 

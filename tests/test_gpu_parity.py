@@ -698,11 +698,12 @@ def _hio_inputs(L, B, seed):
 def test_hio_iterations_vs_oracle(tb, L, B, iters, pos, tmem):
     """HIO iterations (no support update) against the oracle, 1e-5 relative L2
     per iteration; at 128^2 both the tensor-memory kernel (tmem 1) and the
-    L2 kernel (tmem 0)."""
+    L2 kernel (tmem 0), at 256^2 and 512^2 the line passes (the cluster
+    kernel has its own tests below)."""
     torch, cb = tb
     A, S0, x0 = _hio_inputs(L, B, seed=L + iters)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
-    assert impl.set_option(cb.OPT_TMEM, tmem)
+    assert impl.set_option(cb.OPT_TMEM, tmem) and impl.set_option(cb.OPT_HIO_CLUSTER, 0)
     x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
     assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=0, positivity=pos)
     assert impl.Sync()
@@ -711,17 +712,19 @@ def test_hio_iterations_vs_oracle(tb, L, B, iters, pos, tmem):
     np.testing.assert_array_equal(host(S), So.astype(np.float32))   # no update: support unchanged
 
 
-@pytest.mark.parametrize("L,tmem", [(32, 1), (64, 1), (128, 1), (128, 0)])
-def test_hio_fused_split_calls_bitwise(tb, L, tmem):
-    """The fused HIO kernel carries x in registers from one iteration to the
-    next and writes half of it to memory only after its last iteration: 7
-    iterations in one call equal 3 + 4 iterations in two calls (which restart
-    from memory), bit for bit, with and without positivity."""
+@pytest.mark.parametrize("L,tmem,cluster", [(32, 1, 0), (64, 1, 0), (128, 1, 0), (128, 0, 0), (128, 1, 8),
+                                            (256, 1, 8)])
+def test_hio_fused_split_calls_bitwise(tb, L, tmem, cluster):
+    """The fused HIO kernels carry x on chip from one iteration to the next
+    and write it to memory only after their last iteration: 7 iterations in
+    one call equal 3 + 4 iterations in two calls (which restart from memory),
+    bit for bit, with and without positivity; the one-CTA kernels and the
+    cluster kernel (8 CTAs per pattern)."""
     torch, cb = tb
     B = 3
     A, S0, x0 = _hio_inputs(L, B, seed=L + 11)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
-    assert impl.set_option(cb.OPT_TMEM, tmem)
+    assert impl.set_option(cb.OPT_TMEM, tmem) and impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
     Ad = dev(torch, A.ravel())
     for pos in (False, True):
         x1, S1 = dev(torch, x0.ravel()), dev(torch, S0.ravel())
@@ -784,15 +787,15 @@ def test_hio_shrinkwrap_full_run_rfactor(tb):
 
 # ---- 256 and 512: the same iteration as line passes over chunks of patterns --------------
 def test_hio_large_chunking_is_exact(tb):
-    """Patterns are independent, so the chunk size (patterns per pass) must
-    not change a bit of x, S or the estimate."""
+    """Patterns are independent, so the chunk size (patterns per pass) of the
+    line passes must not change a bit of x, S or the estimate."""
     torch, cb = tb
     L, B = 256, 3
     A, S0, x0 = _hio_inputs(L, B, seed=7)
     out = []
     for chunk in (0, 1, 2):
         impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
-        assert impl.set_option(cb.OPT_HIO_CHUNK, chunk)
+        assert impl.set_option(cb.OPT_HIO_CHUNK, chunk) and impl.set_option(cb.OPT_HIO_CLUSTER, 0)
         x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
         est = torch.empty_like(x)
         assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, 12, beta=0.9, sw_every=5, estimate=est)
@@ -803,13 +806,15 @@ def test_hio_large_chunking_is_exact(tb):
             np.testing.assert_array_equal(a, b)
 
 
-@pytest.mark.parametrize("L", [256, 512])
-def test_hio_large_shrinkwrap_support_vs_oracle(tb, L):
-    """Support masks after shrinkwrap updates differ in <= 0.1% of pixels."""
+@pytest.mark.parametrize("L,cluster", [(256, 0), (512, 0), (256, 8)])
+def test_hio_large_shrinkwrap_support_vs_oracle(tb, L, cluster):
+    """Support masks after shrinkwrap updates differ in <= 0.1% of pixels
+    (line passes; at 256 also the cluster kernel, 8 CTAs per pattern)."""
     torch, cb = tb
     B = 2
     A, S0, x0 = _hio_inputs(L, B, seed=11)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
     x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
     assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, 20, beta=0.9, sw_every=10) and impl.Sync()
     xo, So, _ = O.hio_shrinkwrap(x0, A, S0, L, B, 20, 0.9, sw_every=10)
@@ -834,16 +839,19 @@ def test_hio_large_estimate_only(tb):
     np.testing.assert_array_equal(host(x), x0.ravel())
 
 
-def test_hio_large_full_run_rfactor(tb):
+@pytest.mark.parametrize("cluster", [0, 8])
+def test_hio_large_full_run_rfactor(tb, cluster):
     """The uneven-size configuration's 256x256 bucket shape: HIO beta 0.9, 100
     iterations, shrinkwrap every 20 (sigma 3 -> 1.5, threshold 0.1), support
-    radius ~0.19 of the side.  Bars as for the 128x128 run: mean R-factor of
-    the reconstructions within 1% (relative) of the float64 oracle's, median
-    per-pattern difference < 3%, worst < 25%."""
+    radius ~0.19 of the side; line passes (cluster 0) and the cluster kernel
+    (8 CTAs per pattern).  Bars as for the 128x128 run (chaotic iteration):
+    mean R-factor of the reconstructions within 2% (relative) of the float64
+    oracle's, median per-pattern difference < 4%, worst < 25%."""
     torch, cb = tb
     L, B = 256, 8
     A, S0, x0 = _hio_inputs(L, B, seed=2)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
     x, S, Ad = dev(torch, x0.ravel()), dev(torch, S0.ravel()), dev(torch, A.ravel())
     est = torch.empty_like(x)
     assert impl.hio_shrinkwrap(x, Ad, S, B, 100, beta=0.9, sw_every=20, sigma_start=3.0, sigma_end=1.5,
@@ -859,13 +867,116 @@ def test_hio_large_full_run_rfactor(tb):
     assert np.all(e[host(S).reshape(B, -1) < 0.5] == 0)
 
 
+# ---- one pattern over a thread-block cluster -----------------------------------------------
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+@pytest.mark.parametrize("pos", [False, True])
+def test_hio_cluster_128_equals_tmem_kernel_bitwise(tb, cluster, pos):
+    """At 128^2 the cluster kernel runs the tensor-memory kernel's line
+    transforms and per-element steps in the same order, with the rows and
+    the columns of a pattern owned by different CTAs: x, the support and the
+    estimate are the same bits for 2, 4 and 8 CTAs per pattern, through two
+    shrinkwrap updates."""
+    torch, cb = tb
+    L, B = 128, 3
+    A, S0, x0 = _hio_inputs(L, B, seed=40 + cluster)
+    out = []
+    for cl in (0, cluster):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert impl.set_option(cb.OPT_TMEM, 1) and impl.set_option(cb.OPT_HIO_CLUSTER, cl)
+        x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        est = torch.empty_like(x)
+        assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, 25, beta=0.9, sw_every=10, positivity=pos,
+                                   estimate=est)
+        assert impl.Sync()
+        out.append((host(x), host(S), host(est)))
+        impl.close()
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("cluster,pos", [(8, False), (16, True)])
+def test_hio_cluster_256_vs_oracle(tb, cluster, pos):
+    """256^2 over 8 or 16 CTAs per pattern: HIO iterations (no support
+    update) against the oracle, 1e-5 relative L2 per iteration."""
+    torch, cb = tb
+    L, B, iters = 256, 2, 3
+    A, S0, x0 = _hio_inputs(L, B, seed=50 + cluster)
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
+    x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+    assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=0, positivity=pos)
+    assert impl.Sync()
+    xo, So, _ = O.hio_shrinkwrap(x0, A, S0, L, B, iters, 0.9, sw_every=0, positivity=pos)
+    assert O.rel_l2(host(x), xo) < FP32_DM_TOL * iters
+    np.testing.assert_array_equal(host(S), So.astype(np.float32))
+
+
+def test_hio_cluster_256_sizes_bitwise(tb):
+    """8 and 16 CTAs per 256^2 pattern run the same line transforms: the same
+    bits of x, the support and the estimate through two shrinkwrap updates."""
+    torch, cb = tb
+    L, B = 256, 3
+    A, S0, x0 = _hio_inputs(L, B, seed=61)
+    out = []
+    for cl in (8, 16):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert impl.set_option(cb.OPT_HIO_CLUSTER, cl)
+        x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        est = torch.empty_like(x)
+        assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, 25, beta=0.9, sw_every=10, estimate=est)
+        assert impl.Sync()
+        out.append((host(x), host(S), host(est)))
+        impl.close()
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("B", [4, 40])
+def test_autotune_hio_cluster_bitwise(tb, B):
+    """With CPRA_B200_OPT_AUTOTUNE and the automatic cluster choice, a 128^2
+    call measures one CTA per pattern against clusters of 2, 4 and 8 (on
+    copies of x and S); whatever it picks, x, the support and the estimate
+    are the bits of the tensor-memory kernel, on the measuring call and on
+    the cached one; the automatic choice without the tuner gives them too."""
+    torch, cb = tb
+    L, iters, sw = 128, 12, 5
+    A, S0, x0 = _hio_inputs(L, B, seed=90 + B)
+    res = []
+    for tune, cluster in ((0, 0), (0, 1), (1, 1)):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert impl.set_option(cb.OPT_AUTOTUNE, tune) and impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
+        for _ in range(2 if tune else 1):
+            x, Sd = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+            est = torch.empty_like(x)
+            assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), Sd, B, iters, beta=0.9, sw_every=sw, estimate=est)
+            assert impl.Sync()
+            res.append((host(x), host(Sd), host(est)))
+        impl.close()
+    for r in res[1:]:
+        for a, b in zip(r, res[0]):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_hio_cluster_option_checked(tb):
+    torch, cb = tb
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 128, 128, 1, 1)
+    assert impl.get_option(cb.OPT_HIO_CLUSTER) == 1   # automatic by default
+    for v in (0, 1, 2, 4, 8, 16):
+        assert impl.set_option(cb.OPT_HIO_CLUSTER, v)
+        assert impl.get_option(cb.OPT_HIO_CLUSTER) == v
+    for v in (-1, 3, 32):
+        assert not impl.set_option(cb.OPT_HIO_CLUSTER, v)
+    impl.close()
+
+
 # ---- uneven sizes in one call --------------------------------------------------------------
-@pytest.mark.parametrize("own_sigma", [False, True])
-def test_hio_batched_matches_per_size_calls(tb, own_sigma):
+@pytest.mark.parametrize("own_sigma,cluster", [(False, 0), (True, 0), (True, 8)])
+def test_hio_batched_matches_per_size_calls(tb, own_sigma, cluster):
     """Each bucket of the uneven-size call gives the same bits as a
     single-size call with the same patterns (the buckets only share the
     device, not data); with own_sigma each bucket has its own blur schedule
-    (3 -> 1.5 px times side / 128) and the CUDA backend's DataConstraint."""
+    (3 -> 1.5 px times side / 128) and the CUDA backend's DataConstraint;
+    with cluster 8 the 128 and 256 buckets run on the cluster kernel."""
     torch, cb = tb
     sizes = [(64, 3), (128, 2), (256, 2), (512, 3)]
     iters, sw = 12, 5
@@ -882,11 +993,13 @@ def test_hio_batched_matches_per_size_calls(tb, own_sigma):
         buckets.append(b)
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 64, 64, 1, 1)
     assert impl.set_option(cb.OPT_DATA_MODE, 1 if own_sigma else 0)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, cluster)
     assert impl.hio_batched(buckets, iters, beta=0.9, sw_every=sw) and impl.Sync()
     for (L, B), b in zip(sizes, buckets):
         A, S0, x0 = data[L]
         one = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
         assert one.set_option(cb.OPT_DATA_MODE, 1 if own_sigma else 0)
+        assert one.set_option(cb.OPT_HIO_CLUSTER, cluster)
         x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
         est = torch.empty_like(x)
         assert one.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=sw,
@@ -1218,6 +1331,7 @@ def test_autotune_constraint3d_and_hio_chunk_bitwise(tb):
     for tune, chunk in ((0, 4), (0, 2), (0, 1), (1, 0)):
         impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
         assert impl.set_option(cb.OPT_AUTOTUNE, tune) and impl.set_option(cb.OPT_HIO_CHUNK, chunk)
+        assert impl.set_option(cb.OPT_HIO_CLUSTER, 0)   # the line passes
         for _ in range(2 if tune else 1):
             x, Sd = dev(torch, x0.ravel()), dev(torch, S0.ravel())
             est = torch.empty_like(x)
