@@ -22,7 +22,7 @@ __all__ = [
     "IMPL_TYPE", "CpraB200Error", "B200Impl", "NewCpraImpl", "library_path", "lib",
     "OK", "EARG", "ECUDA", "EUNSUP", "OPT_FUSION", "OPT_SPACE_MODE", "OPT_DATA_MODE", "OPT_SEED",
     "OPT_KERNEL_TIMING", "OPT_HIO_CHUNK", "OPT_GRAPH", "OPT_LANES", "OPT_IO_CHUNK", "OPT_AUTOTUNE", "OPT_TMEM",
-    "OPT_FUSED3D", "OPT_HIO_CLUSTER",
+    "OPT_FUSED3D", "OPT_HIO_CLUSTER", "OPT_FAILURE_TEST",
 ]
 
 OK, EARG, ECUDA, EUNSUP = 0, 1, 2, 3
@@ -34,6 +34,7 @@ OPT_AUTOTUNE = 10
 OPT_TMEM = 11
 OPT_FUSED3D = 12
 OPT_HIO_CLUSTER = 13
+OPT_FAILURE_TEST = 14
 
 _HERE = Path(__file__).resolve().parent
 

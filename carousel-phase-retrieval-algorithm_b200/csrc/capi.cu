@@ -260,6 +260,9 @@ struct cpra_b200_ctx {
     // every Sync reads it (and clears it when set)
     int* dev_err = nullptr;
     bool err_pending = false;
+    // CPRA_B200_OPT_FAILURE_TEST: the next cluster HIO launch withholds one
+    // CTA's first blocks (its peers' waits run out)
+    bool failure_test = false;
 
     size_t esize() const { return dbl ? sizeof(double) : sizeof(float); }
     size_t csize() const { return 2 * esize(); }
@@ -795,6 +798,7 @@ int cpra_b200_set_option(cpra_b200_ctx* c, int option, int64_t value) {
                 return fail(CPRA_B200_EARG, "hio cluster must be 0, 1, 2, 4, 8 or 16");
             c->hio_cluster = (int)value;
             break;
+        case CPRA_B200_OPT_FAILURE_TEST: c->failure_test = value != 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;
@@ -1372,6 +1376,8 @@ int hio_enqueue(cpra_b200_ctx* c, const HioJob& j, const HioParams& h, uint64_t 
     if (r) return r;
     if (const int cl = hio_cluster_for(c, j.L, j.batch)) {
         a.err = c->dev_err;
+        a.withhold = c->failure_test ? 1 : 0;
+        c->failure_test = false;
         c->err_pending = true;
         CPRA_CHECK_CUDA(launch_hio_cluster(a, cl, twiddles(c, j.L), st), "hio_shrinkwrap");
         return CPRA_B200_OK;
@@ -1990,6 +1996,7 @@ int cpra_b200_get_option(cpra_b200_ctx* c, int option, int64_t* value) {
         case CPRA_B200_OPT_TMEM: *value = c->tmem ? 1 : 0; break;
         case CPRA_B200_OPT_FUSED3D: *value = c->fused3d ? 1 : 0; break;
         case CPRA_B200_OPT_HIO_CLUSTER: *value = c->hio_cluster; break;
+        case CPRA_B200_OPT_FAILURE_TEST: *value = c->failure_test ? 1 : 0; break;
         default: return fail(CPRA_B200_EARG, "unknown option");
     }
     return CPRA_B200_OK;

@@ -182,6 +182,7 @@ struct HioArgs {
     double beta, threshold;
     int tmem = 1;  // 128 x 128: the half of x that k_hio sends through L2 stays in tensor memory
     int* err = nullptr;  // cluster kernel: device word set to 1 when a wait for a peer's data ran out
+    int withhold = 0;    // cluster kernel, failure test: the first CTA withholds its first blocks
 };
 bool hio_fused_supported(bool dbl, uint64_t M, uint64_t N);
 cudaError_t launch_hio_iterations(bool dbl, const HioArgs& a, const void* tw, cudaStream_t st);

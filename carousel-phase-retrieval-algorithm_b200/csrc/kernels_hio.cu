@@ -42,6 +42,7 @@ struct HioDev {
     const Cx<float>* tw;
     const float* blur;  // [updates][L]: g at the frequency of each (D-shifted) row/column index
     int* err;           // cluster kernel: set to 1 when a wait for a peer's data ran out
+    int withhold;       // cluster kernel, failure test: CTA 0 sends none of its first row blocks
     float scale, beta, thresh;
     int iters, sw_every, positivity, data_mode;
 };
@@ -571,7 +572,9 @@ __global__ void __launch_bounds__(ClGeom<L, CL>::NT, 1) k_hio_cl(const HioDev p)
         for (int i = 0; i < R; ++i) rw[q + TPL * brev<R>(i)] = v[i];
         fence_proxy_async_smem();
         __syncwarp();
-        if (q < CL && ok)
+        // (failure test: the launch's first CTA withholds its first phase's
+        // blocks, so its peers' waits for them run out)
+        if (q < CL && ok && !(p.withhold && blockIdx.x == 0 && done_c == 0))
             bulk_copy_to_cta(cluster_map(cb + 8u * (uint32_t)(grow * CP), (uint32_t)q),
                              rb + 8u * (uint32_t)(row * LS + q * RPC), G::BLOCK_BYTES, cluster_map(mb_c, (uint32_t)q));
     };
@@ -760,6 +763,7 @@ HioDev hio_dev(const HioArgs& a, const void* tw) {
     d.tw = (const Cx<float>*)tw;
     d.blur = (const float*)a.blur;
     d.err = a.err;
+    d.withhold = a.withhold;
     d.scale = 1.0f / (float)(a.M * a.N);
     d.beta = (float)a.beta;
     d.thresh = (float)a.threshold;

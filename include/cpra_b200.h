@@ -94,6 +94,11 @@ extern "C" {
                                     difference map gives the same results either way; HIO with 1 splits
                                     each line over 8 threads (4 with 0), as the 128 x 128 operator
                                     transforms do, and agrees with 0 to rounding, not bit for bit. */
+#define CPRA_B200_OPT_FAILURE_TEST 14 /* test of the cluster kernel's bounded waits: 1 makes the next cluster
+                                    HIO launch withhold one CTA's first row blocks, so that its peers'
+                                    waits run out after a second; the launch is marked failed (the next
+                                    cpra_b200_sync returns CPRA_B200_ECUDA), the context stays usable.
+                                    Cleared by that launch. */
 #define CPRA_B200_OPT_HIO_CLUSTER 13 /* cpra_b200_hio_shrinkwrap and cpra_b200_hio_batched: each pattern of
                                     side 128 or 256 spread over a thread-block cluster of this many CTAs
                                     (128: 2, 4 or 8; 256: 8 or 16), the plane exchanged between the CTAs'

@@ -957,6 +957,38 @@ def test_autotune_hio_cluster_bitwise(tb, B):
             np.testing.assert_array_equal(a, b)
 
 
+def test_hio_cluster_wait_runs_out_reports_error(tb):
+    """The cluster kernel's waits for its peers' blocks are bounded.  With the
+    failure test armed the launch's first CTA withholds its first row blocks;
+    its peers' waits run out after about a second, the launch marks itself
+    failed and Sync raises.  The context stays usable: the same call again
+    gives the bits of a fresh context."""
+    import time
+    torch, cb = tb
+    L, B, iters = 128, 2, 3
+    A, S0, x0 = _hio_inputs(L, B, seed=71)
+    Ad = dev(torch, A.ravel())
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, 8) and impl.set_option(cb.OPT_FAILURE_TEST, 1)
+    x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+    t0 = time.monotonic()
+    assert impl.hio_shrinkwrap(x, Ad, S, B, iters, beta=0.9, sw_every=0)
+    with pytest.raises(cb.CpraB200Error, match="ran out"):
+        impl.Sync()
+    assert 0.9 < time.monotonic() - t0 < 60
+    assert impl.get_option(cb.OPT_FAILURE_TEST) == 0   # cleared by the launch
+    x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+    assert impl.hio_shrinkwrap(x, Ad, S, B, iters, beta=0.9, sw_every=0) and impl.Sync()
+    fresh = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert fresh.set_option(cb.OPT_HIO_CLUSTER, 8)
+    xf, Sf = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+    assert fresh.hio_shrinkwrap(xf, Ad, Sf, B, iters, beta=0.9, sw_every=0) and fresh.Sync()
+    np.testing.assert_array_equal(host(x), host(xf))
+    np.testing.assert_array_equal(host(S), host(Sf))
+    impl.close()
+    fresh.close()
+
+
 def test_hio_cluster_option_checked(tb):
     torch, cb = tb
     impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, 128, 128, 1, 1)
