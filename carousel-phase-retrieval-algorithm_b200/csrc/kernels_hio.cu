@@ -453,7 +453,8 @@ size_t hio_tm_smem_bytes() {
 // the rows of a half-warp 4 apart at TPL 8, so its slots fall on distinct
 // bank pairs); the column buffer [L][CP], row-major over the owned columns
 // (CP = RPC + 2: a half-warp's two columns and 8 ranks on distinct bank
-// pairs at TPL 8; rows 16-byte aligned for the copies); A of the owned
+// pairs, at TPL 16 with the two columns interleaved lane by lane; rows
+// 16-byte aligned for the copies); A of the owned
 // columns, column-major (pitch ACP); twiddles; a blur table row; maxima.
 template <int L, int CL>
 struct ClGeom {
@@ -487,6 +488,22 @@ struct ClGeom {
         else
             return t / TPL;
     }
+    // the column of thread t in the column phase, and its rank there: at
+    // TPL 16 a warp holds two columns interleaved lane by lane, so a
+    // half-warp reads 8 ranks of two columns, 16 distinct bank pairs at the
+    // even pitch CP (one column of 16 ranks per half-warp would collide 2-way)
+    __device__ __forceinline__ static int col_of(int t) {
+        if constexpr (TPL == 16)
+            return 2 * (t >> 5) + (t & 1);
+        else
+            return t / TPL;
+    }
+    __device__ __forceinline__ static int col_rank(int t) {
+        if constexpr (TPL == 16)
+            return (t & 31) >> 1;
+        else
+            return t % TPL;
+    }
 };
 
 // a second: far above any phase of a healthy launch
@@ -508,7 +525,8 @@ __global__ void __launch_bounds__(ClGeom<L, CL>::NT, 1) k_hio_cl(const HioDev p)
     float* cmax = red + G::WARPS;  // [CL] every CTA's maximum
     const int t = threadIdx.x, q = t % TPL, warp = t >> 5;
     const int row = G::row_of(t);  // this CTA's row in the row phases
-    const int cl = t / TPL;        // this CTA's column in the column phase
+    const int cl = G::col_of(t);   // this CTA's column in the column phase
+    const int qc = G::col_rank(t);  // and the thread's rank in it
     const int rank = (int)cluster_ctarank();
     const int grow = rank * RPC + row, gcol = rank * RPC + cl;
     const uint32_t base = smem_addr_u32(smem_raw);
@@ -585,16 +603,16 @@ __global__ void __launch_bounds__(ClGeom<L, CL>::NT, 1) k_hio_cl(const HioDev p)
         Cx<float>* col = cbuf + cl;
         Cx<float> v[R];
 #pragma unroll
-        for (int k = 0; k < R; ++k) v[k] = col[(q + TPL * k) * CP];
+        for (int k = 0; k < R; ++k) v[k] = col[(qc + TPL * k) * CP];
         Cx<float> o[J][TPL];
-        F::template natural_to_split<false>(v, o, col, CP, tw, q);
+        F::template natural_to_split<false>(v, o, col, CP, tw, qc);
 #pragma unroll
         for (int j = 0; j < J; ++j)
 #pragma unroll
-            for (int s = 0; s < TPL; ++s) o[j][s] = op(o[j][s], pos(j, s));
-        F::template split_to_natural<true>(o, v, col, CP, tw, q);
+            for (int s = 0; s < TPL; ++s) o[j][s] = op(o[j][s], qc + TPL * j + R * s);
+        F::template split_to_natural<true>(o, v, col, CP, tw, qc);
 #pragma unroll
-        for (int i = 0; i < R; ++i) col[(q + TPL * brev<R>(i)) * CP] = v[i];
+        for (int i = 0; i < R; ++i) col[(qc + TPL * brev<R>(i)) * CP] = v[i];
         fence_proxy_async_smem();
         __syncthreads();
         if (t < L && ok) {
