@@ -957,6 +957,47 @@ def test_autotune_hio_cluster_bitwise(tb, B):
             np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("B,iters,sw,cluster", [(2, 0, 0, 8), (3, 20, 10, 4), (18, 10, 5, 1), (1, 7, 7, 2)])
+def test_hio_cluster_128_edges_bitwise(tb, B, iters, sw, cluster):
+    """Edge cases of the cluster kernel against the one-CTA tensor-memory
+    kernel, bit for bit: the estimate alone (no iteration), a support update
+    after the last iteration (then the estimate), the automatic choice at its
+    boundary (18 patterns x 8 CTAs = 144 SMs), a single pattern."""
+    torch, cb = tb
+    L = 128
+    A, S0, x0 = _hio_inputs(L, B, seed=300 + B + iters)
+    out = []
+    for cl in (0, cluster):
+        impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+        assert impl.set_option(cb.OPT_HIO_CLUSTER, cl)
+        x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+        est = torch.empty_like(x)
+        assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, iters, beta=0.9, sw_every=sw, estimate=est)
+        assert impl.Sync()
+        out.append((host(x), host(S), host(est)))
+        impl.close()
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_hio_cluster_256_estimate_only_vs_oracle(tb):
+    """iters = 0 with an estimate at 256^2 over 8 CTAs: S (.) P_M(x) of the
+    input within the per-iteration bar, x untouched, S binarised."""
+    torch, cb = tb
+    L, B = 256, 2
+    A, S0, x0 = _hio_inputs(L, B, seed=17)
+    S0 = S0 * 0.75
+    impl = cb.NewCpraImpl(cb.IMPL_TYPE.B200, L, L, 1, B)
+    assert impl.set_option(cb.OPT_HIO_CLUSTER, 8)
+    x, S = dev(torch, x0.ravel()), dev(torch, S0.ravel())
+    est = torch.empty_like(x)
+    assert impl.hio_shrinkwrap(x, dev(torch, A.ravel()), S, B, 0, sw_every=0, estimate=est) and impl.Sync()
+    _, _, eo = O.hio_shrinkwrap(x0, A, (S0 > 0.5).astype(np.float32), L, B, 0, 0.9, sw_every=0)
+    assert O.rel_l2(host(est), eo) < FP32_DM_TOL
+    np.testing.assert_array_equal(host(S), (S0 > 0.5).astype(np.float32).ravel())
+    np.testing.assert_array_equal(host(x), x0.ravel())
+
+
 def test_hio_cluster_wait_runs_out_reports_error(tb):
     """The cluster kernel's waits for its peers' blocks are bounded.  With the
     failure test armed the launch's first CTA withholds its first row blocks;
