@@ -8,7 +8,8 @@
 // Besides one wrapper per operator it restates the reference's driver loops
 // (src/CPRA_MKL.cpp:35-140) as functions that take seeded initial guesses
 // instead of the reference's unseeded Initialize() fill, so that identical
-// inputs can be given to the oracle, this build and the B200 backend.
+// inputs can be given to the numpy oracle, these compiled reference operators
+// and the B200 backend.
 // The reference reaches MKL_Impl.hpp through CPRA.hpp, which includes these
 // first (include/CPRA.hpp:2-5); MKL_Impl.hpp relies on them.
 #include <cstddef>
