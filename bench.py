@@ -54,6 +54,10 @@ def parse():
                          "profiling runs); ops2d / ops3d: one launch of each kernel family (for ncu captures)")
     ap.add_argument("--uneven-counts", default="192,192,96,32", help="patterns at 64^2,128^2,256^2,512^2")
     ap.add_argument("--uneven-iters", type=int, default=100)
+    # plain2d case: the plain 2D configuration by default; other sides and counts for profiling runs
+    ap.add_argument("--plain2d-patterns", type=int, default=16)
+    ap.add_argument("--plain2d-side", type=int, default=128, choices=[64, 128, 256, 512])
+    ap.add_argument("--plain2d-iters", type=int, default=200)
     # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
     ap.add_argument("--angle-step", type=float, default=1.0, help="degrees between projections")
     ap.add_argument("--photons", type=float, default=1e8)
@@ -339,7 +343,8 @@ def main():
             print(json.dumps(out), flush=True)
         return
     if a.case == "plain2d":
-        out = plain2d(torch, cpra_b200, torch.device("cuda", local), reps=max(1, a.steps))
+        out = plain2d(torch, cpra_b200, torch.device("cuda", local), B=a.plain2d_patterns, n=a.plain2d_side,
+                      iters=a.plain2d_iters, reps=max(1, a.steps))
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -878,7 +883,7 @@ def plain2d(torch, cpra_b200, dev, B=16, n=128, iters=200, sw_every=20, reps=3):
     one CTA per pattern (the tensor-memory kernel: 16 SMs).  Both write the
     same bits."""
     from cpra_b200 import synth
-    d = synth.patterns_2d(count=B, n=n, radius=24, seed=0)
+    d = synth.patterns_2d(count=B, n=n, radius=int(0.19 * n), seed=0)   # 24 px at 128^2
     S0 = synth.autocorrelation_support(d["A"])
     x0 = synth.random_phase_start(d["A"], seed=1)
     A = torch.from_numpy(d["A"].ravel()).to(dev)
@@ -912,8 +917,9 @@ def plain2d(torch, cpra_b200, dev, B=16, n=128, iters=200, sw_every=20, reps=3):
     return {"workload": f"plain 2D HIO + shrinkwrap: {B} x {n}^2, {iters} iterations, shrinkwrap every {sw_every}",
             "value": a["value"], "unit": METRIC, "ms": a["ms"], "rfactor_mean": a["rfactor_mean"],
             "rfactor_median": a["rfactor_median"], "one_cta": out["one_cta"],
-            "note": "automatic: each pattern over a cluster of 8 CTAs (rows and columns exchanged between the "
-                    "CTAs' shared memories by bulk copies); one_cta: one CTA per pattern, 16 of the SMs"}
+            "note": "automatic: at 16 x 128^2 each pattern over a cluster of 8 CTAs (rows and columns exchanged "
+                    "between the CTAs' shared memories by bulk copies); one_cta: one CTA per pattern at 128^2 (16 "
+                    "of the SMs), line passes at 256^2 and 512^2"}
 
 
 UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns): 512 patterns, 18,612,224 pixels
