@@ -82,7 +82,9 @@ extern "C" {
                                     operator kernels (one iteration each; CPRA_B200_OPT_FUSED3D is then
                                     ignored there); for cpra_b200_hio_shrinkwrap at 256 and 512 with
                                     CPRA_B200_OPT_HIO_CHUNK 0, the line passes' chunk among the whole batch,
-                                    a half and a quarter (min(iters, 20) iterations each).  No measurement
+                                    a half and a quarter (min(iters, 20) iterations each); for
+                                    cpra_b200_hio_shrinkwrap at 128 with CPRA_B200_OPT_HIO_CLUSTER 1, one
+                                    CTA per pattern against clusters of 2, 4 and 8.  No measurement
                                     during a stream capture or when the copy cannot be allocated. */
 #define CPRA_B200_OPT_FUSED3D 12   /* 1: cpra_b200_constraint3d and the recognised 3D difference-map iteration
                                     run as fused axis passes (5 and 10 passes per iteration); 0 (default):
