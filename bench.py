@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--plain2d-patterns", type=int, default=16)
     ap.add_argument("--plain2d-side", type=int, default=128, choices=[64, 128, 256, 512])
     ap.add_argument("--plain2d-iters", type=int, default=200)
+    # ops3d case: the volume side and slices of the 3D kernel families (default 256^3, 180 at 1 deg)
+    ap.add_argument("--ops3d-size", type=int, default=256)
+    ap.add_argument("--ops3d-angles", type=int, default=180)
+    ap.add_argument("--ops3d-step", type=float, default=1.0, help="degrees between the ops3d slices")
     # carousel3d case: the synthetic volume and the refinement (defaults: the 256^3 configuration)
     ap.add_argument("--angle-step", type=float, default=1.0, help="degrees between projections")
     ap.add_argument("--photons", type=float, default=1e8)
@@ -349,7 +353,8 @@ def main():
             print(json.dumps(out), flush=True)
         return
     if a.case in ("ops2d", "ops3d"):
-        out = kernel_families(torch, cpra_b200, torch.device("cuda", local), a.case)
+        out = kernel_families(torch, cpra_b200, torch.device("cuda", local), a.case, n3=a.ops3d_size,
+                              p3=a.ops3d_angles, step3=a.ops3d_step)
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -738,7 +743,7 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     x = torch.empty_like(x0)
     err = np.zeros(P * B, np.float32)
     st = torch.cuda.ExternalStream(impl.stream(), device=dev)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
 
     def run2d(e, it, timing=False):
         x.copy_(x0)
@@ -806,11 +811,14 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
     ev[0].record(st3)
     impl2.Forward2D(planes)
     impl2.Sync()
-    slices = planes.view(P, n, n).transpose(1, 2).contiguous().view(-1)
+    with torch.cuda.stream(st3):
+        slices = planes.view(P, n, n).transpose(1, 2).contiguous().view(-1)
+    ev[2].record(st3)
     impl3.Complex2DTo3DInterpolation(slices, V, d["angles_nominal"], n, n, P, n)
     ev[1].record(st3)
     impl3.Sync()
-    merge_ms = ev[0].elapsed_time(ev[1])
+    merge_prep_ms = ev[0].elapsed_time(ev[2])   # Forward2D of the planes and their transpose
+    merge_ms = ev[2].elapsed_time(ev[1])        # the trilinear merge kernel
     a_true, r_true = d["angles_true"].double(), d["rot_true"].double()
 
     def rms_deg(a, r):
@@ -859,7 +867,7 @@ def carousel3d_adjoint(torch, cpra_b200, dev, n=256, P=180, B=16, epi=10, iters=
                     "convergence_error_median": float(np.median(err))},
         "best_start": {"index": best, "mean_rfactor": float(scores[best]),
                        "median_rfactor_over_starts": float(np.median(scores))},
-        "merge_ms": merge_ms,
+        "merge_ms": merge_ms, "merge_prep_ms": merge_prep_ms,
         "refine": {"steps": refine_steps, "ms": refine_ms, "ms_per_step": refine_ms / refine_steps,
                    "parameters": "real-space volume, tilt and in-plane rotation per pattern (Adam; volume lr 1e-3, "
                                  "angles lr 2e-4 rad)",
@@ -926,12 +934,13 @@ UNEVEN_SIZES = ((64, 192), (128, 192), (256, 96), (512, 32))  # (side, patterns)
 HIO_BYTES_PER_PIXEL = 24  # read+write x (complex64) + read A, S (float32) per HIO pattern-iteration
 
 
-def kernel_families(torch, cpra_b200, dev, case):
+def kernel_families(torch, cpra_b200, dev, case, n3=256, p3=180, step3=1.0):
     """One launch of each kernel family on inputs larger than L2, for ncu
     captures (no timing here).  ops2d: the per-operator 2D kernels on 2000
     planes of 128^2 (262 MB per complex array): Forward2D, Backward2D,
     SpaceConstraint, DataConstraint (real and complex), MergeAddData,
-    Normalization, FFTShift2D, ConvergeError.  ops3d at 256^3 with 180 slices:
+    Normalization, FFTShift2D, ConvergeError.  ops3d on an n3^3 volume with p3
+    slices step3 degrees apart (default 256^3, 180 at 1 degree):
     the trilinear merge, the slice operator's loss, gradients and adjoint, the
     slice operator, one real-space refinement step (transform, slice, adjoints,
     transform adjoint, Adam), Forward3D, the benchmark's 3D step on the
@@ -962,11 +971,11 @@ def kernel_families(torch, cpra_b200, dev, case):
         impl.Sync()
         impl.close()
     else:
-        n, P = 256, 180
+        n, P = n3, p3
         vox = n ** 3
         impl3 = cpra_b200.B200Impl(n, n, n, 1)
         impl3.set_option(cpra_b200.OPT_FUSION, 0)
-        ang = torch.deg2rad(torch.arange(P, device=dev, dtype=torch.float32))
+        ang = torch.deg2rad(torch.arange(P, device=dev, dtype=torch.float32) * step3)
         rot = torch.zeros(P, device=dev)
         src = torch.rand(P * n * n, dtype=torch.complex64, device=dev, generator=g)
         V = torch.zeros(vox, dtype=torch.complex64, device=dev)
