@@ -13,6 +13,8 @@
 #pragma once
 #include <cstdint>
 
+#include "cpra_common.cuh"
+
 namespace cpra_b200 {
 
 constexpr int ANGLE_TABLE_MAX = 4096;  // slices; above this the gathers visit every slice
@@ -23,6 +25,7 @@ struct AngleTable {
     const int* idx;     // [P] slice index
     const double2* sc;  // [P] (sin a, cos a) of that slice
     int64_t P;
+    unsigned long long* next;  // work counter of the gather that reads the table (zeroed before its launch)
 };
 
 // byte offsets of the three arrays in a table buffer of angle_table_bytes(P)
@@ -30,12 +33,53 @@ __host__ __device__ inline uint64_t angle_table_idx_offset(uint64_t P) { return 
 __host__ __device__ inline uint64_t angle_table_sc_offset(uint64_t P) {
     return angle_table_idx_offset(P) + (P * 4 + 255) / 256 * 256;
 }
-__host__ __device__ inline uint64_t angle_table_bytes(uint64_t P) { return angle_table_sc_offset(P) + P * 16; }
+__host__ __device__ inline uint64_t angle_table_next_offset(uint64_t P) {
+    return angle_table_sc_offset(P) + (P * 16 + 255) / 256 * 256;
+}
+__host__ __device__ inline uint64_t angle_table_bytes(uint64_t P) { return angle_table_next_offset(P) + 256; }
 
 inline AngleTable angle_table_view(void* buf, int64_t P) {
     char* b = static_cast<char*>(buf);
     return AngleTable{reinterpret_cast<const double*>(b), reinterpret_cast<const int*>(b + angle_table_idx_offset(P)),
-                      reinterpret_cast<const double2*>(b + angle_table_sc_offset(P)), P};
+                      reinterpret_cast<const double2*>(b + angle_table_sc_offset(P)), P,
+                      reinterpret_cast<unsigned long long*>(b + angle_table_next_offset(P))};
+}
+
+// The voxels of a gather over slices cost very different amounts (a voxel
+// near the tilt axis is near many slices, a far one near few), so they are
+// handed out dynamically: each warp takes 32 * GATHER_VOXELS_PER_LANE
+// consecutive voxel indices from the counter at a time until the volume is
+// done, and calls f(i) for each of its lanes' indices.  Every voxel is still
+// computed by one thread with the same arithmetic.  Launch exactly the
+// resident CTAs (the counter replaces the grid-stride loop) with the counter
+// zeroed on the same stream; all 32 lanes of every warp take part.
+constexpr int GATHER_VOXELS_PER_LANE = 4;
+template <class Fn>
+__device__ __forceinline__ void for_voxels_dynamic(unsigned long long* next, uint64_t total, Fn f) {
+    const int lane = threadIdx.x & 31;
+    constexpr unsigned long long CHUNK = 32ull * GATHER_VOXELS_PER_LANE;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(next, CHUNK);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) return;
+#pragma unroll 1
+        for (int r = 0; r < GATHER_VOXELS_PER_LANE; ++r) {
+            const uint64_t i = base + (uint64_t)r * 32 + (uint64_t)lane;
+            if (i < total) f(i);
+        }
+    }
+}
+
+// CTAs of `kernel` resident on the whole device at `threads` per CTA
+template <class K>
+inline unsigned resident_grid(K kernel, unsigned threads, size_t smem = 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, (int)threads, smem) != cudaSuccess || n < 1) {
+        (void)cudaGetLastError();
+        n = 1;
+    }
+    return (unsigned)n * (unsigned)sm_count();
 }
 
 // one block of 1024 threads; dynamic shared memory 12 * N bytes, N the

@@ -260,7 +260,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __re
 
 // the same gather visiting only the slices whose plane passes near the voxel
 // (angle_table.cuh: ordered by tilt, which alone fixes the plane), in
-// direction order
+// direction order; voxels handed out dynamically (their cost varies with
+// the distance from the tilt axis)
 template <typename T>
 __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __restrict__ G, const AngleTable at,
                                                                  const Orient<T>* __restrict__ tab,
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __
                                                                  int64_t L) {
     const uint64_t total = (uint64_t)L * N * M;
     const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
-    for (uint64_t i = tid_g(); i < total; i += str_g()) {
+    for_voxels_dynamic(at.next, total, [&](uint64_t i) {
         const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
         const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
         T re = T(0), im = T(0);
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __
             gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
         });
         gV[i] = Cx<T>{re, im};
-    }
+    });
 }
 
 // Adam (Kingma & Ba, 2015), in the form with bias-corrected step and
@@ -395,8 +396,10 @@ cudaError_t slice_loss_grad_t(const void* V, const void* ang, const void* tab, c
         e = launch_sort_angles<T>((const T*)ang, (int64_t)p, atab, st);
         if (e != cudaSuccess) return e;
         const AngleTable t = angle_table_view(atab, (int64_t)p);
-        k_slice_adjoint_w<T><<<g, ADJ_THREADS, 0, st>>>((const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n,
-                                                         l);
+        e = cudaMemsetAsync(t.next, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        k_slice_adjoint_w<T><<<resident_grid(k_slice_adjoint_w<T>, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
+            (const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n, l);
         count_launches(2);
         return cudaGetLastError();
     }

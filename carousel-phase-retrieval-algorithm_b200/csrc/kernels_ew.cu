@@ -369,13 +369,13 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d(const Cx<T>* __r
 }
 
 // the same merge visiting only the slices that can reach the voxel
-// (angle_table.cuh), in direction order
+// (angle_table.cuh), in direction order; voxels handed out dynamically
 template <typename T>
 __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d_w(const Cx<T>* __restrict__ src,
                                                                   Cx<T>* __restrict__ dst, const AngleTable tab,
                                                                   int64_t M, int64_t N, int64_t L) {
     const uint64_t total = (uint64_t)M * N * L;
-    for (uint64_t idx = gtid(); idx < total; idx += gstride()) {
+    for_voxels_dynamic(tab.next, total, [&](uint64_t idx) {
         const int64_t y = (int64_t)(idx % M);
         const int64_t x = (int64_t)((idx / M) % N);
         const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d_w(const Cx<T>* _
             merge_slice(src, p, M, N, x, j, l, (T)sa, (T)ca, accx, accy, wsum);
         });
         dst[idx] = (wsum > T(0)) ? Cx<T>{accx / wsum, accy / wsum} : Cx<T>{T(0), T(0)};
-    }
+    });
 }
 
 }  // namespace
@@ -572,12 +572,14 @@ cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const v
                             : launch_sort_angles<float>((const float*)angles, (int64_t)p, atab, st);
         if (e != cudaSuccess) return e;
         const AngleTable t = angle_table_view(atab, (int64_t)p);
+        e = cudaMemsetAsync(t.next, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
         if (dbl)
-            k_complex2d_to_3d_w<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst, t,
-                                                                  (int64_t)m, (int64_t)n, (int64_t)l);
+            k_complex2d_to_3d_w<double><<<resident_grid(k_complex2d_to_3d_w<double>, EW_THREADS), EW_THREADS, 0, st>>>(
+                (const Cx<double>*)src, (Cx<double>*)dst, t, (int64_t)m, (int64_t)n, (int64_t)l);
         else
-            k_complex2d_to_3d_w<float><<<g, EW_THREADS, 0, st>>>((const Cx<float>*)src, (Cx<float>*)dst, t,
-                                                                 (int64_t)m, (int64_t)n, (int64_t)l);
+            k_complex2d_to_3d_w<float><<<resident_grid(k_complex2d_to_3d_w<float>, EW_THREADS), EW_THREADS, 0, st>>>(
+                (const Cx<float>*)src, (Cx<float>*)dst, t, (int64_t)m, (int64_t)n, (int64_t)l);
         count_launches(2);
         return cudaGetLastError();
     }
