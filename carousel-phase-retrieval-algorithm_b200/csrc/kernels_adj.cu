@@ -219,19 +219,21 @@ __device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const
     const T xc = o.cr * u + o.sr * v, yc = o.cr * v - o.sr * u;
     const T ar = absT(o.cr), as = absT(o.sr);
     const T hx = ar + as * T(ADJ_SQRT2) + T(1e-3), hy = as + ar * T(ADJ_SQRT2) + T(1e-3);
-    const int64_t xr0 = floor_i(xc - hx) + 1, xr1 = floor_i(xc + hx);
-    const int64_t yr0 = floor_i(yc - hy) + 1, yr1 = floor_i(yc + hy);
-    for (int64_t xr = xr0; xr <= xr1; ++xr) {
-        const int64_t xIn = xr + N / 2;
-        if (xIn < 0 || xIn >= N) continue;
-        for (int64_t yr = yr0; yr <= yr1; ++yr) {
-            const int64_t yIn = M / 2 - yr;
-            if (yIn < 0 || yIn >= M) continue;
+    // 32-bit window and pixel indices (a slice is at most 2^31 pixels)
+    const int m = (int)M, n = (int)N;
+    const int xr0 = (int)floor_i(xc - hx) + 1, xr1 = (int)floor_i(xc + hx);
+    const int yr0 = (int)floor_i(yc - hy) + 1, yr1 = (int)floor_i(yc + hy);
+    for (int xr = xr0; xr <= xr1; ++xr) {
+        const int xIn = xr + n / 2;
+        if (xIn < 0 || xIn >= n) continue;
+        for (int yr = yr0; yr <= yr1; ++yr) {
+            const int yIn = m / 2 - yr;
+            if (yIn < 0 || yIn >= m) continue;
             T zf, xf, yf, xq, yq;
             pixel_point(o, (T)xr, (T)yr, hl, hn, hm, zf, xf, yf, xq, yq);
             const T wz = T(1) - absT(zf - (T)z), wx = T(1) - absT(xf - (T)x), wy = T(1) - absT(yf - (T)y);
             if (!(wz > T(0)) || !(wx > T(0)) || !(wy > T(0))) continue;
-            const Cx<T> g = Gp[xIn * M + yIn];
+            const Cx<T> g = Gp[xIn * m + yIn];
             const T w = wz * wx * wy;
             re += w * g.x;
             im += w * g.y;
@@ -269,8 +271,19 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __
                                                                  int64_t L) {
     const uint64_t total = (uint64_t)L * N * M;
     const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
+    const bool narrow = total <= 0xffffffffull;  // 32-bit index arithmetic
     for_voxels_dynamic(at.next, total, [&](uint64_t i) {
-        const int64_t y = (int64_t)(i % M), x = (int64_t)((i / M) % N), z = (int64_t)(i / ((uint64_t)M * N));
+        int64_t y, x, z;
+        if (narrow) {
+            const uint32_t i32 = (uint32_t)i, m32 = (uint32_t)M, n32 = (uint32_t)N, q = i32 / m32;
+            y = (int64_t)(i32 - q * m32);
+            x = (int64_t)(q % n32);
+            z = (int64_t)(q / n32);
+        } else {
+            y = (int64_t)(i % M);
+            x = (int64_t)((i / M) % N);
+            z = (int64_t)(i / ((uint64_t)M * N));
+        }
         const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
         T re = T(0), im = T(0);
         for_slices_near(at, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double, double) {
