@@ -22,6 +22,11 @@
 // each support update, whose blur reuses those registers (x is read back in
 // full after it), and after the last iteration.  Optionally the kernel also
 // writes the estimate S (.) P_M(x) of the final x.
+//
+// Two more forms of the same iteration follow: k_hio_tm (128 x 128, 1024
+// threads, x in the SM's tensor memory) and k_hio_cl (128 x 128 and
+// 256 x 256 patterns spread over a thread-block cluster, for batches that
+// would leave SMs idle with one CTA per pattern).
 #include "cpra_internal.h"
 #include "fft2d_cta.cuh"
 #include "ops_ew.cuh"
