@@ -323,19 +323,22 @@ __global__ void k_adam_volume(T* __restrict__ V, const T* __restrict__ g, T* __r
                               uint64_t n, T lr, T b1, T b2, T eps, T c1, T c2) {
     using W = typename Vec16<T>::type;
     constexpr int K = Vec16<T>::N;
-    const uint64_t nv = VEC ? n / K : 0;
-    for (uint64_t i = tid_g(); i < nv; i += str_g()) {
-        W pv = reinterpret_cast<W*>(V)[i], gv = reinterpret_cast<const W*>(g)[i];
-        W mv = reinterpret_cast<W*>(m)[i], vv = reinterpret_cast<W*>(v)[i];
-        T* pp = reinterpret_cast<T*>(&pv);
-        const T* gp = reinterpret_cast<const T*>(&gv);
-        T* mp = reinterpret_cast<T*>(&mv);
-        T* vp = reinterpret_cast<T*>(&vv);
+    uint64_t nv = 0;
+    if constexpr (VEC) {
+        nv = n / K;
+        for (uint64_t i = tid_g(); i < nv; i += str_g()) {
+            W pv = reinterpret_cast<W*>(V)[i], gv = reinterpret_cast<const W*>(g)[i];
+            W mv = reinterpret_cast<W*>(m)[i], vv = reinterpret_cast<W*>(v)[i];
+            T* pp = reinterpret_cast<T*>(&pv);
+            const T* gp = reinterpret_cast<const T*>(&gv);
+            T* mp = reinterpret_cast<T*>(&mv);
+            T* vp = reinterpret_cast<T*>(&vv);
 #pragma unroll
-        for (int k = 0; k < K; ++k) adam_apply(pp[k], gp[k], mp[k], vp[k], lr, b1, b2, eps, c1, c2);
-        reinterpret_cast<W*>(V)[i] = pv;
-        reinterpret_cast<W*>(m)[i] = mv;
-        reinterpret_cast<W*>(v)[i] = vv;
+            for (int k = 0; k < K; ++k) adam_apply(pp[k], gp[k], mp[k], vp[k], lr, b1, b2, eps, c1, c2);
+            reinterpret_cast<W*>(V)[i] = pv;
+            reinterpret_cast<W*>(m)[i] = mv;
+            reinterpret_cast<W*>(v)[i] = vv;
+        }
     }
     for (uint64_t i = nv * K + tid_g(); i < n; i += str_g()) adam_apply(V[i], g[i], m[i], v[i], lr, b1, b2, eps, c1, c2);
 }
