@@ -305,22 +305,31 @@ __global__ void k_real2d_to_3d(const T* __restrict__ src, T* __restrict__ dst, c
 // Coordinates, weights and sums are in the element type T, as the
 // reference's merge kernel computes (CUDA_Impl_Kernel.cuh:68-108); the
 // sines and cosines are evaluated once per slice in double and rounded to T.
+// The part of one slice's contribution that depends only on the voxel's
+// (j, l) and the slice: false if the plane is too far, else its weight wd,
+// the first sampled row y0 and the fraction fy.
 template <typename T>
-__device__ __forceinline__ void merge_slice(const Cx<T>* __restrict__ src, int64_t p, int64_t M, int64_t N,
-                                            int64_t x, T j, T l, T sa, T ca, T& accx, T& accy, T& wsum) {
+__device__ __forceinline__ bool merge_plane(int64_t M, T j, T l, T sa, T ca, T& wd, int64_t& y0, T& fy) {
     const T d = j * ca - l * sa;
-    const T wd = T(1) - (d < T(0) ? -d : d);
-    if (!(wd > T(0))) return;
+    wd = T(1) - (d < T(0) ? -d : d);
+    if (!(wd > T(0))) return false;
     const T yIn = (T)(M / 2) - (j * sa + l * ca);
     const T y0f = floor(yIn);
-    const int64_t y0 = (int64_t)y0f;
-    const T fy = yIn - y0f;
+    y0 = (int64_t)y0f;
+    fy = yIn - y0f;
+    return true;
+}
+// the rest for the voxel column x: the row of the slice at x (`row`, M
+// pixels) sampled linearly at y0 + fy, weighted by wd into the sums
+template <typename T>
+__device__ __forceinline__ void merge_row(const Cx<T>* __restrict__ row, int64_t M, T wd, int64_t y0, T fy, T& accx,
+                                          T& accy, T& wsum) {
     T sx = T(0), sy = T(0), sw = T(0);
     for (int dy = 0; dy < 2; ++dy) {
         const int64_t yy = y0 + dy;
         const T wy = dy ? fy : T(1) - fy;
         if (yy < 0 || yy >= M || wy == T(0)) continue;
-        const Cx<T> v = src[p * M * N + x * M + yy];
+        const Cx<T> v = row[yy];
         sx += wy * v.x;
         sy += wy * v.y;
         sw += wy;
@@ -329,6 +338,14 @@ __device__ __forceinline__ void merge_slice(const Cx<T>* __restrict__ src, int64
     accx += wd * sx;
     accy += wd * sy;
     wsum += wd * sw;
+}
+template <typename T>
+__device__ __forceinline__ void merge_slice(const Cx<T>* __restrict__ src, int64_t p, int64_t M, int64_t N,
+                                            int64_t x, T j, T l, T sa, T ca, T& accx, T& accy, T& wsum) {
+    T wd, fy;
+    int64_t y0;
+    if (!merge_plane(M, j, l, sa, ca, wd, y0, fy)) return;
+    merge_row(src + p * M * N + x * M, M, wd, y0, fy, accx, accy, wsum);
 }
 
 template <typename T>
@@ -369,23 +386,51 @@ __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d(const Cx<T>* __r
 }
 
 // the same merge visiting only the slices that can reach the voxel
-// (angle_table.cuh), in direction order; voxels handed out dynamically
-template <typename T>
+// (angle_table.cuh), in direction order; the work handed out dynamically.
+// A work item is XC voxels along the tilt axis at one (z, y): the slices
+// near them and each slice's plane terms depend only on (z, y), so they are
+// found once for the item, and each voxel sums its slices in the same order
+// as alone.  Consecutive items take consecutive y (coalesced rows and stores).
+template <typename T, int XC>
 __global__ void __launch_bounds__(EW_THREADS) k_complex2d_to_3d_w(const Cx<T>* __restrict__ src,
                                                                   Cx<T>* __restrict__ dst, const AngleTable tab,
                                                                   int64_t M, int64_t N, int64_t L) {
-    const uint64_t total = (uint64_t)M * N * L;
+    const int64_t chunks = N / XC;
+    const uint64_t total = (uint64_t)M * chunks * L;
     for_voxels_dynamic(tab.next, total, [&](uint64_t idx) {
         const int64_t y = (int64_t)(idx % M);
-        const int64_t x = (int64_t)((idx / M) % N);
-        const int64_t z = (int64_t)(idx / ((uint64_t)M * N));
+        const int64_t x0 = (int64_t)((idx / M) % chunks) * XC;
+        const int64_t z = (int64_t)(idx / ((uint64_t)M * chunks));
         const T j = (T)(L / 2 - z), l = (T)(M / 2 - y);
-        T accx = T(0), accy = T(0), wsum = T(0);
+        T accx[XC], accy[XC], wsum[XC];
+#pragma unroll
+        for (int t = 0; t < XC; ++t) accx[t] = accy[t] = wsum[t] = T(0);
         for_slices_near(tab, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double sa, double ca) {
-            merge_slice(src, p, M, N, x, j, l, (T)sa, (T)ca, accx, accy, wsum);
+            T wd, fy;
+            int64_t y0;
+            if (!merge_plane(M, j, l, (T)sa, (T)ca, wd, y0, fy)) return;
+            const Cx<T>* __restrict__ rows = src + p * M * N + x0 * M;
+#pragma unroll
+            for (int t = 0; t < XC; ++t) merge_row(rows + t * M, M, wd, y0, fy, accx[t], accy[t], wsum[t]);
         });
-        dst[idx] = (wsum > T(0)) ? Cx<T>{accx / wsum, accy / wsum} : Cx<T>{T(0), T(0)};
+#pragma unroll
+        for (int t = 0; t < XC; ++t)
+            dst[((uint64_t)z * N + x0 + t) * M + y] =
+                (wsum[t] > T(0)) ? Cx<T>{accx[t] / wsum[t], accy[t] / wsum[t]} : Cx<T>{T(0), T(0)};
     });
+}
+
+// the windowed merge: four voxels per item where the side allows
+template <typename T>
+cudaError_t merge_windowed(const Cx<T>* src, Cx<T>* dst, const AngleTable& t, int64_t m, int64_t n, int64_t l,
+                           cudaStream_t st) {
+    if (n % 4 == 0)
+        k_complex2d_to_3d_w<T, 4><<<resident_grid(k_complex2d_to_3d_w<T, 4>, EW_THREADS), EW_THREADS, 0, st>>>(
+            src, dst, t, m, n, l);
+    else
+        k_complex2d_to_3d_w<T, 1><<<resident_grid(k_complex2d_to_3d_w<T, 1>, EW_THREADS), EW_THREADS, 0, st>>>(
+            src, dst, t, m, n, l);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -574,14 +619,12 @@ cudaError_t launch_complex2d_to_3d(bool dbl, const void* src, void* dst, const v
         const AngleTable t = angle_table_view(atab, (int64_t)p);
         e = cudaMemsetAsync(t.next, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
-        if (dbl)
-            k_complex2d_to_3d_w<double><<<resident_grid(k_complex2d_to_3d_w<double>, EW_THREADS), EW_THREADS, 0, st>>>(
-                (const Cx<double>*)src, (Cx<double>*)dst, t, (int64_t)m, (int64_t)n, (int64_t)l);
-        else
-            k_complex2d_to_3d_w<float><<<resident_grid(k_complex2d_to_3d_w<float>, EW_THREADS), EW_THREADS, 0, st>>>(
-                (const Cx<float>*)src, (Cx<float>*)dst, t, (int64_t)m, (int64_t)n, (int64_t)l);
+        e = dbl ? merge_windowed<double>((const Cx<double>*)src, (Cx<double>*)dst, t, (int64_t)m, (int64_t)n,
+                                         (int64_t)l, st)
+                : merge_windowed<float>((const Cx<float>*)src, (Cx<float>*)dst, t, (int64_t)m, (int64_t)n,
+                                        (int64_t)l, st);
         count_launches(2);
-        return cudaGetLastError();
+        return e;
     }
     if (dbl)
         k_complex2d_to_3d<double><<<g, EW_THREADS, 0, st>>>((const Cx<double>*)src, (Cx<double>*)dst,
