@@ -46,13 +46,14 @@ inline AngleTable angle_table_view(void* buf, int64_t P) {
 }
 
 // The voxels of a gather over slices cost very different amounts (a voxel
-// near the tilt axis is near many slices, a far one near few), so they are
-// handed out dynamically: each warp takes 32 * GATHER_VOXELS_PER_LANE
-// consecutive voxel indices from the counter at a time until the volume is
-// done, and calls f(i) for each of its lanes' indices.  Every voxel is still
-// computed by one thread with the same arithmetic.  Launch exactly the
-// resident CTAs (the counter replaces the grid-stride loop) with the counter
-// zeroed on the same stream; all 32 lanes of every warp take part.
+// near the tilt axis is near many slices, a far one near few), so the work
+// items (voxels, or short runs of them) are handed out dynamically: each warp
+// takes 32 * GATHER_VOXELS_PER_LANE consecutive item indices from the
+// counter at a time until all `total` are done, and calls f(i) for each of
+// its lanes' indices.  Every item is still computed by one thread with the
+// same arithmetic.  Launch exactly the resident CTAs (the counter replaces
+// the grid-stride loop) with the counter zeroed on the same stream; all 32
+// lanes of every warp take part.
 constexpr int GATHER_VOXELS_PER_LANE = 4;
 template <class Fn>
 __device__ __forceinline__ void for_voxels_dynamic(unsigned long long* next, uint64_t total, Fn f) {
