@@ -663,12 +663,14 @@ def test_rfactor_vs_oracle(tb, L, B, shared):
     np.testing.assert_array_equal(host(xd), x)   # input untouched
 
 
-@pytest.mark.parametrize("M,P,tol", [(24, 10, 1e-5), (64, 40, 1e-4)])
+@pytest.mark.parametrize("M,P,tol", [(24, 10, 1e-5), (64, 40, 1e-4), (18, 12, 1e-5)])
 def test_complex_merge_vs_oracle(tb, M, P, tol):
     """Project-defined trilinear gather merge (Complex2DTo3DInterpolation)
     against the float64 oracle.  Coordinates and weights are float: their
     rounding (about M/2 * 2^-23 absolute) bounds the relative L2 error at
-    1e-5 for 24^3 and 1e-4 for 64^3."""
+    1e-5 for 24^3 and 1e-4 for 64^3.  At 24^3 and 64^3 a work item is four
+    voxels along the tilt axis; 18 is no multiple of 4, so 18^3 runs one
+    voxel per item."""
     torch, cb = tb
     rng = np.random.default_rng(21)
     N = L = M
