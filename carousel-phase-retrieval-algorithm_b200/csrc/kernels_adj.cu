@@ -209,13 +209,12 @@ __global__ void k_sum3_final(const double* __restrict__ partials, double* __rest
 // |xq - u| < 1, |yq - v| < sqrt 2; turned back by -r that rectangle bounds the
 // candidate (xr, yr), whose weight is then computed as in the forward sample.
 constexpr double ADJ_SQRT2 = 1.4142135623730951;
+// the pixels part: (u, v) the voxel's in-plane coordinates before the
+// rotation (u = k along the tilt axis, v from the voxel's (j, l) only)
 template <typename T>
-__device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const Orient<T>& o, int64_t M, int64_t N,
-                                             T hl, T hn, T hm, T j, T k, T l, int64_t z, int64_t x, int64_t y, T& re,
-                                             T& im) {
-    const T d = j * o.ca - l * o.sa;
-    if (!(absT(d) < T(ADJ_SQRT2 + 1e-3))) return;
-    const T u = k, v = j * o.sa + l * o.ca;
+__device__ __forceinline__ void gather_pixels(const Cx<T>* __restrict__ Gp, const Orient<T>& o, int64_t M, int64_t N,
+                                              T hl, T hn, T hm, T u, T v, int64_t z, int64_t x, int64_t y, T& re,
+                                              T& im) {
     const T xc = o.cr * u + o.sr * v, yc = o.cr * v - o.sr * u;
     const T ar = absT(o.cr), as = absT(o.sr);
     const T hx = ar + as * T(ADJ_SQRT2) + T(1e-3), hy = as + ar * T(ADJ_SQRT2) + T(1e-3);
@@ -239,6 +238,22 @@ __device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const
             im += w * g.y;
         }
     }
+}
+// the plane part first: the slice's distance d from the voxel's point (j, l)
+// decides whether the slice can reach it at all
+template <typename T>
+__device__ __forceinline__ bool gather_plane(const Orient<T>& o, T j, T l, T& v) {
+    const T d = j * o.ca - l * o.sa;
+    if (!(absT(d) < T(ADJ_SQRT2 + 1e-3))) return false;
+    v = j * o.sa + l * o.ca;
+    return true;
+}
+template <typename T>
+__device__ __forceinline__ void gather_slice(const Cx<T>* __restrict__ Gp, const Orient<T>& o, int64_t M, int64_t N,
+                                             T hl, T hn, T hm, T j, T k, T l, int64_t z, int64_t x, int64_t y, T& re,
+                                             T& im) {
+    T v;
+    if (gather_plane(o, j, l, v)) gather_pixels(Gp, o, M, N, hl, hn, hm, k, v, z, x, y, re, im);
 }
 
 // gradient with respect to V, every slice visited (more slices than the
@@ -264,32 +279,51 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint(const Cx<T>* __re
 // (angle_table.cuh: ordered by tilt, which alone fixes the plane), in
 // direction order; voxels handed out dynamically (their cost varies with
 // the distance from the tilt axis)
-template <typename T>
+// XC voxels along the tilt axis per work item at one (z, y): the slices near
+// them and each slice's plane part depend only on (z, y), so they are found
+// once for the item; each voxel sums its slices' pixels in the same order as
+// alone.  Consecutive items take consecutive y (coalesced reads and stores).
+// Two voxels per item pay where the slices are dense (a voxel then has many
+// candidates): measured 21.5 -> 19.7 ms at 512^3 x 720 slices, but 1.51 ->
+// 1.68 ms at 256^3 x 180, so from ADJ_XC2_SLICES slices on (between the two).
+constexpr int ADJ_XC2_SLICES = 360;
+template <typename T, int XC>
 __global__ void __launch_bounds__(ADJ_THREADS) k_slice_adjoint_w(const Cx<T>* __restrict__ G, const AngleTable at,
                                                                  const Orient<T>* __restrict__ tab,
                                                                  Cx<T>* __restrict__ gV, int64_t M, int64_t N,
                                                                  int64_t L) {
-    const uint64_t total = (uint64_t)L * N * M;
+    const int64_t chunks = N / XC;
+    const uint64_t total = (uint64_t)L * chunks * M;
     const T hl = (T)(L / 2), hn = (T)(N / 2), hm = (T)(M / 2);
     const bool narrow = total <= 0xffffffffull;  // 32-bit index arithmetic
     for_voxels_dynamic(at.next, total, [&](uint64_t i) {
-        int64_t y, x, z;
+        int64_t y, c, z;
         if (narrow) {
-            const uint32_t i32 = (uint32_t)i, m32 = (uint32_t)M, n32 = (uint32_t)N, q = i32 / m32;
+            const uint32_t i32 = (uint32_t)i, m32 = (uint32_t)M, c32 = (uint32_t)chunks, q = i32 / m32;
             y = (int64_t)(i32 - q * m32);
-            x = (int64_t)(q % n32);
-            z = (int64_t)(q / n32);
+            c = (int64_t)(q % c32);
+            z = (int64_t)(q / c32);
         } else {
             y = (int64_t)(i % M);
-            x = (int64_t)((i / M) % N);
-            z = (int64_t)(i / ((uint64_t)M * N));
+            c = (int64_t)((i / M) % chunks);
+            z = (int64_t)(i / ((uint64_t)M * chunks));
         }
-        const T j = (T)(L / 2 - z), k = (T)(x - N / 2), l = (T)(M / 2 - y);
-        T re = T(0), im = T(0);
+        const int64_t x0 = c * XC;
+        const T j = (T)(L / 2 - z), l = (T)(M / 2 - y);
+        T re[XC], im[XC];
+#pragma unroll
+        for (int t = 0; t < XC; ++t) re[t] = im[t] = T(0);
         for_slices_near(at, (double)(L / 2 - z), (double)(M / 2 - y), [&](int64_t p, double, double) {
-            gather_slice(G + p * N * M, tab[p], M, N, hl, hn, hm, j, k, l, z, x, y, re, im);
+            const Orient<T> o = tab[p];
+            T v;
+            if (!gather_plane(o, j, l, v)) return;
+            const Cx<T>* __restrict__ Gp = G + p * N * M;
+#pragma unroll
+            for (int t = 0; t < XC; ++t)
+                gather_pixels(Gp, o, M, N, hl, hn, hm, (T)(x0 + t - N / 2), v, z, x0 + t, y, re[t], im[t]);
         });
-        gV[i] = Cx<T>{re, im};
+#pragma unroll
+        for (int t = 0; t < XC; ++t) gV[((uint64_t)z * N + x0 + t) * M + y] = Cx<T>{re[t], im[t]};
     });
 }
 
@@ -414,8 +448,12 @@ cudaError_t slice_loss_grad_t(const void* V, const void* ang, const void* tab, c
         const AngleTable t = angle_table_view(atab, (int64_t)p);
         e = cudaMemsetAsync(t.next, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
-        k_slice_adjoint_w<T><<<resident_grid(k_slice_adjoint_w<T>, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
-            (const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n, l);
+        if (p >= (uint64_t)ADJ_XC2_SLICES && n % 2 == 0)
+            k_slice_adjoint_w<T, 2><<<resident_grid(k_slice_adjoint_w<T, 2>, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
+                (const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n, l);
+        else
+            k_slice_adjoint_w<T, 1><<<resident_grid(k_slice_adjoint_w<T, 1>, ADJ_THREADS), ADJ_THREADS, 0, st>>>(
+                (const Cx<T>*)G, t, (const Orient<T>*)tab, (Cx<T>*)gV, m, n, l);
         count_launches(2);
         return cudaGetLastError();
     }

@@ -276,6 +276,26 @@ def test_loss_grad_orient_vs_oracle(tb, dtype):
     np.testing.assert_allclose(gr, gro, rtol=10 * tol, atol=10 * tol * np.abs(gro).max())
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_loss_grad_orient_dense_slices_vs_oracle(tb, dtype):
+    """400 slices (dense: the adjoint gather takes two voxels along the tilt
+    axis per work item from 360 slices on) against the float64 oracle, at
+    the same tolerances as the sparse case."""
+    torch, cb = tb
+    M, P, L = 16, 400, 16
+    cdt = np.complex64 if dtype == "float32" else np.complex128
+    V, ang, rot, A = _orient_problem(M, P, L, 41, cdt)
+    impl = cb.B200Impl(M, M, L, 1, dtype=dtype)
+    gV = torch.zeros(V.size, dtype=torch.complex64 if dtype == "float32" else torch.complex128, device="cuda")
+    loss, ga, gr = impl.slice_loss_grad_orient(torch.from_numpy(V).cuda(), torch.from_numpy(ang).cuda(),
+                                               torch.from_numpy(rot).cuda(), torch.from_numpy(A).cuda(),
+                                               M, M, P, L, gV)
+    lo, gVo, gao, gro = O.slice_loss_grad_orient(V, ang, rot, A, M, M, P, L)
+    tol = 1e-5 if dtype == "float32" else 1e-12
+    assert abs(loss - lo) / lo < tol
+    assert O.rel_l2(gV.cpu().numpy(), gVo.ravel()) < tol
+
+
 def test_loss_grad_orient_vs_finite_differences(tb):
     """Central differences in float64: h = 1e-3 on the volume, h = 1e-6 on the
     tilts and rotations (trilinear weights have kinks where a sample point
@@ -398,13 +418,15 @@ def test_refine_orient_recovers_tilt_and_rotation(tb):
     np.testing.assert_array_equal(v.cpu().numpy(), vol)   # lr_volume 0 holds the volume
 
 
-def test_gathers_deterministic_with_dynamic_voxels(tb):
-    """The merge and the adjoint gather hand their voxels to the resident
+@pytest.mark.parametrize("P", [90, 400])
+def test_gathers_deterministic_with_dynamic_voxels(tb, P):
+    """The merge and the adjoint gather hand their work to the resident
     warps from a counter, in whatever order the warps come; each voxel is
     still summed by one thread in a fixed order, so repeated calls (the
-    counter reused, the context fresh or not) give the same bits."""
+    counter reused, the context fresh or not) give the same bits (at 400
+    slices the adjoint takes two voxels per work item)."""
     torch, cb = tb
-    M, P, L = 64, 90, 64
+    M, L = 64, 64
     V, ang, A = _problem(M, P, L, 31)
     rot = (np.random.default_rng(32).standard_normal(P) * 0.005).astype(np.float32)
     Vd, angd, Ad, rotd = (torch.from_numpy(a).cuda() for a in (V, ang, A, rot))
